@@ -1,0 +1,249 @@
+"""ctypes access to the C oracle (liboracle.so) and to the reference CPU factor
+built under oracle/_ref/.  Test infrastructure: imported only by tests/,
+__graft_entry__.smoke() and the CPU-baseline leg of bench.py.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_BIN = os.path.join(HERE, "_ref", "rchol_ref_cpu")
+REF_BIN_PINNED = os.path.join(HERE, "_ref", "rchol_ref_cpu_pinned")
+
+MODE_B200 = 0
+MODE_REF_REPLAY = 1
+STOP_RELRES = 0
+STOP_PRECOND = 1
+STOP_ABS_R2 = 2
+
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+
+
+class FactorStats(C.Structure):
+    _fields_ = [("nnz_strict", C.c_int64), ("fills", C.c_int64), ("merged_away", C.c_int64),
+                ("max_degree", C.c_int32), ("max_gather", C.c_int32)]
+
+
+class PcgInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("relres_true", C.c_double),
+                ("relres_rec", C.c_double), ("precond_ratio", C.c_double)]
+
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.orc_zero_sum_vector.argtypes = [_f64p, C.c_int64, C.c_uint32]
+        L.orc_philox4x32_10.argtypes = [_u32p, _u32p, _u32p]
+        L.orc_sample_uniform.argtypes = [C.c_uint64, C.c_int32, C.c_int32]
+        L.orc_sample_uniform.restype = C.c_double
+        L.orc_has_diagonal.argtypes = [C.c_int64, _i32p, _i32p]
+        L.orc_triplets_to_csc.argtypes = [C.c_int32, C.c_int64, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p]
+        L.orc_triplets_to_csc.restype = C.c_int64
+        L.orc_lower_count.argtypes = [C.c_int32, _i32p, _i32p]
+        L.orc_lower_count.restype = C.c_int64
+        L.orc_lower_triangle.argtypes = [C.c_int32, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p]
+        L.orc_dependency_counts.argtypes = [C.c_int32, _i32p, _i32p, _i32p]
+        L.orc_trim_last.argtypes = [C.c_int32, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p]
+        L.orc_trim_last.restype = C.c_int64
+        L.orc_factor_run.argtypes = [C.c_int32, _i32p, _i32p, _f64p, _i32p, C.c_int, C.c_uint64]
+        L.orc_factor_run.restype = C.c_void_p
+        L.orc_factor_stats_get.argtypes = [C.c_void_p, C.POINTER(FactorStats)]
+        L.orc_factor_export.argtypes = [C.c_void_p, _i64p, _i32p, _f64p, _f64p, _i32p]
+        L.orc_factor_free.argtypes = [C.c_void_p]
+        L.orc_spmv.argtypes = [C.c_int32, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int]
+        L.orc_precond_apply.argtypes = [C.c_int32, _i64p, _i32p, _f64p, _f64p, _f64p, _f64p, _f64p]
+        L.orc_pcg.argtypes = [C.c_int32, _i32p, _i32p, _f64p, _i64p, _i32p, _f64p, _f64p,
+                              _f64p, _f64p, C.c_double, C.c_int32, C.c_int, C.c_int,
+                              C.POINTER(PcgInfo)]
+        L.orc_pcg.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def zero_sum_vector(n, seed=0):
+    out = np.empty(n, np.float64)
+    lib().orc_zero_sum_vector(out, n, seed)
+    return out
+
+
+def philox(ctr, key):
+    out = np.zeros(4, np.uint32)
+    lib().orc_philox4x32_10(np.asarray(ctr, np.uint32), np.asarray(key, np.uint32), out)
+    return out
+
+
+def sample_uniform(seed, vertex, i):
+    return lib().orc_sample_uniform(seed, vertex, i)
+
+
+def triplets_to_csc(n, rows, cols, vals):
+    rows, cols, vals = _i32(rows), _i32(cols), _f64(vals)
+    has_diag = lib().orc_has_diagonal(len(rows), rows, cols)
+    total = len(rows) + (0 if has_diag else n)
+    colptr = np.zeros(n + 1, np.int32)
+    rowind = np.zeros(max(total, 1), np.int32)
+    val = np.zeros(max(total, 1), np.float64)
+    got = lib().orc_triplets_to_csc(n, len(rows), rows, cols, vals, colptr, rowind, val)
+    return colptr, rowind[:got], val[:got]
+
+
+def lower_triangle(n, colptr, rowind, val):
+    colptr, rowind, val = _i32(colptr), _i32(rowind), _f64(val)
+    cnt = lib().orc_lower_count(n, colptr, rowind)
+    lcp = np.zeros(n + 1, np.int32)
+    lr = np.zeros(max(cnt, 1), np.int32)
+    lv = np.zeros(max(cnt, 1), np.float64)
+    lib().orc_lower_triangle(n, colptr, rowind, val, lcp, lr, lv)
+    return lcp, lr[:cnt], lv[:cnt]
+
+
+def dependency_counts(n, colptr, rowind):
+    dep = np.zeros(n, np.int32)
+    lib().orc_dependency_counts(n, _i32(colptr), _i32(rowind), dep)
+    return dep
+
+
+def trim_last(n, colptr, rowind, val):
+    colptr, rowind, val = _i32(colptr), _i32(rowind), _f64(val)
+    ocp = np.zeros(n, np.int32)
+    orow = np.zeros(max(len(rowind), 1), np.int32)
+    oval = np.zeros(max(len(rowind), 1), np.float64)
+    got = lib().orc_trim_last(n, colptr, rowind, val, ocp, orow, oval)
+    return ocp, orow[:got], oval[:got]
+
+
+def factor(n, lcolptr, lrow, lval, dep0, mode=MODE_B200, seed=1):
+    L = lib()
+    h = L.orc_factor_run(n, _i32(lcolptr), _i32(lrow), _f64(lval), _i32(dep0), mode, seed)
+    if not h:
+        raise MemoryError("oracle factor failed")
+    st = FactorStats()
+    L.orc_factor_stats_get(h, C.byref(st))
+    nnz = st.nnz_strict
+    colptr = np.zeros(n + 1, np.int64)
+    rowind = np.zeros(max(nnz, 1), np.int32)
+    val = np.zeros(max(nnz, 1), np.float64)
+    diag = np.zeros(max(n, 1), np.float64)
+    fills = np.zeros(max(n, 1), np.int32)
+    L.orc_factor_export(h, colptr, rowind, val, diag, fills)
+    L.orc_factor_free(h)
+    return dict(colptr=colptr, rowind=rowind[:nnz], val=val[:nnz], diag=diag[:n],
+                fills_received=fills[:n],
+                stats=dict(nnz_strict=st.nnz_strict, fills=st.fills, merged_away=st.merged_away,
+                           max_degree=st.max_degree, max_gather=st.max_gather))
+
+
+def spmv(n, rowptr, colind, val, x, nthreads=1):
+    y = np.zeros(n, np.float64)
+    lib().orc_spmv(n, _i32(rowptr), _i32(colind), _f64(val), _f64(x), y, nthreads)
+    return y
+
+
+def precond_apply(n, lcolptr, lrow, lval, diag, r):
+    z = np.zeros(n, np.float64)
+    work = np.zeros(n, np.float64)
+    lib().orc_precond_apply(n, np.ascontiguousarray(lcolptr, np.int64), _i32(lrow), _f64(lval),
+                            _f64(diag), _f64(r), z, work)
+    return z
+
+
+def pcg(n, arowptr, acolind, aval, lcolptr, lrow, lval, diag, b, tol=1e-6, max_iter=1000,
+        stop_rule=STOP_RELRES, nthreads=1):
+    x = np.zeros(n, np.float64)
+    info = PcgInfo()
+    rc = lib().orc_pcg(n, _i32(arowptr), _i32(acolind), _f64(aval),
+                       np.ascontiguousarray(lcolptr, np.int64), _i32(lrow), _f64(lval),
+                       _f64(diag), _f64(b), x, tol, max_iter, stop_rule, nthreads, C.byref(info))
+    if rc != 0:
+        raise MemoryError("oracle pcg failed")
+    return x, dict(iterations=info.iterations, converged=bool(info.converged),
+                   relres_true=info.relres_true, relres_rec=info.relres_rec,
+                   precond_ratio=info.precond_ratio)
+
+
+# ---------------------------------------------------------------------------
+# MatrixMarket text IO (small test inputs) and the reference CPU factor
+# ---------------------------------------------------------------------------
+
+def write_mtx(path, n, rows, cols, vals):
+    """1-based coordinate/real/general file, entries in the given order."""
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n")
+        f.write(f"{n} {n} {len(rows)}\n")
+        lines = [f"{r + 1} {c + 1} {v:.17g}\n" for r, c, v in zip(rows, cols, vals)]
+        f.write("".join(lines))
+
+
+def read_factor_files(prefix, n):
+    """Read <prefix>l_sol.mtx (1-based CSC of L incl. unit diagonal) and
+    <prefix>sol_diag.txt as written by driver_local.cpp:958-988."""
+    with open(prefix + "l_sol.mtx") as f:
+        header = f.readline()
+        assert header.startswith("%%MatrixMarket")
+        line = f.readline()
+        while line.startswith("%"):
+            line = f.readline()
+        nr, nc, nnz = map(int, line.split())
+        data = np.loadtxt(f, dtype=np.float64, ndmin=2) if nnz else np.zeros((0, 3))
+    rows = data[:, 0].astype(np.int64) - 1
+    cols = data[:, 1].astype(np.int64) - 1
+    vals = data[:, 2]
+    diag = np.loadtxt(prefix + "sol_diag.txt", dtype=np.float64, ndmin=1)
+    return rows, cols, vals, diag
+
+
+def run_reference(mtx_path, threads=1, physics=False, pinned_seed=None, want_factor=True,
+                  timeout=600):
+    """Run the reference CPU factor (cpu_implementation/driver_local.cpp main,
+    :1325-1350): `driver <mtx> <threads> <out_prefix> [1]`.  Returns the
+    parsed factor time and, if requested, the written factor."""
+    binary = REF_BIN_PINNED if pinned_seed is not None else REF_BIN
+    env = dict(os.environ)
+    env["OMP_NUM_THREADS"] = str(threads)
+    env.setdefault("OMP_PROC_BIND", "close")
+    if pinned_seed is not None:
+        env["RCHOL_REF_SEED"] = str(pinned_seed)
+    with tempfile.TemporaryDirectory() as td:
+        prefix = (td + "/") if want_factor else ""
+        args = [binary, mtx_path, str(threads), prefix] + (["1"] if physics else [])
+        p = subprocess.run(args, env=env, capture_output=True, text=True, timeout=timeout)
+        if p.returncode != 0:
+            raise RuntimeError(f"reference factor failed ({p.returncode}): {p.stderr[-2000:]}")
+        m = re.search(r"Factorization execution time: ([0-9.eE+-]+) seconds", p.stdout)
+        t = float(m.group(1)) if m else float("nan")
+        m2 = re.search(r"factor nnz: (\d+)", p.stdout)
+        out = dict(factor_time=t, factor_nnz=int(m2.group(1)) if m2 else -1, stdout=p.stdout)
+        if want_factor:
+            nm = re.search(r"number of nodes: (\d+)", p.stdout)
+            n = int(nm.group(1))
+            rows, cols, vals, diag = read_factor_files(prefix, n)
+            out.update(rows=rows, cols=cols, vals=vals, diag=diag, n=n)
+        return out

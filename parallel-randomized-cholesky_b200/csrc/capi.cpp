@@ -1,0 +1,1096 @@
+// C-ABI implementation (include/rchol.h): context, matrix upload, factor
+// orchestration with capacity retries, PCG, the reference drop-ins.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/rchol.h"
+#include "host_io.h"
+#include "rchol_internal.h"
+
+using rchol::DevCsc;
+using rchol::DevFactor;
+using rchol::FactorWork;
+
+struct rchol_ctx {
+    rchol_opts o;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    DevCsc A;        // as loaded (ground vertex included when trim)
+    DevCsc At;       // the matrix of the solve (A itself when not trimmed)
+    bool trim = false;
+    bool have = false;
+    int32_t max_col = 0;  // largest column length of A
+    FactorWork w;
+    bool w_ready = false;
+    // solver cache
+    rchol::PcgSolver* solver = nullptr;
+    const rchol_factor_t* solver_f = nullptr;
+    int solver_k = 0, solver_fp32 = -1, solver_stop = -1, solver_maxit = -1;
+    double solver_tol = -1;
+    // device staging for solves (row-major blocks)
+    double* dB = nullptr;
+    double* dX = nullptr;
+    size_t stage_elems = 0;
+};
+
+struct rchol_factor {
+    rchol_ctx* ctx = nullptr;
+    DevFactor F;
+    rchol_factor_info info;
+};
+
+namespace {
+
+rchol_status fail(rchol_ctx* c, rchol_status s, const std::string& msg) {
+    if (c) c->err = msg;
+    return s;
+}
+
+rchol_status cuda_fail(rchol_ctx* c, cudaError_t e, const char* where) {
+    return fail(c, RCHOL_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call, where)                                   \
+    do {                                                  \
+        cudaError_t e__ = (call);                         \
+        if (e__ != cudaSuccess) return cuda_fail(ctx, e__, where); \
+    } while (0)
+
+template <typename T>
+cudaError_t dalloc(T** p, int64_t n) {
+    return cudaMalloc((void**)p, sizeof(T) * (size_t)(n > 0 ? n : 1));
+}
+
+void free_csc(DevCsc& a) {
+    cudaFree(a.colptr);
+    cudaFree(a.rowind);
+    cudaFree(a.val);
+    a = DevCsc();
+}
+
+void free_work(FactorWork& w) {
+    void* ps[] = {w.lcolptr, w.lrow,  w.lval, w.dep,  w.queue,  w.fcnt,   w.brow,     w.bval,       w.chead,
+                  w.cnext,   w.crow,  w.cval, w.prow, w.pval,   w.pstart, w.pcnt,     w.diag,       w.gscratch,
+                  w.counters, w.counters64, w.scan_tmp};
+    for (void* p : ps) cudaFree(p);
+    w = FactorWork();
+}
+
+void free_factor(DevFactor& f) {
+    void* ps[] = {f.lc_ptr, f.lc_idx, f.lc_val, f.lc_val32, f.lr_ptr, f.lr_idx, f.lr_val, f.lr_val32, f.diag,
+                  f.diag32};
+    for (void* p : ps) cudaFree(p);
+    f = DevFactor();
+}
+
+int64_t pow2_ge(int64_t x) {
+    int64_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+bool has_device() {
+    int n = 0;
+    return cudaGetDeviceCount(&n) == cudaSuccess && n > 0;
+}
+
+// Sizes of the factor work pools.
+struct PoolPlan {
+    int c0;
+    int32_t nchunks;
+    int64_t pool_cap;
+    int64_t gscratch_entries;
+    int grid, block;
+};
+
+rchol_status alloc_work(rchol_ctx* ctx, const PoolPlan& pp) {
+    FactorWork& w = ctx->w;
+    const int32_t n = ctx->A.n;
+    w.n = n;
+    w.c0 = pp.c0;
+    w.nchunks = pp.nchunks;
+    w.pool_cap = pp.pool_cap;
+    w.gscratch_entries = pp.gscratch_entries;
+    const int64_t warps = (int64_t)pp.grid * (pp.block / 32);
+    CK(dalloc(&w.lcolptr, (int64_t)n + 1), "alloc lcolptr");
+    CK(dalloc(&w.lrow, w.lnnz), "alloc lrow");
+    CK(dalloc(&w.lval, w.lnnz), "alloc lval");
+    CK(dalloc(&w.dep, n), "alloc dep");
+    CK(dalloc(&w.queue, n), "alloc queue");
+    CK(dalloc(&w.fcnt, n), "alloc fcnt");
+    CK(dalloc(&w.brow, (int64_t)n * w.c0), "alloc bucket rows");
+    CK(dalloc(&w.bval, (int64_t)n * w.c0), "alloc bucket values");
+    CK(dalloc(&w.chead, n), "alloc chunk heads");
+    CK(dalloc(&w.cnext, w.nchunks), "alloc chunk links");
+    CK(dalloc(&w.crow, (int64_t)w.nchunks * 64), "alloc chunk rows");
+    CK(dalloc(&w.cval, (int64_t)w.nchunks * 64), "alloc chunk values");
+    CK(dalloc(&w.prow, w.pool_cap), "alloc pool rows");
+    CK(dalloc(&w.pval, w.pool_cap), "alloc pool values");
+    CK(dalloc(&w.pstart, n), "alloc pool starts");
+    CK(dalloc(&w.pcnt, n), "alloc pool counts");
+    CK(dalloc(&w.diag, n), "alloc diag");
+    CK(cudaMalloc((void**)&w.gscratch, (size_t)warps * (size_t)w.gscratch_entries * 32), "alloc slab scratch");
+    CK(dalloc(&w.counters, 16), "alloc counters");
+    CK(dalloc(&w.counters64, 4), "alloc counters64");
+    CK(cudaMalloc(&w.scan_tmp, rchol::scan_tmp_bytes(n)), "alloc scan scratch");
+    return RCHOL_OK;
+}
+
+// Strict-lower nnz of the loaded matrix (device count + scan).
+rchol_status lower_nnz(rchol_ctx* ctx, int64_t* out) {
+    const int32_t n = ctx->A.n;
+    int32_t* cnt = nullptr;
+    int64_t* ptr = nullptr;
+    void* tmp = nullptr;
+    CK(dalloc(&cnt, n), "alloc counts");
+    CK(dalloc(&ptr, (int64_t)n + 1), "alloc ptr");
+    CK(cudaMalloc(&tmp, rchol::scan_tmp_bytes(n)), "alloc scan");
+    CK(rchol::launch_count_lower(ctx->A, cnt, ctx->stream), "count lower");
+    CK(rchol::exclusive_scan_i32_to_i64(cnt, ptr, n, tmp, ctx->stream), "scan lower");
+    CK(cudaMemcpyAsync(out, ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream), "copy lnnz");
+    CK(cudaStreamSynchronize(ctx->stream), "sync lnnz");
+    cudaFree(cnt);
+    cudaFree(ptr);
+    cudaFree(tmp);
+    return RCHOL_OK;
+}
+
+rchol_status install_host_csc(rchol_ctx* ctx, const rchol::HostCsc& h, int trim_ground) {
+    if (trim_ground && h.n < 2)
+        return fail(ctx, RCHOL_ERR_INVALID, "trim_ground needs at least two vertices");
+    for (double v : h.val)
+        if (!std::isfinite(v)) return fail(ctx, RCHOL_ERR_NUMERIC, "non-finite matrix entry");
+    return rchol_set_csc(ctx, h.n, h.colptr.data(), h.rowind.data(), h.val.data(), 0, trim_ground);
+}
+
+void drop_solver(rchol_ctx* ctx) {
+    if (ctx->solver) rchol::pcg_destroy(ctx->solver);
+    ctx->solver = nullptr;
+    ctx->solver_f = nullptr;
+}
+
+rchol_status ensure_stage(rchol_ctx* ctx, size_t elems) {
+    if (ctx->stage_elems >= elems) return RCHOL_OK;
+    cudaFree(ctx->dB);
+    cudaFree(ctx->dX);
+    ctx->dB = ctx->dX = nullptr;
+    ctx->stage_elems = 0;
+    CK(cudaMalloc(&ctx->dB, sizeof(double) * elems), "alloc rhs staging");
+    CK(cudaMalloc(&ctx->dX, sizeof(double) * elems), "alloc solution staging");
+    ctx->stage_elems = elems;
+    return RCHOL_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// context
+// ===========================================================================
+
+extern "C" rchol_status rchol_opts_default(rchol_opts* o) {
+    if (!o) return RCHOL_ERR_INVALID;
+    std::memset(o, 0, sizeof(*o));
+    o->precision = RCHOL_PREC_FP64;
+    o->seed = 1;
+    o->num_blocks = 0;
+    o->warps_per_block = 8;
+    o->slab_entries = 256;
+    o->bucket_cap = 32;
+    o->pool_mult = 6.0;
+    o->max_iter = 1000;
+    o->tol = 1e-6;
+    o->stop_rule = RCHOL_STOP_RELRES;
+    o->unroll = 4;
+    o->use_graph = 1;
+    o->device = 0;
+    o->timeout_s = 30.0;
+    o->verbose = 0;
+    return RCHOL_OK;
+}
+
+static rchol_status check_opts(const rchol_opts* o, std::string& why) {
+    if (o->precision != RCHOL_PREC_FP64 && o->precision != RCHOL_PREC_FP32_FACTOR) why = "precision";
+    else if (o->warps_per_block < 1 || o->warps_per_block > 8) why = "warps_per_block must be 1..8";
+    else if (o->slab_entries < 32 || (o->slab_entries & (o->slab_entries - 1))) why = "slab_entries must be a power of two >= 32";
+    else if (o->bucket_cap < 1) why = "bucket_cap must be positive";
+    else if (!(o->pool_mult >= 1.0)) why = "pool_mult must be >= 1";
+    else if (o->max_iter < 1) why = "max_iter must be positive";
+    else if (!(o->tol > 0.0)) why = "tol must be positive";
+    else if (o->stop_rule < 0 || o->stop_rule > 2) why = "stop_rule";
+    else if (o->unroll < 1 || o->unroll > 64) why = "unroll must be 1..64";
+    else if (!(o->timeout_s > 0.0)) why = "timeout_s must be positive";
+    else return RCHOL_OK;
+    return RCHOL_ERR_INVALID;
+}
+
+extern "C" rchol_status rchol_create(rchol_ctx** out, const rchol_opts* opts) {
+    if (!out) return RCHOL_ERR_INVALID;
+    *out = nullptr;
+    rchol_opts o;
+    if (opts) o = *opts;
+    else rchol_opts_default(&o);
+    std::string why;
+    if (check_opts(&o, why) != RCHOL_OK) return RCHOL_ERR_INVALID;
+    if (!has_device()) return RCHOL_ERR_NO_DEVICE;
+    if (cudaSetDevice(o.device) != cudaSuccess) return RCHOL_ERR_NO_DEVICE;
+    rchol_ctx* ctx = new rchol_ctx();
+    ctx->o = o;
+    ctx->device = o.device;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return RCHOL_ERR_CUDA;
+    }
+    *out = ctx;
+    return RCHOL_OK;
+}
+
+extern "C" void rchol_destroy(rchol_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    drop_solver(ctx);
+    free_work(ctx->w);
+    if (ctx->trim) free_csc(ctx->At);
+    free_csc(ctx->A);
+    cudaFree(ctx->dB);
+    cudaFree(ctx->dX);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+extern "C" rchol_status rchol_set_opts(rchol_ctx* ctx, const rchol_opts* o) {
+    if (!ctx || !o) return RCHOL_ERR_INVALID;
+    std::string why;
+    if (check_opts(o, why) != RCHOL_OK) return fail(ctx, RCHOL_ERR_INVALID, "bad option: " + why);
+    if (o->device != ctx->device) return fail(ctx, RCHOL_ERR_INVALID, "device cannot change");
+    bool pools = o->bucket_cap != ctx->o.bucket_cap || o->pool_mult != ctx->o.pool_mult ||
+                 o->slab_entries != ctx->o.slab_entries || o->warps_per_block != ctx->o.warps_per_block ||
+                 o->num_blocks != ctx->o.num_blocks;
+    ctx->o = *o;
+    if (pools) {
+        free_work(ctx->w);
+        ctx->w_ready = false;
+    }
+    drop_solver(ctx);
+    return RCHOL_OK;
+}
+
+extern "C" const char* rchol_status_string(rchol_status s) {
+    switch (s) {
+        case RCHOL_OK: return "ok";
+        case RCHOL_ERR_INVALID: return "invalid argument";
+        case RCHOL_ERR_IO: return "i/o error";
+        case RCHOL_ERR_CUDA: return "CUDA error";
+        case RCHOL_ERR_CAPACITY: return "device pool capacity exceeded";
+        case RCHOL_ERR_TIMEOUT: return "device wait timed out";
+        case RCHOL_ERR_NOT_CONVERGED: return "PCG did not converge";
+        case RCHOL_ERR_NO_DEVICE: return "no CUDA device";
+        case RCHOL_ERR_NUMERIC: return "non-finite or invalid numeric input";
+        case RCHOL_ERR_NO_MATRIX: return "no matrix loaded";
+    }
+    return "unknown status";
+}
+
+extern "C" const char* rchol_last_error(const rchol_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+// ===========================================================================
+// input
+// ===========================================================================
+
+extern "C" rchol_status rchol_set_csc(rchol_ctx* ctx, int n, const int* colptr, const int* rowind,
+                                      const double* val, int on_device, int trim_ground) {
+    if (!ctx || n <= 0 || !colptr || !rowind || !val) return fail(ctx, RCHOL_ERR_INVALID, "bad CSC arguments");
+    if (trim_ground && n < 2) return fail(ctx, RCHOL_ERR_INVALID, "trim_ground needs n >= 2");
+    cudaSetDevice(ctx->device);
+    drop_solver(ctx);
+    free_work(ctx->w);
+    ctx->w_ready = false;
+    if (ctx->trim) free_csc(ctx->At);
+    free_csc(ctx->A);
+    ctx->have = false;
+    int32_t nnz32 = 0;
+    std::vector<int32_t> hptr;
+    if (on_device) {
+        CK(cudaMemcpy(&nnz32, colptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost), "read nnz");
+    } else {
+        nnz32 = colptr[n];
+        for (int i = 0; i < n; ++i)
+            if (colptr[i + 1] < colptr[i]) return fail(ctx, RCHOL_ERR_INVALID, "colptr is not monotone");
+    }
+    if (nnz32 < 0) return fail(ctx, RCHOL_ERR_INVALID, "negative nnz");
+    DevCsc A;
+    A.n = n;
+    A.nnz = nnz32;
+    CK(dalloc(&A.colptr, (int64_t)n + 1), "alloc colptr");
+    CK(dalloc(&A.rowind, A.nnz), "alloc rowind");
+    CK(dalloc(&A.val, A.nnz), "alloc val");
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CK(cudaMemcpyAsync(A.colptr, colptr, sizeof(int32_t) * ((size_t)n + 1), kind, ctx->stream), "copy colptr");
+    CK(cudaMemcpyAsync(A.rowind, rowind, sizeof(int32_t) * (size_t)A.nnz, kind, ctx->stream), "copy rowind");
+    CK(cudaMemcpyAsync(A.val, val, sizeof(double) * (size_t)A.nnz, kind, ctx->stream), "copy val");
+    ctx->A = A;
+    ctx->trim = trim_ground != 0;
+    if (ctx->trim) {
+        CK(rchol::trim_matrix(ctx->A, ctx->At, ctx->stream), "trim matrix");
+    } else {
+        ctx->At = ctx->A;
+    }
+    CK(cudaStreamSynchronize(ctx->stream), "sync upload");
+    // largest column (bounds the gather of early vertices)
+    std::vector<int32_t> cp((size_t)n + 1);
+    CK(cudaMemcpy(cp.data(), ctx->A.colptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyDeviceToHost), "read colptr");
+    int32_t mx = 0;
+    for (int i = 0; i < n; ++i) mx = std::max(mx, cp[(size_t)i + 1] - cp[(size_t)i]);
+    ctx->max_col = mx;
+    ctx->have = true;
+    return RCHOL_OK;
+}
+
+extern "C" rchol_status rchol_set_triplets(rchol_ctx* ctx, int n, long long nnz, const int* rows, const int* cols,
+                                           const double* vals, int trim_ground) {
+    if (!ctx || n <= 0 || nnz < 0 || (nnz > 0 && (!rows || !cols || !vals)))
+        return fail(ctx, RCHOL_ERR_INVALID, "bad triplet arguments");
+    rchol::Triplets t;
+    t.n = n;
+    t.rows.assign(rows, rows + nnz);
+    t.cols.assign(cols, cols + nnz);
+    t.vals.assign(vals, vals + nnz);
+    rchol::HostCsc h;
+    std::string err;
+    if (!rchol::triplets_to_csc(t, h, err)) return fail(ctx, RCHOL_ERR_INVALID, err);
+    return install_host_csc(ctx, h, trim_ground);
+}
+
+extern "C" rchol_status rchol_load_mtx(rchol_ctx* ctx, const char* path, int trim_ground) {
+    if (!ctx || !path) return fail(ctx, RCHOL_ERR_INVALID, "null path");
+    rchol::Triplets t;
+    std::string err;
+    if (!rchol::read_mtx(path, t, err)) return fail(ctx, RCHOL_ERR_IO, err);
+    rchol::HostCsc h;
+    if (!rchol::triplets_to_csc(t, h, err)) return fail(ctx, RCHOL_ERR_INVALID, err);
+    return install_host_csc(ctx, h, trim_ground);
+}
+
+extern "C" rchol_status rchol_matrix_info(const rchol_ctx* ctx, int* n, long long* nnz) {
+    if (!ctx) return RCHOL_ERR_INVALID;
+    if (!ctx->have) return RCHOL_ERR_NO_MATRIX;
+    if (n) *n = ctx->A.n;
+    if (nnz) *nnz = ctx->A.nnz;
+    return RCHOL_OK;
+}
+
+extern "C" rchol_status rchol_matrix_copy_to_host(const rchol_ctx* cctx, int* colptr, int* rowind, double* val) {
+    rchol_ctx* ctx = const_cast<rchol_ctx*>(cctx);
+    if (!ctx) return RCHOL_ERR_INVALID;
+    if (!ctx->have) return RCHOL_ERR_NO_MATRIX;
+    if (colptr) CK(cudaMemcpy(colptr, ctx->A.colptr, sizeof(int32_t) * ((size_t)ctx->A.n + 1), cudaMemcpyDeviceToHost), "copy");
+    if (rowind) CK(cudaMemcpy(rowind, ctx->A.rowind, sizeof(int32_t) * (size_t)ctx->A.nnz, cudaMemcpyDeviceToHost), "copy");
+    if (val) CK(cudaMemcpy(val, ctx->A.val, sizeof(double) * (size_t)ctx->A.nnz, cudaMemcpyDeviceToHost), "copy");
+    return RCHOL_OK;
+}
+
+// ===========================================================================
+// factorization
+// ===========================================================================
+
+extern "C" rchol_status rchol_factor(rchol_ctx* ctx, rchol_factor_t** out) {
+    if (!ctx || !out) return fail(ctx, RCHOL_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (!ctx->have) return fail(ctx, RCHOL_ERR_NO_MATRIX, "no matrix loaded");
+    cudaSetDevice(ctx->device);
+    const rchol_opts& o = ctx->o;
+    const int block = 32 * o.warps_per_block;
+    const int max_grid = rchol::factor_resident_grid(block, o.slab_entries, ctx->device);
+    if (max_grid <= 0) return fail(ctx, RCHOL_ERR_CUDA, "factor kernel does not fit on the device");
+    int grid = max_grid;
+    if (o.num_blocks > 0) grid = std::max(1, std::min(max_grid, (o.num_blocks + o.warps_per_block - 1) / o.warps_per_block));
+
+    if (!ctx->w_ready) {
+        int64_t lnnz = 0;
+        rchol_status s = lower_nnz(ctx, &lnnz);
+        if (s != RCHOL_OK) return s;
+        ctx->w.lnnz = lnnz;
+        PoolPlan pp;
+        pp.c0 = o.bucket_cap;
+        pp.nchunks = (int32_t)std::min<int64_t>(INT32_MAX / 64, std::max<int64_t>(4096, lnnz / 16 + ctx->A.n / 8));
+        pp.pool_cap = (int64_t)(o.pool_mult * (double)lnnz) + ctx->A.n + (int64_t)max_grid * (block / 32) * 1024;
+        pp.gscratch_entries = std::max<int64_t>(1024, pow2_ge(4 * (int64_t)ctx->max_col));
+        pp.grid = max_grid;
+        pp.block = block;
+        s = alloc_work(ctx, pp);
+        if (s != RCHOL_OK) return s;
+        ctx->w_ready = true;
+    }
+    FactorWork& w = ctx->w;
+    cudaEvent_t ev[4];
+    for (auto& e : ev) CK(cudaEventCreate(&e), "event");
+    rchol_factor_info info;
+    std::memset(&info, 0, sizeof(info));
+    int32_t counters[16];
+    unsigned long long c64[4];
+    int attempt = 0;
+    for (;; ++attempt) {
+        CK(cudaEventRecord(ev[0], ctx->stream), "record");
+        CK(rchol::launch_lower_and_deps(ctx->A, w, ctx->stream), "lower triangle");
+        CK(rchol::launch_init_factor_state(w, ctx->stream), "init factor state");
+        CK(cudaEventRecord(ev[1], ctx->stream), "record");
+        rchol::FactorLaunch fl;
+        fl.grid = grid;
+        fl.block = block;
+        fl.smem_slab = o.slab_entries;
+        fl.seed = o.seed;
+        fl.timeout_s = o.timeout_s;
+        CK(rchol::launch_factor(w, fl, ctx->stream), "factor launch");
+        CK(cudaEventRecord(ev[2], ctx->stream), "record");
+        CK(cudaMemcpyAsync(counters, w.counters, sizeof(counters), cudaMemcpyDeviceToHost, ctx->stream), "counters");
+        CK(cudaMemcpyAsync(c64, w.counters64, sizeof(c64), cudaMemcpyDeviceToHost, ctx->stream), "counters");
+        CK(cudaStreamSynchronize(ctx->stream), "factor");
+        const int st = counters[3];
+        if (st == 0) break;
+        if (st == rchol::kDevTimeout) return fail(ctx, RCHOL_ERR_TIMEOUT, "factor: a device wait timed out");
+        if (st != rchol::kDevCapacity || attempt >= 3)
+            return fail(ctx, st == rchol::kDevCapacity ? RCHOL_ERR_CAPACITY : RCHOL_ERR_INVALID,
+                        "factor: device status " + std::to_string(st));
+        // grow the pool that ran out and retry from scratch
+        PoolPlan pp{w.c0, w.nchunks, w.pool_cap, w.gscratch_entries, max_grid, block};
+        if (counters[2] >= w.nchunks) pp.nchunks = (int32_t)std::min<int64_t>(INT32_MAX / 64, 2ll * w.nchunks + 1024);
+        if ((int64_t)c64[0] > w.pool_cap) pp.pool_cap = 2 * w.pool_cap;
+        if ((int64_t)counters[6] > w.gscratch_entries) pp.gscratch_entries = pow2_ge(2 * (int64_t)counters[6]);
+        if (pp.nchunks == w.nchunks && pp.pool_cap == w.pool_cap && pp.gscratch_entries == w.gscratch_entries) {
+            pp.nchunks = (int32_t)std::min<int64_t>(INT32_MAX / 64, 2ll * w.nchunks);
+            pp.pool_cap *= 2;
+            pp.gscratch_entries *= 2;
+        }
+        int64_t lnnz = w.lnnz;
+        free_work(w);
+        w.lnnz = lnnz;
+        rchol_status s = alloc_work(ctx, pp);
+        if (s != RCHOL_OK) return s;
+    }
+    rchol_factor_t* f = new rchol_factor_t();
+    f->ctx = ctx;
+    cudaError_t e = rchol::assemble_factor(w, ctx->trim, o.precision == RCHOL_PREC_FP32_FACTOR, f->F, ctx->stream);
+    if (e != cudaSuccess) {
+        free_factor(f->F);
+        delete f;
+        return cuda_fail(ctx, e, "assemble");
+    }
+    CK(cudaEventRecord(ev[3], ctx->stream), "record");
+    CK(cudaEventSynchronize(ev[3]), "sync");
+    int32_t sort_status = 0;
+    CK(cudaMemcpy(&sort_status, w.counters + 3, sizeof(int32_t), cudaMemcpyDeviceToHost), "status");
+    if (sort_status != 0) {
+        free_factor(f->F);
+        delete f;
+        return fail(ctx, RCHOL_ERR_CAPACITY, "assembly: row sort scratch too small");
+    }
+    cudaEventElapsedTime(&info.ms_setup, ev[0], ev[1]);
+    cudaEventElapsedTime(&info.ms_factor, ev[1], ev[2]);
+    cudaEventElapsedTime(&info.ms_assemble, ev[2], ev[3]);
+    for (auto& x : ev) cudaEventDestroy(x);
+    info.n = f->F.n;
+    info.n_factored = ctx->A.n;
+    info.nnz_strict = f->F.nnz;
+    info.nnz_lower_a = w.lnnz;
+    info.max_gather = counters[6];
+    info.big_vertices = counters[5];
+    info.overflow_fills = counters[7];
+    info.chunks_used = counters[2];
+    info.factor_grid = grid;
+    info.attempts = attempt + 1;
+    info.lc_ptr = reinterpret_cast<const long long*>(f->F.lc_ptr);
+    info.lc_idx = f->F.lc_idx;
+    info.lc_val = f->F.lc_val;
+    info.lr_ptr = reinterpret_cast<const long long*>(f->F.lr_ptr);
+    info.lr_idx = f->F.lr_idx;
+    info.lr_val = f->F.lr_val;
+    info.diag = f->F.diag;
+    info.fills = (long long)c64[1];
+    f->info = info;
+    *out = f;
+    return RCHOL_OK;
+}
+
+extern "C" rchol_status rchol_factor_get_info(const rchol_factor_t* f, rchol_factor_info* info) {
+    if (!f || !info) return RCHOL_ERR_INVALID;
+    *info = f->info;
+    return RCHOL_OK;
+}
+
+extern "C" rchol_status rchol_factor_copy_to_host(const rchol_factor_t* f, long long* colptr, int* rowind,
+                                                  double* val, double* diag) {
+    if (!f) return RCHOL_ERR_INVALID;
+    rchol_ctx* ctx = f->ctx;
+    cudaSetDevice(ctx->device);
+    const DevFactor& F = f->F;
+    if (colptr) CK(cudaMemcpy(colptr, F.lc_ptr, sizeof(int64_t) * ((size_t)F.n + 1), cudaMemcpyDeviceToHost), "copy");
+    if (rowind) CK(cudaMemcpy(rowind, F.lc_idx, sizeof(int32_t) * (size_t)F.nnz, cudaMemcpyDeviceToHost), "copy");
+    if (val) CK(cudaMemcpy(val, F.lc_val, sizeof(double) * (size_t)F.nnz, cudaMemcpyDeviceToHost), "copy");
+    if (diag) CK(cudaMemcpy(diag, F.diag, sizeof(double) * (size_t)F.n, cudaMemcpyDeviceToHost), "copy");
+    return RCHOL_OK;
+}
+
+extern "C" rchol_status rchol_factor_write(const rchol_factor_t* f, const char* prefix) {
+    if (!f || !prefix) return RCHOL_ERR_INVALID;
+    rchol_ctx* ctx = f->ctx;
+    const DevFactor& F = f->F;
+    std::vector<int64_t> cp((size_t)F.n + 1);
+    std::vector<int32_t> ri((size_t)F.nnz);
+    std::vector<double> v((size_t)F.nnz), d((size_t)F.n);
+    rchol_status s = rchol_factor_copy_to_host(f, reinterpret_cast<long long*>(cp.data()), ri.data(), v.data(), d.data());
+    if (s != RCHOL_OK) return s;
+    std::string err;
+    if (!rchol::write_factor_files(prefix, F.n, cp, ri, v, d, err)) return fail(ctx, RCHOL_ERR_IO, err);
+    return RCHOL_OK;
+}
+
+namespace {
+
+// Build a DevFactor from a host strict CSC of L and D (transpose on device).
+rchol_status factor_from_host_csc(rchol_ctx* ctx, int32_t n, const std::vector<int64_t>& cp,
+                                  const std::vector<int32_t>& ri, const std::vector<double>& v,
+                                  const std::vector<double>& d, rchol_factor_t** out) {
+    // host transpose (the adopted factor is a one-off input)
+    const int64_t nnz = cp[(size_t)n];
+    std::vector<int64_t> rp((size_t)n + 1, 0);
+    for (int64_t p = 0; p < nnz; ++p) rp[(size_t)ri[(size_t)p] + 1]++;
+    for (int32_t i = 0; i < n; ++i) rp[(size_t)i + 1] += rp[(size_t)i];
+    std::vector<int64_t> cur(rp.begin(), rp.end() - 1);
+    std::vector<int32_t> ci((size_t)nnz);
+    std::vector<double> cv((size_t)nnz);
+    for (int32_t j = 0; j < n; ++j)
+        for (int64_t p = cp[(size_t)j]; p < cp[(size_t)j + 1]; ++p) {
+            int64_t q = cur[(size_t)ri[(size_t)p]]++;
+            ci[(size_t)q] = j;
+            cv[(size_t)q] = v[(size_t)p];
+        }
+    rchol_factor_t* f = new rchol_factor_t();
+    f->ctx = ctx;
+    DevFactor& F = f->F;
+    F.n = n;
+    F.nnz = nnz;
+    std::vector<float> v32(v.begin(), v.end()), cv32(cv.begin(), cv.end()), d32(d.begin(), d.end());
+    auto up = [&](auto** dst, const auto& src) -> cudaError_t {
+        using T = typename std::remove_reference<decltype(src)>::type::value_type;
+        cudaError_t e = cudaMalloc((void**)dst, sizeof(T) * std::max<size_t>(src.size(), 1));
+        if (e != cudaSuccess) return e;
+        return cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice);
+    };
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = up(&F.lc_ptr, cp);
+    if (e == cudaSuccess) e = up(&F.lc_idx, ri);
+    if (e == cudaSuccess) e = up(&F.lc_val, v);
+    if (e == cudaSuccess) e = up(&F.lc_val32, v32);
+    if (e == cudaSuccess) e = up(&F.lr_ptr, rp);
+    if (e == cudaSuccess) e = up(&F.lr_idx, ci);
+    if (e == cudaSuccess) e = up(&F.lr_val, cv);
+    if (e == cudaSuccess) e = up(&F.lr_val32, cv32);
+    if (e == cudaSuccess) e = up(&F.diag, d);
+    if (e == cudaSuccess) e = up(&F.diag32, d32);
+    if (e != cudaSuccess) {
+        free_factor(F);
+        delete f;
+        return cuda_fail(ctx, e, "upload factor");
+    }
+    std::memset(&f->info, 0, sizeof(f->info));
+    f->info.n = n;
+    f->info.n_factored = n;
+    f->info.nnz_strict = nnz;
+    f->info.lc_ptr = reinterpret_cast<const long long*>(F.lc_ptr);
+    f->info.lc_idx = F.lc_idx;
+    f->info.lc_val = F.lc_val;
+    f->info.lr_ptr = reinterpret_cast<const long long*>(F.lr_ptr);
+    f->info.lr_idx = F.lr_idx;
+    f->info.lr_val = F.lr_val;
+    f->info.diag = F.diag;
+    *out = f;
+    return RCHOL_OK;
+}
+
+}  // namespace
+
+extern "C" rchol_status rchol_factor_read(rchol_ctx* ctx, const char* prefix, rchol_factor_t** out) {
+    if (!ctx || !prefix || !out) return fail(ctx, RCHOL_ERR_INVALID, "null argument");
+    cudaSetDevice(ctx->device);
+    int32_t n = 0;
+    std::vector<int64_t> cp;
+    std::vector<int32_t> ri;
+    std::vector<double> v, d;
+    std::string err;
+    if (!rchol::read_factor_files(prefix, n, cp, ri, v, d, err)) return fail(ctx, RCHOL_ERR_IO, err);
+    if (ctx->have && ctx->trim && n == ctx->A.n) {
+        // a factor written before the ground trim: drop the last vertex
+        std::vector<int64_t> cp2((size_t)n, 0);
+        std::vector<int32_t> ri2;
+        std::vector<double> v2;
+        for (int32_t j = 0; j + 1 < n; ++j) {
+            for (int64_t p = cp[(size_t)j]; p < cp[(size_t)j + 1]; ++p)
+                if (ri[(size_t)p] < n - 1) {
+                    ri2.push_back(ri[(size_t)p]);
+                    v2.push_back(v[(size_t)p]);
+                }
+            cp2[(size_t)j + 1] = (int64_t)ri2.size();
+        }
+        d.resize((size_t)n - 1);
+        return factor_from_host_csc(ctx, n - 1, cp2, ri2, v2, d, out);
+    }
+    return factor_from_host_csc(ctx, n, cp, ri, v, d, out);
+}
+
+extern "C" rchol_status rchol_factor_from_csr_upper(rchol_ctx* ctx, int n, const int* rowptr, const int* colind,
+                                                    const double* val, const double* diag, int on_device,
+                                                    rchol_factor_t** out) {
+    if (!ctx || n <= 0 || !rowptr || !colind || !val || !diag || !out)
+        return fail(ctx, RCHOL_ERR_INVALID, "null argument");
+    cudaSetDevice(ctx->device);
+    std::vector<int32_t> rp((size_t)n + 1);
+    const cudaMemcpyKind k = cudaMemcpyDeviceToHost;
+    if (on_device) CK(cudaMemcpy(rp.data(), rowptr, sizeof(int32_t) * rp.size(), k), "copy rowptr");
+    else std::memcpy(rp.data(), rowptr, sizeof(int32_t) * rp.size());
+    const int64_t nz = rp[(size_t)n];
+    std::vector<int32_t> ci((size_t)nz);
+    std::vector<double> cv((size_t)nz), d((size_t)n);
+    if (on_device) {
+        CK(cudaMemcpy(ci.data(), colind, sizeof(int32_t) * ci.size(), k), "copy colind");
+        CK(cudaMemcpy(cv.data(), val, sizeof(double) * cv.size(), k), "copy val");
+        CK(cudaMemcpy(d.data(), diag, sizeof(double) * d.size(), k), "copy diag");
+    } else {
+        std::memcpy(ci.data(), colind, sizeof(int32_t) * ci.size());
+        std::memcpy(cv.data(), val, sizeof(double) * cv.size());
+        std::memcpy(d.data(), diag, sizeof(double) * d.size());
+    }
+    // row r of L^T = column r of L; drop the unit diagonal, sort rows
+    std::vector<int64_t> cp((size_t)n + 1, 0);
+    std::vector<int32_t> ri;
+    std::vector<double> v;
+    ri.reserve((size_t)nz);
+    v.reserve((size_t)nz);
+    for (int32_t j = 0; j < n; ++j) {
+        std::vector<std::pair<int32_t, double>> col;
+        for (int32_t p = rp[(size_t)j]; p < rp[(size_t)j + 1]; ++p) {
+            if (ci[(size_t)p] < j) return fail(ctx, RCHOL_ERR_INVALID, "factor is not upper triangular");
+            if (ci[(size_t)p] == j) continue;
+            col.emplace_back(ci[(size_t)p], cv[(size_t)p]);
+        }
+        std::sort(col.begin(), col.end());
+        for (auto& e : col) {
+            ri.push_back(e.first);
+            v.push_back(e.second);
+        }
+        cp[(size_t)j + 1] = (int64_t)ri.size();
+    }
+    return factor_from_host_csc(ctx, n, cp, ri, v, d, out);
+}
+
+extern "C" void rchol_factor_free(rchol_factor_t* f) {
+    if (!f) return;
+    rchol_ctx* ctx = f->ctx;
+    if (ctx) {
+        cudaSetDevice(ctx->device);
+        if (ctx->solver_f == f) drop_solver(ctx);
+    }
+    free_factor(f->F);
+    delete f;
+}
+
+// ===========================================================================
+// solve
+// ===========================================================================
+
+namespace {
+
+bool valid_k(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32; }
+
+rchol_status get_solver(rchol_ctx* ctx, const rchol_factor_t* f, int k) {
+    const rchol_opts& o = ctx->o;
+    const int fp32 = o.precision == RCHOL_PREC_FP32_FACTOR;
+    if (ctx->solver && ctx->solver_f == f && ctx->solver_k == k && ctx->solver_fp32 == fp32 &&
+        ctx->solver_stop == o.stop_rule && ctx->solver_maxit == o.max_iter && ctx->solver_tol == o.tol)
+        return RCHOL_OK;
+    drop_solver(ctx);
+    rchol::SolveConfig cfg;
+    cfg.k = k;
+    cfg.fp32_factor = fp32 != 0;
+    cfg.tol = o.tol;
+    cfg.max_iter = o.max_iter;
+    cfg.stop_rule = o.stop_rule;
+    cfg.unroll = o.unroll;
+    cfg.use_graph = o.use_graph != 0;
+    cfg.timeout_s = o.timeout_s;
+    if (cfg.fp32_factor && !f->F.lr_val32)
+        return fail(ctx, RCHOL_ERR_INVALID, "factor has no FP32 copy (factor with RCHOL_PREC_FP32_FACTOR)");
+    cudaError_t e = cudaSuccess;
+    ctx->solver = rchol::pcg_create(ctx->At, f->F, cfg, ctx->device, ctx->stream, &e);
+    if (!ctx->solver) return cuda_fail(ctx, e, "create solver");
+    ctx->solver_f = f;
+    ctx->solver_k = k;
+    ctx->solver_fp32 = fp32;
+    ctx->solver_stop = o.stop_rule;
+    ctx->solver_maxit = o.max_iter;
+    ctx->solver_tol = o.tol;
+    return RCHOL_OK;
+}
+
+// Bring a column-major block (host or device) into the row-major staging buffer.
+rchol_status stage_in(rchol_ctx* ctx, const double* B, int ldb, int k, int on_device, double* dst) {
+    const int32_t n = ctx->At.n;
+    if (k == 1 && on_device) {
+        CK(cudaMemcpyAsync(dst, B, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream), "copy rhs");
+        return RCHOL_OK;
+    }
+    if (on_device) {
+        CK(rchol::cm_to_rm(B, ldb, dst, n, k, ctx->stream), "layout");
+        return RCHOL_OK;
+    }
+    // host: upload column by column into the X staging (as column-major), then transpose
+    double* tmp = dst == ctx->dB ? ctx->dX : ctx->dB;
+    for (int c = 0; c < k; ++c)
+        CK(cudaMemcpyAsync(tmp + (size_t)c * n, B + (size_t)c * ldb, sizeof(double) * (size_t)n,
+                           cudaMemcpyHostToDevice, ctx->stream),
+           "upload rhs");
+    if (k == 1) {
+        CK(cudaMemcpyAsync(dst, tmp, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+    } else {
+        CK(rchol::cm_to_rm(tmp, n, dst, n, k, ctx->stream), "layout");
+    }
+    return RCHOL_OK;
+}
+
+rchol_status stage_out(rchol_ctx* ctx, const double* src, double* X, int ldb, int k, int on_device) {
+    const int32_t n = ctx->At.n;
+    if (on_device) {
+        if (k == 1) CK(cudaMemcpyAsync(X, src, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+        else CK(rchol::rm_to_cm(src, X, ldb, n, k, ctx->stream), "layout");
+        return RCHOL_OK;
+    }
+    const double* cm = src;
+    if (k > 1) {
+        double* tmp = src == ctx->dX ? ctx->dB : ctx->dX;
+        CK(rchol::rm_to_cm(src, tmp, n, n, k, ctx->stream), "layout");
+        cm = tmp;
+    }
+    for (int c = 0; c < k; ++c)
+        CK(cudaMemcpyAsync(X + (size_t)c * ldb, cm + (size_t)c * n, sizeof(double) * (size_t)n,
+                           cudaMemcpyDeviceToHost, ctx->stream),
+           "download solution");
+    return RCHOL_OK;
+}
+
+}  // namespace
+
+extern "C" rchol_status rchol_pcg_solve(rchol_ctx* ctx, const rchol_factor_t* f, int k, const double* B, double* X,
+                                        int ldb, int on_device, rchol_solve_info* info) {
+    if (!ctx || !f || !B || !X) return fail(ctx, RCHOL_ERR_INVALID, "null argument");
+    if (!ctx->have) return fail(ctx, RCHOL_ERR_NO_MATRIX, "no matrix loaded");
+    if (!valid_k(k)) return fail(ctx, RCHOL_ERR_INVALID, "k must be 1, 2, 4, 8, 16 or 32");
+    if (f->F.n != ctx->At.n) return fail(ctx, RCHOL_ERR_INVALID, "factor and matrix sizes differ");
+    if (ldb < ctx->At.n) return fail(ctx, RCHOL_ERR_INVALID, "ldb < n");
+    cudaSetDevice(ctx->device);
+    rchol_status s = get_solver(ctx, f, k);
+    if (s != RCHOL_OK) return s;
+    s = ensure_stage(ctx, (size_t)ctx->At.n * (size_t)k);
+    if (s != RCHOL_OK) return s;
+    s = stage_in(ctx, B, ldb, k, on_device, ctx->dB);
+    if (s != RCHOL_OK) return s;
+    rchol::SolveResult r;
+    cudaError_t e = rchol::pcg_solve(ctx->solver, ctx->dB, ctx->dX, &r);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "pcg");
+    s = stage_out(ctx, ctx->dX, X, ldb, k, on_device);
+    if (s != RCHOL_OK) return s;
+    CK(cudaStreamSynchronize(ctx->stream), "sync solve");
+    if (info) {
+        info->iterations = r.iterations;
+        info->converged = r.converged;
+        info->device_status = r.status;
+        info->relres_true = r.relres_true;
+        info->relres_rec = r.relres_rec;
+        info->precond_ratio = r.precond_ratio;
+        info->ms_total = r.ms_total;
+        info->ms_iterations = r.ms_iterations;
+        info->kernel_launches = r.kernel_launches;
+        info->graph_launches = r.graph_launches;
+    }
+    if (r.status == rchol::kDevTimeout) return fail(ctx, RCHOL_ERR_TIMEOUT, "pcg: a device wait timed out");
+    if (!r.converged) return fail(ctx, RCHOL_ERR_NOT_CONVERGED, "pcg did not reach the tolerance");
+    return RCHOL_OK;
+}
+
+extern "C" rchol_status rchol_precond_apply(rchol_ctx* ctx, const rchol_factor_t* f, int k, const double* R,
+                                            double* Z, int ldb, int on_device, int fp32) {
+    if (!ctx || !f || !R || !Z) return fail(ctx, RCHOL_ERR_INVALID, "null argument");
+    if (!valid_k(k)) return fail(ctx, RCHOL_ERR_INVALID, "k must be 1, 2, 4, 8, 16 or 32");
+    if (ldb < f->F.n) return fail(ctx, RCHOL_ERR_INVALID, "ldb < n");
+    if (fp32 && !f->F.lr_val32) return fail(ctx, RCHOL_ERR_INVALID, "factor has no FP32 copy");
+    if (!ctx->have || ctx->At.n != f->F.n) return fail(ctx, RCHOL_ERR_INVALID, "factor does not match the matrix");
+    cudaSetDevice(ctx->device);
+    const size_t elems = (size_t)f->F.n * (size_t)k;
+    rchol_status s = ensure_stage(ctx, 2 * elems);
+    if (s != RCHOL_OK) return s;
+    s = stage_in(ctx, R, ldb, k, on_device, ctx->dB);
+    if (s != RCHOL_OK) return s;
+    int status = 0;
+    // ctx->dX holds z, its second half the y work vector
+    CK(rchol::precond_apply(f->F, ctx->dB, ctx->dX, ctx->dX + elems, k, fp32 != 0, &status, ctx->o.timeout_s,
+                            ctx->stream),
+       "precond apply");
+    if (status != 0) return fail(ctx, RCHOL_ERR_TIMEOUT, "precond apply: a device wait timed out");
+    s = stage_out(ctx, ctx->dX, Z, ldb, k, on_device);
+    if (s != RCHOL_OK) return s;
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    return RCHOL_OK;
+}
+
+extern "C" rchol_status rchol_spmv(rchol_ctx* ctx, int k, const double* X, double* Y, int ldb, int on_device) {
+    if (!ctx || !X || !Y) return fail(ctx, RCHOL_ERR_INVALID, "null argument");
+    if (!ctx->have) return fail(ctx, RCHOL_ERR_NO_MATRIX, "no matrix loaded");
+    if (!valid_k(k)) return fail(ctx, RCHOL_ERR_INVALID, "k must be 1, 2, 4, 8, 16 or 32");
+    if (ldb < ctx->At.n) return fail(ctx, RCHOL_ERR_INVALID, "ldb < n");
+    cudaSetDevice(ctx->device);
+    const size_t elems = (size_t)ctx->At.n * (size_t)k;
+    rchol_status s = ensure_stage(ctx, elems);
+    if (s != RCHOL_OK) return s;
+    s = stage_in(ctx, X, ldb, k, on_device, ctx->dB);
+    if (s != RCHOL_OK) return s;
+    CK(rchol::spmv_f64(ctx->At, ctx->dB, ctx->dX, k, ctx->stream), "spmv");
+    s = stage_out(ctx, ctx->dX, Y, ldb, k, on_device);
+    if (s != RCHOL_OK) return s;
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    return RCHOL_OK;
+}
+
+// ===========================================================================
+// reference drop-ins
+// ===========================================================================
+
+namespace {
+
+// generate_zero_sum_vector (solver.hpp:43-61): libstdc++'s std::mt19937 and
+// uniform_real_distribution, as the reference.
+void zero_sum_rhs(std::vector<double>& b, size_t n, unsigned long seed) {
+    std::mt19937 gen(seed);
+    std::uniform_real_distribution<double> dist(0.0, 1.0);
+    double sum = 0.0;
+    b.resize(n);
+    for (size_t i = 0; i < n; ++i) {
+        b[i] = dist(gen);
+        sum += b[i];
+    }
+    double mean = sum / (double)n;
+    for (size_t i = 0; i < n; ++i) b[i] -= mean;
+}
+
+// generate_random_vector (solver.hpp:29-41): U(-1,1), seed 0
+void random_vec(std::vector<double>& v, size_t n, unsigned long seed) {
+    std::mt19937 gen(seed);
+    std::uniform_real_distribution<double> dist(-1.0, 1.0);
+    v.resize(n);
+    for (size_t i = 0; i < n; ++i) v[i] = dist(gen);
+}
+
+}  // namespace
+
+extern "C" rchol_status rchol_factorization_driver(const char* path, int num_blocks, int check_solve, double tol,
+                                                   int physics) {
+    rchol_opts o;
+    rchol_opts_default(&o);
+    o.num_blocks = num_blocks;
+    o.tol = tol;
+    o.stop_rule = RCHOL_STOP_PRECOND;
+    o.max_iter = 300;
+    o.verbose = 1;
+    rchol_ctx* ctx = nullptr;
+    rchol_status s = rchol_create(&ctx, &o);
+    if (s != RCHOL_OK) {
+        std::fprintf(stderr, "rchol: %s\n", rchol_status_string(s));
+        return s;
+    }
+    std::printf("problem: %s\n", path);
+    auto t0 = std::chrono::high_resolution_clock::now();
+    s = rchol_load_mtx(ctx, path, physics);
+    if (s != RCHOL_OK) {
+        std::fprintf(stderr, "rchol: %s: %s\n", rchol_status_string(s), rchol_last_error(ctx));
+        rchol_destroy(ctx);
+        return s;
+    }
+    auto t1 = std::chrono::high_resolution_clock::now();
+    std::printf("number of nodes: %d\nnumber of nonzeros: %lld\n", ctx->A.n, (long long)ctx->A.nnz);
+    std::printf("initial preprocessing time (read, sort, upload; not part of the algorithm): %lld milliseconds\n",
+                (long long)std::chrono::duration_cast<std::chrono::milliseconds>(t1 - t0).count());
+    rchol_factor_t* f = nullptr;
+    s = rchol_factor(ctx, &f);
+    if (s != RCHOL_OK) {
+        std::fprintf(stderr, "rchol: %s: %s\n", rchol_status_string(s), rchol_last_error(ctx));
+        rchol_destroy(ctx);
+        return s;
+    }
+    std::printf("Kernel execution time: %f ms\n", f->info.ms_factor);
+    std::printf("total conversion time: %f milliseconds\n", f->info.ms_assemble + f->info.ms_setup);
+    std::printf("nnz ratio: %f, factor nnz: %lld, original lower triangular nnz (exclude diagonal): %lld\n",
+                (double)(f->info.nnz_strict + f->info.n) / (double)std::max<long long>(1, f->info.nnz_lower_a),
+                f->info.nnz_strict + f->info.n, f->info.nnz_lower_a);
+    if (check_solve) {
+        const int32_t n = ctx->At.n;
+        std::vector<double> b, x((size_t)n, 0.0);
+        zero_sum_rhs(b, (size_t)n, 0);
+        rchol_solve_info si;
+        s = rchol_pcg_solve(ctx, f, 1, b.data(), x.data(), n, 0, &si);
+        std::printf("final iteration: %d, residual: %e\n", si.iterations, si.precond_ratio);
+        std::printf("pcg time: %f ms\n", si.ms_total);
+        std::printf("normalized diff norm: %.16f\n", si.relres_true);
+        if (s == RCHOL_ERR_NOT_CONVERGED) s = RCHOL_OK;  // the reference reports and exits normally
+    }
+    rchol_factor_free(f);
+    rchol_destroy(ctx);
+    return s;
+}
+
+extern "C" rchol_status rchol_prepare_and_solve(int lap_n, long long lap_nnz, const int* lap_rowptr,
+                                                const int* lap_colind, const double* lap_val, const int* csr_rowptr,
+                                                const double* csr_val, const int* csr_colind, const double* diag,
+                                                double tol, int physics, long long factor_nnz, int removal, double* X,
+                                                rchol_solve_info* info) {
+    (void)factor_nnz;
+    (void)removal;  // unused by the reference as well (solver.hpp:236-593)
+    if (lap_n <= 0 || !lap_rowptr || !lap_colind || !lap_val || !csr_rowptr || !csr_val || !csr_colind || !diag)
+        return RCHOL_ERR_INVALID;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    rchol_opts o;
+    rchol_opts_default(&o);
+    o.device = dev;
+    o.tol = tol;
+    o.stop_rule = RCHOL_STOP_PRECOND;
+    o.max_iter = 300;
+    rchol_ctx* ctx = nullptr;
+    rchol_status s = rchol_create(&ctx, &o);
+    if (s != RCHOL_OK) return s;
+    (void)lap_nnz;
+    s = rchol_set_csc(ctx, lap_n, lap_rowptr, lap_colind, lap_val, 1, 0);
+    rchol_factor_t* f = nullptr;
+    if (s == RCHOL_OK) s = rchol_factor_from_csr_upper(ctx, lap_n, csr_rowptr, csr_colind, csr_val, diag, 1, &f);
+    std::vector<double> b;
+    if (s == RCHOL_OK) {
+        if (physics) {
+            zero_sum_rhs(b, (size_t)lap_n, 0);
+        } else {
+            std::vector<double> v;
+            random_vec(v, (size_t)lap_n, 0);
+            b.resize((size_t)lap_n);
+            s = rchol_spmv(ctx, 1, v.data(), b.data(), lap_n, 0);
+        }
+    }
+    if (s == RCHOL_OK) {
+        std::vector<double> x((size_t)lap_n, 0.0);
+        rchol_solve_info si;
+        s = rchol_pcg_solve(ctx, f, 1, b.data(), x.data(), lap_n, 0, &si);
+        if (info) *info = si;
+        if (X) cudaMemcpy(X, x.data(), sizeof(double) * (size_t)lap_n, cudaMemcpyHostToDevice);
+        if (s == RCHOL_ERR_NOT_CONVERGED) s = RCHOL_OK;
+    }
+    if (f) rchol_factor_free(f);
+    rchol_destroy(ctx);
+    return s;
+}
+
+// ===========================================================================
+// synthetic inputs
+// ===========================================================================
+
+extern "C" rchol_status rchol_generate(const char* kind, const long long* dims, int ndims, double wlo, double whi,
+                                       int log_weights, double aniso_z, double excess_frac, double excess_lo,
+                                       double excess_hi, int ordering, unsigned long long seed, int* n_out,
+                                       long long* nnz_out, int** rows, int** cols, double** vals, int* has_ground) {
+    if (!kind || !dims || ndims <= 0 || !n_out || !nnz_out || !rows || !cols || !vals) return RCHOL_ERR_INVALID;
+    rchol::GenSpec sp;
+    sp.kind = kind;
+    sp.dims.assign(dims, dims + ndims);
+    sp.wlo = wlo;
+    sp.whi = whi;
+    sp.log_weights = log_weights != 0;
+    sp.aniso_z = aniso_z;
+    sp.excess_frac = excess_frac;
+    sp.excess_lo = excess_lo;
+    sp.excess_hi = excess_hi;
+    sp.ordering = ordering;
+    sp.seed = seed;
+    rchol::Triplets t;
+    bool g = false;
+    std::string err;
+    if (!rchol::generate(sp, t, g, err)) {
+        std::fprintf(stderr, "rchol_generate: %s\n", err.c_str());
+        return RCHOL_ERR_INVALID;
+    }
+    const size_t nz = t.rows.size();
+    *rows = (int*)std::malloc(sizeof(int) * std::max<size_t>(nz, 1));
+    *cols = (int*)std::malloc(sizeof(int) * std::max<size_t>(nz, 1));
+    *vals = (double*)std::malloc(sizeof(double) * std::max<size_t>(nz, 1));
+    if (!*rows || !*cols || !*vals) return RCHOL_ERR_INVALID;
+    std::memcpy(*rows, t.rows.data(), sizeof(int) * nz);
+    std::memcpy(*cols, t.cols.data(), sizeof(int) * nz);
+    std::memcpy(*vals, t.vals.data(), sizeof(double) * nz);
+    *n_out = t.n;
+    *nnz_out = (long long)nz;
+    if (has_ground) *has_ground = g ? 1 : 0;
+    return RCHOL_OK;
+}
+
+extern "C" void rchol_free_host(void* p) { std::free(p); }
+
+extern "C" rchol_status rchol_csc_from_triplets(int n, long long nnz, const int* rows, const int* cols,
+                                                const double* vals, int* colptr, int* rowind, double* val,
+                                                long long* nnz_out) {
+    if (n <= 0 || nnz < 0 || (nnz > 0 && (!rows || !cols || !vals)) || !nnz_out) return RCHOL_ERR_INVALID;
+    rchol::Triplets t;
+    t.n = n;
+    t.rows.assign(rows, rows + nnz);
+    t.cols.assign(cols, cols + nnz);
+    t.vals.assign(vals, vals + nnz);
+    rchol::HostCsc h;
+    std::string err;
+    if (!rchol::triplets_to_csc(t, h, err)) return err.find("finite") != std::string::npos ? RCHOL_ERR_NUMERIC
+                                                                                          : RCHOL_ERR_INVALID;
+    *nnz_out = (long long)h.rowind.size();
+    if (colptr) {
+        if (!rowind || !val) return RCHOL_ERR_INVALID;
+        std::memcpy(colptr, h.colptr.data(), sizeof(int) * h.colptr.size());
+        std::memcpy(rowind, h.rowind.data(), sizeof(int) * h.rowind.size());
+        std::memcpy(val, h.val.data(), sizeof(double) * h.val.size());
+    }
+    return RCHOL_OK;
+}
+
+extern "C" rchol_status rchol_read_mtx(const char* path, int* n, long long* nnz, int** rows, int** cols,
+                                       double** vals) {
+    if (!path || !n || !nnz || !rows || !cols || !vals) return RCHOL_ERR_INVALID;
+    rchol::Triplets t;
+    std::string err;
+    if (!rchol::read_mtx(path, t, err)) return RCHOL_ERR_IO;
+    const size_t nz = t.rows.size();
+    *rows = (int*)std::malloc(sizeof(int) * std::max<size_t>(nz, 1));
+    *cols = (int*)std::malloc(sizeof(int) * std::max<size_t>(nz, 1));
+    *vals = (double*)std::malloc(sizeof(double) * std::max<size_t>(nz, 1));
+    if (!*rows || !*cols || !*vals) return RCHOL_ERR_INVALID;
+    std::memcpy(*rows, t.rows.data(), sizeof(int) * nz);
+    std::memcpy(*cols, t.cols.data(), sizeof(int) * nz);
+    std::memcpy(*vals, t.vals.data(), sizeof(double) * nz);
+    *n = t.n;
+    *nnz = (long long)nz;
+    return RCHOL_OK;
+}
+
+extern "C" rchol_status rchol_write_mtx(const char* path, int n, long long nnz, const int* rows, const int* cols,
+                                        const double* vals) {
+    if (!path || n <= 0 || nnz < 0) return RCHOL_ERR_INVALID;
+    std::string err;
+    if (!rchol::write_mtx(path, n, nnz, rows, cols, vals, err)) return RCHOL_ERR_IO;
+    return RCHOL_OK;
+}

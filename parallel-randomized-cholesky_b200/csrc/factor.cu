@@ -1,0 +1,561 @@
+// Randomized-Cholesky elimination of a graph Laplacian on sm_100a.
+//
+// Restates the algorithm of gpu_implementation/driver.cu:43-1302 and
+// cpu_implementation/driver_local.cpp:302-707 with a B200-first design:
+//   * one persistent launch sized to the resident capacity; every warp pulls
+//     ready vertices from a global FIFO (driver.cu:142-234) and releases its
+//     neighbours through per-vertex dependency counters with acquire/release
+//     atomics (driver.cu:1179-1202 used relaxed atomics and never re-read);
+//   * the neighbour merge is a warp bitonic sort + segmented sum staged in a
+//     shared-memory slab (a per-warp global slab for large vertices);
+//   * sampling uniforms come from Philox4x32-10 keyed by (seed, vertex,
+//     slot), so the factor does not depend on which warp took which vertex;
+//   * fill edges are appended to per-column buckets by atomics (driver.cu
+//     used an open-addressing hash over 4*nnz slots, :1068-1150): a fixed
+//     first chunk per column plus 64-entry overflow chunks linked lock-free.
+// FP64 arithmetic uses explicitly rounded intrinsics (no contraction), which
+// makes the factor bit-identical to the CPU oracle's ORC_MODE_B200.
+#include <climits>
+#include <cstdio>
+
+#include "device_common.cuh"
+#include "rchol_internal.h"
+
+namespace rchol {
+
+namespace {
+
+constexpr int kChunk = 64;                 // overflow chunk entries
+constexpr int kPoolGrab = 1024;            // L-pool entries grabbed per warp at once
+constexpr unsigned long long kInfBits = 0x7ff0000000000000ull;
+constexpr int kSlabBytesPerEntry = 32;     // 8 (a_val) + 8 (b_val) + 8 (b_aux) + 4 + 4
+
+enum Counter { kQHead = 0, kQTail = 1, kChunkCursor = 2, kStatus = 3, kAbort = 4, kBigCount = 5,
+               kMaxGather = 6, kOverflowFills = 7 };
+
+__device__ __forceinline__ int pow2_at_least(int x) {
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+// One warp's staging area: a_* hold the gathered entries and, after the
+// value sort, the prefix sums; b_* hold the merged neighbours.
+struct Slab {
+    double* a_val;
+    int32_t* a_row;
+    double* b_val;
+    int32_t* b_row;
+    long long* b_aux;  // (multiplicity << 32) | row-order position
+};
+
+__device__ __forceinline__ Slab make_slab(unsigned char* base, int cap) {
+    Slab s;
+    s.a_val = reinterpret_cast<double*>(base);
+    s.b_val = s.a_val + cap;
+    s.b_aux = reinterpret_cast<long long*>(s.b_val + cap);
+    s.a_row = reinterpret_cast<int32_t*>(s.b_aux + cap);
+    s.b_row = s.a_row + cap;
+    return s;
+}
+
+// ---- bitonic sorts over slab arrays (P a power of two) -------------------
+
+// ascending by (row, value bits)
+__device__ void sort_row_value(int32_t* row, double* val, int P, int lane) {
+    for (int k = 2; k <= P; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < P; i += kWarp) {
+                int l = i ^ j;
+                if (l > i) {
+                    int32_t ri = row[i], rl = row[l];
+                    unsigned long long vi = (unsigned long long)__double_as_longlong(val[i]);
+                    unsigned long long vl = (unsigned long long)__double_as_longlong(val[l]);
+                    bool gt = (ri > rl) || (ri == rl && vi > vl);
+                    bool asc = (i & k) == 0;
+                    if (gt == asc) {
+                        row[i] = rl;
+                        row[l] = ri;
+                        val[i] = __longlong_as_double((long long)vl);
+                        val[l] = __longlong_as_double((long long)vi);
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// ascending by (value, row) carrying aux
+__device__ void sort_value_row(double* val, int32_t* row, long long* aux, int P, int lane) {
+    for (int k = 2; k <= P; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < P; i += kWarp) {
+                int l = i ^ j;
+                if (l > i) {
+                    double vi = val[i], vl = val[l];
+                    int32_t ri = row[i], rl = row[l];
+                    bool gt = (vi > vl) || (vi == vl && ri > rl);
+                    bool asc = (i & k) == 0;
+                    if (gt == asc) {
+                        val[i] = vl;
+                        val[l] = vi;
+                        row[i] = rl;
+                        row[l] = ri;
+                        long long ai = aux[i];
+                        aux[i] = aux[l];
+                        aux[l] = ai;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+struct FactorArgs {
+    int32_t n;
+    const int32_t* __restrict__ lcolptr;
+    const int32_t* __restrict__ lrow;
+    const double* __restrict__ lval;
+    int32_t* dep;
+    int32_t* queue;
+    int32_t c0;
+    int32_t* fcnt;
+    int32_t* brow;
+    double* bval;
+    int32_t* chead;
+    int32_t* cnext;
+    int32_t* crow;
+    double* cval;
+    int32_t nchunks;
+    int64_t pool_cap;
+    int32_t* prow;
+    double* pval;
+    int64_t* pstart;
+    int32_t* pcnt;
+    double* diag;
+    unsigned char* gscratch;
+    int64_t gscratch_entries;
+    int32_t* counters;
+    unsigned long long* pool_cursor;
+    uint64_t seed;
+    int smem_slab;
+    unsigned long long timeout_ns;
+};
+
+__device__ __forceinline__ bool aborted(const FactorArgs& a) { return ld_relaxed(a.counters + kAbort) != 0; }
+
+__device__ __forceinline__ void fail(const FactorArgs& a, int code) {
+    raise_error(a.counters + kStatus, code);
+    atomicExch(a.counters + kAbort, 1);
+}
+
+// Append one fill edge (row > col) to column col's bucket.  Returns false on
+// pool exhaustion.  Chunks are linked with CAS, so no thread ever waits.
+__device__ bool append_fill(const FactorArgs& a, int32_t col, int32_t row, double v) {
+    int s = atomicAdd(a.fcnt + col, 1);
+    if (s < a.c0) {
+        size_t o = (size_t)col * (size_t)a.c0 + (size_t)s;
+        a.brow[o] = row;
+        a.bval[o] = v;
+        return true;
+    }
+    atomicAdd(a.counters + kOverflowFills, 1);
+    int t = s - a.c0;
+    int ci = t / kChunk, off = t % kChunk;
+    int32_t* link = a.chead + col;
+    int cur = -1;
+    for (int lvl = 0;; ++lvl) {
+        cur = ld_relaxed(link);
+        if (cur < 0) {
+            int nc = atomicAdd(a.counters + kChunkCursor, 1);
+            if (nc >= a.nchunks) return false;
+            int old = atomicCAS(link, -1, nc);
+            cur = (old == -1) ? nc : old;
+        }
+        if (lvl == ci) break;
+        link = a.cnext + cur;
+    }
+    size_t o = (size_t)cur * kChunk + (size_t)off;
+    a.crow[o] = row;
+    a.cval[o] = v;
+    return true;
+}
+
+__device__ __forceinline__ void push_ready(const FactorArgs& a, int32_t r) {
+    int t = atomicAdd(a.counters + kQTail, 1);
+    if (t < a.n) st_release(a.queue + t, r);
+    else fail(a, kDevBadInput);
+}
+
+// Eliminate vertex k with one warp.  Returns false if the kernel must stop.
+__device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_global, int lane,
+                          int64_t& pool_cur, int64_t& pool_end, long long& fills) {
+    const int nf = ld_relaxed(a.fcnt + k);
+    const int o0 = a.lcolptr[k];
+    const int no = a.lcolptr[k + 1] - o0;
+    const int total = nf + no;
+    if (total == 0) {  // driver_local.cpp:470-477: empty column, D = 0
+        if (lane == 0) {
+            a.diag[k] = 0.0;
+            a.pcnt[k] = 0;
+            a.pstart[k] = 0;
+        }
+        return true;
+    }
+    Slab s = sm;
+    if (total > a.smem_slab) {
+        if ((int64_t)total > a.gscratch_entries) {
+            if (lane == 0) fail(a, kDevCapacity);
+            return false;
+        }
+        s = make_slab(a.gscratch + (size_t)warp_global * (size_t)a.gscratch_entries * kSlabBytesPerEntry,
+                      (int)a.gscratch_entries);
+        if (lane == 0) atomicAdd(a.counters + kBigCount, 1);
+    }
+    if (lane == 0) atomicMax(a.counters + kMaxGather, total);
+    const int P = pow2_at_least(total);
+
+    // ---- gather: fills (first chunk, then overflow chunks), original column
+    const int n0 = min(nf, a.c0);
+    for (int t = lane; t < n0; t += kWarp) {
+        size_t o = (size_t)k * (size_t)a.c0 + (size_t)t;
+        s.a_row[t] = __ldcg(a.brow + o);
+        s.a_val[t] = __ldcg(a.bval + o);
+    }
+    int rem = nf - n0, pos = n0;
+    int chunk = rem > 0 ? ld_relaxed(a.chead + k) : -1;
+    while (rem > 0) {
+        if (chunk < 0 || chunk >= a.nchunks) {
+            if (lane == 0) fail(a, kDevBadInput);
+            return false;
+        }
+        int cnt = min(rem, kChunk);
+        for (int t = lane; t < cnt; t += kWarp) {
+            s.a_row[pos + t] = __ldcg(a.crow + (size_t)chunk * kChunk + t);
+            s.a_val[pos + t] = __ldcg(a.cval + (size_t)chunk * kChunk + t);
+        }
+        pos += cnt;
+        rem -= cnt;
+        if (rem > 0) chunk = ld_relaxed(a.cnext + chunk);
+    }
+    for (int t = lane; t < no; t += kWarp) {
+        s.a_row[nf + t] = a.lrow[o0 + t];
+        s.a_val[nf + t] = a.lval[o0 + t];
+    }
+    for (int t = total + lane; t < P; t += kWarp) {
+        s.a_row[t] = INT_MAX;
+        s.a_val[t] = __longlong_as_double((long long)kInfBits);
+    }
+    __syncwarp();
+
+    // ---- sort by row and merge duplicates (driver_local.cpp:511-568)
+    sort_row_value(s.a_row, s.a_val, P, lane);
+    int m = 0;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    for (int base = 0; base < total; base += kWarp) {
+        int i = base + lane;
+        bool valid = i < total;
+        int32_t ri = valid ? s.a_row[i] : INT_MAX;
+        bool head = valid && (i == 0 || s.a_row[i - 1] != ri);
+        unsigned bal = __ballot_sync(kFull, head);
+        if (head) {
+            int rank = m + __popc(bal & lt_mask);
+            double acc = s.a_val[i];
+            int cnt = 1;
+            for (int j = i + 1; j < total && s.a_row[j] == ri; ++j) {
+                acc = __dadd_rn(acc, s.a_val[j]);
+                ++cnt;
+            }
+            s.b_val[rank] = acc;
+            s.b_row[rank] = ri;
+            s.b_aux[rank] = ((long long)cnt << 32) | (long long)rank;
+        }
+        m += __popc(bal);
+    }
+    const int P2 = pow2_at_least(m);
+    for (int t = m + lane; t < P2; t += kWarp) {
+        s.b_val[t] = __longlong_as_double((long long)kInfBits);
+        s.b_row[t] = INT_MAX;
+        s.b_aux[t] = 0;
+    }
+    __syncwarp();
+
+    // ---- sort by value, chunked prefix sum (driver_local.cpp:573-593)
+    sort_value_row(s.b_val, s.b_row, s.b_aux, P2, lane);
+    double carry = 0.0;
+    for (int c0 = 0; c0 < m; c0 += kWarp) {
+        double v = (c0 + lane < m) ? s.b_val[c0 + lane] : 0.0;
+#pragma unroll
+        for (int off = 1; off < kWarp; off <<= 1) {
+            double t = __shfl_up_sync(kFull, v, off);
+            if (lane >= off) v = __dadd_rn(v, t);
+        }
+        double f = (c0 == 0) ? v : __dadd_rn(carry, v);
+        if (c0 + lane < m) s.a_val[c0 + lane] = f;
+        carry = __shfl_sync(kFull, f, kWarp - 1);
+    }
+    __syncwarp();
+    const double S = s.a_val[m - 1];
+
+    // ---- L column k into the pool (row order), D_k
+    if (pool_end - pool_cur < m) {
+        int64_t grab = m > kPoolGrab ? (int64_t)m : (int64_t)kPoolGrab;
+        unsigned long long got = 0;
+        if (lane == 0) got = atomicAdd(a.pool_cursor, (unsigned long long)grab);
+        got = __shfl_sync(kFull, got, 0);
+        if ((int64_t)got + grab > a.pool_cap) {
+            if (lane == 0) fail(a, kDevCapacity);
+            return false;
+        }
+        pool_cur = (int64_t)got;
+        pool_end = (int64_t)got + grab;
+    }
+    const int64_t pbase = pool_cur;
+    pool_cur += m;
+    fills += m - 1;
+    if (lane == 0) {
+        a.diag[k] = S;
+        a.pstart[k] = pbase;
+        a.pcnt[k] = m;
+    }
+    for (int i = lane; i < m; i += kWarp) {
+        int p = (int)(s.b_aux[i] & 0xffffffffll);
+        a.prow[pbase + p] = s.b_row[i];
+        a.pval[pbase + p] = __ddiv_rn(s.b_val[i], S);
+    }
+
+    // ---- clique sampling (driver_local.cpp:598-631, auxilliary.hpp:543-592)
+    bool ok = true;
+    for (int i = lane; i < m - 1; i += kWarp) {
+        const double ci = s.a_val[i];
+        const double rem_i = __dsub_rn(S, ci);
+        const double target = __dmul_rn(sample_uniform(a.seed, k, i), rem_i);
+        int lo = i + 1, hi = m;
+        while (lo < hi) {
+            int mid = lo + ((hi - lo) >> 1);
+            if (__dsub_rn(s.a_val[mid], ci) < target) lo = mid + 1;
+            else hi = mid;
+        }
+        const int j = lo < m ? lo : m - 1;
+        const int32_t r_i = s.b_row[i], r_j = s.b_row[j];
+        const int32_t grow = r_i > r_j ? r_i : r_j;
+        const int32_t gcol = r_i > r_j ? r_j : r_i;
+        const double gval = __ddiv_rn(__dmul_rn(s.b_val[i], rem_i), S);
+        if (!append_fill(a, gcol, grow, gval)) ok = false;
+        atomicAdd(a.dep + grow, 1);
+    }
+    if (__any_sync(kFull, !ok)) {
+        if (lane == 0) fail(a, kDevCapacity);
+        return false;
+    }
+    // fills and pool writes must be visible before any neighbour is released
+    __threadfence();
+    __syncwarp();
+    for (int i = lane; i < m; i += kWarp) {
+        const int mult = (int)(s.b_aux[i] >> 32);
+        const int32_t r = s.b_row[i];
+        const int old = atom_add_acq_rel(a.dep + r, -mult);
+        if (old == mult) push_ready(a, r);
+    }
+    __syncwarp();
+    return true;
+}
+
+__global__ void __launch_bounds__(256) factor_kernel(FactorArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & (kWarp - 1);
+    const int wib = threadIdx.x >> 5;
+    const int warp_global = blockIdx.x * (blockDim.x >> 5) + wib;
+    Slab sm = make_slab(smem + (size_t)wib * (size_t)a.smem_slab * kSlabBytesPerEntry, a.smem_slab);
+    const unsigned long long t0 = global_timer_ns();
+    int64_t pool_cur = 0, pool_end = 0;
+    long long fills = 0;
+    while (true) {
+        int idx = 0;
+        if (lane == 0) idx = atomicAdd(a.counters + kQHead, 1);
+        idx = __shfl_sync(kFull, idx, 0);
+        if (idx >= a.n) break;
+        int k = -1;
+        if (lane == 0) {
+            unsigned spins = 0;
+            while ((k = ld_acquire(a.queue + idx)) < 0) {
+                if ((++spins & 255u) == 0) {
+                    if (aborted(a)) break;
+                    if (global_timer_ns() - t0 > a.timeout_ns) {
+                        fail(a, kDevTimeout);
+                        break;
+                    }
+                }
+            }
+        }
+        k = __shfl_sync(kFull, k, 0);
+        if (k < 0) break;
+        __threadfence();
+        if (!eliminate(a, k, sm, warp_global, lane, pool_cur, pool_end, fills)) break;
+        if (aborted(a)) break;
+    }
+    if (lane == 0 && fills) atomicAdd(a.pool_cursor + 1, (unsigned long long)fills);
+}
+
+// ---- setup kernels --------------------------------------------------------
+
+// Per column: entries below the diagonal (lower_cnt) and above it (dep,
+// count_minimum_dependencies, pre_process.hpp:474-496).  One warp/column.
+__global__ void count_lower_kernel(int32_t n, const int32_t* __restrict__ colptr,
+                                   const int32_t* __restrict__ rowind, int32_t* lower_cnt, int32_t* dep) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < n; c += warps) {
+        int lo = 0, up = 0;
+        for (int p = colptr[c] + lane; p < colptr[c + 1]; p += 32) {
+            int r = rowind[p];
+            lo += r > c;
+            up += r < c;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo += __shfl_xor_sync(kFull, lo, o);
+            up += __shfl_xor_sync(kFull, up, o);
+        }
+        if (lane == 0) {
+            lower_cnt[c] = lo;
+            if (dep) dep[c] = up;
+        }
+    }
+}
+
+// Strict lower triangle with |values|, original order within each column
+// (make_lower_triangular, pre_process.hpp:785-867).
+__global__ void scatter_lower_kernel(int32_t n, const int32_t* __restrict__ colptr,
+                                     const int32_t* __restrict__ rowind, const double* __restrict__ val,
+                                     const int32_t* __restrict__ lcolptr, int32_t* lrow, double* lval) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < n; c += warps) {
+        int out = lcolptr[c];
+        for (int base = colptr[c]; base < colptr[c + 1]; base += 32) {
+            int p = base + lane;
+            bool take = p < colptr[c + 1] && rowind[p] > c;
+            unsigned bal = __ballot_sync(kFull, take);
+            if (take) {
+                int o = out + __popc(bal & ((1u << lane) - 1u));
+                lrow[o] = rowind[p];
+                lval[o] = fabs(val[p]);
+            }
+            out += __popc(bal);
+        }
+    }
+}
+
+__global__ void init_queue_kernel(int32_t n, const int32_t* __restrict__ dep, int32_t* queue,
+                                  int32_t* counters) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+        int64_t i = base + threadIdx.x;
+        bool ready = i < n && dep[i] == 0;
+        unsigned bal = __ballot_sync(kFull, ready);
+        int lane = threadIdx.x & 31;
+        int pos = 0;
+        if (lane == 0 && bal) pos = atomicAdd(counters + kQTail, __popc(bal));
+        pos = __shfl_sync(kFull, pos, 0);
+        if (ready) queue[pos + __popc(bal & ((1u << lane) - 1u))] = (int32_t)i;
+    }
+}
+
+int grid_for(int64_t work, int block) {
+    int64_t g = ceil_div(work, block);
+    if (g < 1) g = 1;
+    if (g > 148 * 32) g = 148 * 32;
+    return (int)g;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+
+cudaError_t launch_count_lower(const DevCsc& A, int32_t* lower_cnt, cudaStream_t s) {
+    count_lower_kernel<<<grid_for((int64_t)A.n * 32, 256), 256, 0, s>>>(A.n, A.colptr, A.rowind, lower_cnt,
+                                                                         nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lower_and_deps(const DevCsc& A, FactorWork& w, cudaStream_t s) {
+    // lower counts go to w.pcnt (scratch), dependency counts to w.dep
+    count_lower_kernel<<<grid_for((int64_t)A.n * 32, 256), 256, 0, s>>>(A.n, A.colptr, A.rowind, w.pcnt,
+                                                                         w.dep);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = exclusive_scan_i32_to_i32(w.pcnt, w.lcolptr, A.n, w.scan_tmp, s);
+    if (e != cudaSuccess) return e;
+    scatter_lower_kernel<<<grid_for((int64_t)A.n * 32, 256), 256, 0, s>>>(A.n, A.colptr, A.rowind, A.val,
+                                                                           w.lcolptr, w.lrow, w.lval);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init_factor_state(FactorWork& w, cudaStream_t s) {
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(w.fcnt, 0, sizeof(int32_t) * (size_t)w.n, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(w.chead, 0xff, sizeof(int32_t) * (size_t)w.n, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(w.cnext, 0xff, sizeof(int32_t) * (size_t)w.nchunks, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(w.queue, 0xff, sizeof(int32_t) * (size_t)w.n, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(w.counters, 0, sizeof(int32_t) * 16, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(w.counters64, 0, sizeof(unsigned long long) * 4, s)) != cudaSuccess) return e;
+    init_queue_kernel<<<grid_for(w.n, 256), 256, 0, s>>>(w.n, w.dep, w.queue, w.counters);
+    return cudaGetLastError();
+}
+
+size_t factor_smem_bytes(int block, int smem_slab) {
+    return (size_t)(block / kWarp) * (size_t)smem_slab * kSlabBytesPerEntry;
+}
+
+int factor_resident_grid(int block, int smem_slab, int device) {
+    size_t smem = factor_smem_bytes(block, smem_slab);
+    cudaFuncSetAttribute(factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, factor_kernel, block, smem) != cudaSuccess)
+        return 0;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return per_sm * sms;
+}
+
+cudaError_t launch_factor(FactorWork& w, const FactorLaunch& cfg, cudaStream_t s) {
+    FactorArgs a;
+    a.n = w.n;
+    a.lcolptr = w.lcolptr;
+    a.lrow = w.lrow;
+    a.lval = w.lval;
+    a.dep = w.dep;
+    a.queue = w.queue;
+    a.c0 = w.c0;
+    a.fcnt = w.fcnt;
+    a.brow = w.brow;
+    a.bval = w.bval;
+    a.chead = w.chead;
+    a.cnext = w.cnext;
+    a.crow = w.crow;
+    a.cval = w.cval;
+    a.nchunks = w.nchunks;
+    a.pool_cap = w.pool_cap;
+    a.prow = w.prow;
+    a.pval = w.pval;
+    a.pstart = w.pstart;
+    a.pcnt = w.pcnt;
+    a.diag = w.diag;
+    a.gscratch = w.gscratch;
+    a.gscratch_entries = w.gscratch_entries;
+    a.counters = w.counters;
+    a.pool_cursor = w.counters64;
+    a.seed = cfg.seed;
+    a.smem_slab = cfg.smem_slab;
+    a.timeout_ns = (unsigned long long)(cfg.timeout_s * 1e9);
+    size_t smem = factor_smem_bytes(cfg.block, cfg.smem_slab);
+    cudaError_t e = cudaFuncSetAttribute(factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    factor_kernel<<<cfg.grid, cfg.block, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace rchol

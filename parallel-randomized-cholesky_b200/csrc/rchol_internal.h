@@ -1,0 +1,163 @@
+// Internal declarations shared by the CUDA translation units and the host
+// C-ABI layer.  Nothing here is part of the public interface (include/rchol.h).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rchol {
+
+// Error codes written to the device status word (first writer wins).
+enum DeviceError : int {
+    kDevOk = 0,
+    kDevTimeout = 1,       // a bounded wait gave up
+    kDevCapacity = 2,      // a preallocated pool was too small
+    kDevBadInput = 3,      // an invariant of the input did not hold
+};
+
+// ---------------------------------------------------------------------------
+// Matrix in HBM: the full symmetric Laplacian/SDDM in CSC, which is also its
+// CSR (A = A^T).  int32 indices, FP64 values.
+// ---------------------------------------------------------------------------
+struct DevCsc {
+    int32_t n = 0;
+    int64_t nnz = 0;
+    int32_t* colptr = nullptr;  // [n+1]
+    int32_t* rowind = nullptr;  // [nnz]
+    double* val = nullptr;      // [nnz]
+};
+
+// Working state of one factorization (all device pointers).
+struct FactorWork {
+    int32_t n = 0;
+    // strict lower triangle of A, |a_ij|, CSC
+    int32_t* lcolptr = nullptr;
+    int32_t* lrow = nullptr;
+    double* lval = nullptr;
+    int64_t lnnz = 0;
+    // dependency counters and ready queue (queue[i] = -1 until written)
+    int32_t* dep = nullptr;
+    int32_t* queue = nullptr;
+    // per-column fill buckets: a first chunk of `c0` slots per column, then
+    // 64-slot overflow chunks linked per column
+    int32_t c0 = 32;
+    int32_t* fcnt = nullptr;      // [n] fills appended to each column
+    int32_t* brow = nullptr;      // [n*c0]
+    double* bval = nullptr;       // [n*c0]
+    int32_t* chead = nullptr;     // [n] first overflow chunk of each column (-1)
+    int32_t* cnext = nullptr;     // [nchunks] next chunk (-1)
+    int32_t* crow = nullptr;      // [nchunks*64]
+    double* cval = nullptr;       // [nchunks*64]
+    int32_t nchunks = 0;
+    // L pool: each eliminated column appends its merged neighbours
+    int64_t pool_cap = 0;
+    int32_t* prow = nullptr;      // [pool_cap]
+    double* pval = nullptr;       // [pool_cap]  (w / sum, positive)
+    int64_t* pstart = nullptr;    // [n] column start in the pool
+    int32_t* pcnt = nullptr;      // [n] merged neighbour count
+    double* diag = nullptr;       // [n] D
+    // per-warp scratch for vertices that do not fit the shared-memory slab
+    int64_t gscratch_entries = 0; // entries per warp
+    unsigned char* gscratch = nullptr;
+    // counters: [0] queue head, [1] queue tail, [2] chunk cursor, [3] status,
+    // [4] abort, [5] big-vertex count, [6] max gather, [7] overflow fills;
+    // pool cursor is int64 in counters64[0]
+    int32_t* counters = nullptr;
+    unsigned long long* counters64 = nullptr;
+    void* scan_tmp = nullptr;     // scan_tmp_bytes(n)
+};
+
+// The assembled factor, trimmed when the input carried a ground vertex.
+//   Lc: strict CSC of L  (column j: rows i > j, values L_ij < 0)
+//   Lr: strict CSR of L  (row i: columns j < i), the transpose of Lc
+struct DevFactor {
+    int32_t n = 0;            // size of the factor used by the solve
+    int64_t nnz = 0;          // strict entries
+    int64_t* lc_ptr = nullptr;
+    int32_t* lc_idx = nullptr;
+    double* lc_val = nullptr;
+    float* lc_val32 = nullptr;
+    int64_t* lr_ptr = nullptr;
+    int32_t* lr_idx = nullptr;
+    double* lr_val = nullptr;
+    float* lr_val32 = nullptr;
+    double* diag = nullptr;
+    float* diag32 = nullptr;
+};
+
+struct FactorLaunch {
+    int grid = 0;
+    int block = 256;
+    int smem_slab = 256;      // entries per warp slab in shared memory
+    uint64_t seed = 1;
+    double timeout_s = 20.0;
+};
+
+// ---- setup / factor / assembly (factor.cu) --------------------------------
+cudaError_t launch_lower_and_deps(const DevCsc& A, FactorWork& w, cudaStream_t s);
+cudaError_t launch_count_lower(const DevCsc& A, int32_t* lower_cnt, cudaStream_t s);
+cudaError_t launch_init_factor_state(FactorWork& w, cudaStream_t s);
+cudaError_t launch_factor(FactorWork& w, const FactorLaunch& cfg, cudaStream_t s);
+int factor_resident_grid(int block, int smem_slab, int device);
+size_t factor_smem_bytes(int block, int smem_slab);
+
+// Assemble Lc/Lr (and FP32 copies) from the pool; drop the last vertex when
+// trim_ground is set.  The device arrays of `f` are allocated here.
+cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp32, DevFactor& f,
+                            cudaStream_t s);
+// Drop the last row/column of A (ground vertex) into a new DevCsc.
+cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, cudaStream_t s);
+
+// ---- scans (scan.cu) -------------------------------------------------------
+// out[0] = 0, out[i+1] = sum(in[0..i]); out has n+1 entries.  Uses `tmp`
+// scratch of scan_tmp_bytes(n).
+size_t scan_tmp_bytes(int64_t n);
+cudaError_t exclusive_scan_i32_to_i64(const int32_t* in, int64_t* out, int64_t n, void* tmp,
+                                      cudaStream_t s);
+cudaError_t exclusive_scan_i32_to_i32(const int32_t* in, int32_t* out, int64_t n, void* tmp,
+                                      cudaStream_t s);
+
+// ---- PCG (solve.cu) --------------------------------------------------------
+struct PcgScalars;  // device-resident scalars, defined in solve.cu
+
+struct SolveConfig {
+    int k = 1;                 // right-hand sides in the block
+    bool fp32_factor = false;  // read L and D as FP32
+    double tol = 1e-6;
+    int max_iter = 1000;
+    int stop_rule = 0;         // 0 relres (true residual), 1 precond ratio, 2 abs r^2
+    int unroll = 4;            // iterations per captured graph launch
+    bool use_graph = true;
+    double timeout_s = 20.0;
+};
+
+struct SolveResult {
+    int iterations = 0;
+    int converged = 0;
+    int status = 0;            // device status word
+    double relres_true = 0;    // max over RHS
+    double relres_rec = 0;
+    double precond_ratio = 0;
+    float ms_total = 0;
+    float ms_iterations = 0;
+    int graph_launches = 0;
+    int kernel_launches = 0;
+};
+
+// Solves A X = B for k columns stored row-major (n x k, ldx = k) in device
+// memory; X is overwritten.  `A` and `F` must have the same n.
+class PcgSolver;
+PcgSolver* pcg_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cfg, int device,
+                      cudaStream_t stream, cudaError_t* err);
+cudaError_t pcg_solve(PcgSolver* s, const double* dB, double* dX, SolveResult* res);
+void pcg_destroy(PcgSolver* s);
+
+// Kernel-level entry points used by tests/bench (one operator application).
+cudaError_t spmv_f64(const DevCsc& A, const double* x, double* y, int k, cudaStream_t s);
+// Layout changes between column-major (ld >= n) and row-major n x k blocks.
+cudaError_t cm_to_rm(const double* cm, int ld, double* rm, int32_t n, int k, cudaStream_t s);
+cudaError_t rm_to_cm(const double* rm, double* cm, int ld, int32_t n, int k, cudaStream_t s);
+cudaError_t precond_apply(const DevFactor& F, const double* r, double* z, double* ywork, int k,
+                          bool fp32, int* status, double timeout_s, cudaStream_t s);
+
+}  // namespace rchol

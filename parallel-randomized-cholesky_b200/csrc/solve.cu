@@ -1,0 +1,987 @@
+// Preconditioned conjugate gradient with the randomized-Cholesky
+// preconditioner M = L D L^T on sm_100a (gpu_implementation/solver.hpp:150-593,
+// experiment/custom_cg.hpp:65-265), for a block of k independent right-hand
+// sides stored row-major (n x k) so that every factor and matrix entry is
+// read once per block.
+//
+// One iteration is three kernels, captured into a CUDA graph:
+//   spmv_update  q = A z + beta q,  p = z + beta p,  (p.q) -> alpha
+//                (A p computed as A z + beta A p_old: no separate p pass)
+//   fwd          x += alpha p, r -= alpha q, (r.r); y = L^-1 r   sync-free
+//   bwd          z = L^-T D^+ y, (r.z) -> beta, stop test        sync-free
+// The triangular solves are persistent kernels over the resident grid: each
+// row group waits for the rows it depends on by polling their values, which
+// start as a "pending" NaN bit pattern (no separate ready flags, no level
+// sets, no analysis phase).  Every wait is bounded by a wall-clock limit and
+// reports kDevTimeout instead of hanging.  Reductions write per-block
+// partials and the last block sums them in block order (deterministic).
+#include <cmath>
+#include <cstdio>
+#include <algorithm>
+#include <cstring>
+#include <type_traits>
+#include <vector>
+
+#include "device_common.cuh"
+#include "rchol_internal.h"
+
+namespace rchol {
+
+constexpr int kMaxK = 32;
+
+struct PcgScalars {
+    double alpha[kMaxK];
+    double beta[kMaxK];
+    double rz[kMaxK];
+    double rz0[kMaxK];
+    double rr[kMaxK];
+    double pq[kMaxK];
+    double bnorm2[kMaxK];
+    double tr2[kMaxK];       // ||b - A x||^2 from the true-residual kernel
+    int active[kMaxK];
+    int iters[kMaxK];
+    int done;                // 1: stop iterating (all converged, max iters, error)
+    int iter;                // completed iterations
+    int phase;               // 0: the next bwd pass initialises rz (start/restart)
+    int status;              // device error code
+    unsigned ticket[4];
+};
+
+namespace {
+
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ double pending_value() { return __longlong_as_double((long long)kPendingBits); }
+__device__ __forceinline__ bool is_pending(double v) {
+    return (unsigned long long)__double_as_longlong(v) == kPendingBits;
+}
+
+template <typename TV>
+__device__ __forceinline__ double to_d(TV v) {
+    return (double)v;
+}
+
+struct SolveArgs {
+    int32_t n;
+    // A (CSR == CSC, symmetric)
+    const int32_t* __restrict__ a_ptr;
+    const int32_t* __restrict__ a_idx;
+    const double* __restrict__ a_val;
+    // factor
+    const int64_t* __restrict__ lr_ptr;
+    const int32_t* __restrict__ lr_idx;
+    const void* __restrict__ lr_val;
+    const int64_t* __restrict__ lc_ptr;
+    const int32_t* __restrict__ lc_idx;
+    const void* __restrict__ lc_val;
+    const void* __restrict__ diag;
+    // vectors (n x K row-major)
+    const double* __restrict__ b;
+    double* x;
+    double* r;
+    double* p;
+    double* q;
+    double* y;
+    double* z;
+    // reductions
+    double* part;            // [3][grid_max][K]
+    int grid_max;
+    PcgScalars* sc;
+    // control
+    double tol;
+    int max_iter;
+    int stop_rule;
+    int update;              // fwd: apply the x/r update
+    int reduce;              // compute reductions / scalars
+    unsigned long long timeout_ns;
+};
+
+// Block-wide sum of one double per (thread, column) slot: `v` holds the
+// thread's partial for column (threadIdx.x % K) when K > 1 layouts are
+// column-interleaved; here each thread carries K partials in registers.
+template <int K>
+__device__ void block_partials(const double (&v)[K], double* out_block /* [K] */) {
+    __shared__ double red[kBlock / 32][K];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < K; ++c) {
+        double s = v[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+        if (lane == 0) red[w][c] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double s = 0.0;
+        for (int i = 0; i < kBlock / 32; ++i) s += red[i][threadIdx.x];
+        out_block[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+// Returns true in exactly one thread of the last block to finish; that block
+// then reduces the partials.  `ticket` is reset for the next use.
+__device__ __forceinline__ bool last_block(unsigned* ticket) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned t = atomicAdd(ticket, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (is_last) {
+        __threadfence();
+        return true;
+    }
+    return false;
+}
+
+template <int K>
+__device__ void sum_partials(const double* part, int nblocks, double* out) {
+    // threads < K each sum one column in block order
+    if (threadIdx.x < K) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; ++b) s += part[(size_t)b * K + threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ bool timed_out(unsigned long long t0, unsigned long long limit) {
+    return global_timer_ns() - t0 > limit;
+}
+
+// Poll a solution component until it has been produced.
+__device__ __forceinline__ double wait_value(const double* p, unsigned long long t0, unsigned long long limit,
+                                             int* status, bool& ok) {
+    double v = ld_relaxed_f64(p);
+    if (!is_pending(v)) return v;
+    unsigned spins = 0;
+    while (true) {
+        v = ld_relaxed_f64(p);
+        if (!is_pending(v)) return v;
+        if ((++spins & 1023u) == 0 && timed_out(t0, limit)) {
+            raise_error(status, kDevTimeout);
+            ok = false;
+            return 0.0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// init: x = 0, r = b, p = q = 0, y = pending; ||b||^2
+// ---------------------------------------------------------------------------
+template <int K>
+__global__ void __launch_bounds__(kBlock) init_kernel(SolveArgs a) {
+    double acc[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    const int64_t total = (int64_t)a.n * K;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        double bv = a.b[t];
+        a.x[t] = 0.0;
+        a.r[t] = bv;
+        a.p[t] = 0.0;
+        a.q[t] = 0.0;
+        a.y[t] = pending_value();
+        int c = (int)(t % K);
+#pragma unroll
+        for (int cc = 0; cc < K; ++cc)
+            if (cc == c) acc[cc] += bv * bv;
+    }
+    block_partials<K>(acc, a.part + (size_t)blockIdx.x * K);
+    if (last_block(&a.sc->ticket[0])) {
+        sum_partials<K>(a.part, gridDim.x, a.sc->bnorm2);
+        if (threadIdx.x < K) {
+            int c = threadIdx.x;
+            a.sc->alpha[c] = 0.0;
+            a.sc->beta[c] = 0.0;
+            a.sc->rz[c] = 0.0;
+            a.sc->active[c] = a.sc->bnorm2[c] > 0.0 ? 1 : 0;
+            a.sc->iters[c] = 0;
+        }
+        if (threadIdx.x == 0) {
+            a.sc->ticket[0] = 0;
+            a.sc->iter = 0;
+            a.sc->phase = 0;
+            a.sc->status = 0;
+            int any = 0;
+            for (int c = 0; c < K; ++c) any |= a.sc->bnorm2[c] > 0.0;
+            a.sc->done = any ? 0 : 1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// spmv_update: s = A z; q = s + beta q; p = z + beta p; (p.q); y = pending
+// ---------------------------------------------------------------------------
+template <int K>
+__global__ void __launch_bounds__(kBlock) spmv_update_kernel(SolveArgs a) {
+    if (ld_relaxed(&a.sc->done)) return;
+    constexpr int G = (K == 1) ? 8 : K;           // lanes per row
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % G;
+    const int64_t group = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const int64_t ngroups = (int64_t)gridDim.x * blockDim.x / G;
+    double acc[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    double beta[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) beta[c] = a.sc->beta[c];
+    const unsigned gmask = (G == 32) ? kFull : (((1u << G) - 1u) << ((lane / G) * G));
+    for (int64_t i = group; i < a.n; i += ngroups) {
+        const int s = a.a_ptr[i], e = a.a_ptr[i + 1];
+        if (K == 1) {
+            double sum = 0.0;
+            for (int pp = s + gl; pp < e; pp += G) sum += a.a_val[pp] * a.z[a.a_idx[pp]];
+#pragma unroll
+            for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(gmask, sum, o, G);
+            if (gl == 0) {
+                double qi = sum + beta[0] * a.q[i];
+                double pi = a.z[i] + beta[0] * a.p[i];
+                a.q[i] = qi;
+                a.p[i] = pi;
+                a.y[i] = pending_value();
+                acc[0] += pi * qi;
+            }
+        } else {
+            const int c = gl;  // G == K
+            double sum = 0.0;
+            for (int pp = s; pp < e; ++pp) sum += a.a_val[pp] * a.z[(size_t)a.a_idx[pp] * K + c];
+            size_t o = (size_t)i * K + c;
+            double qi = sum + beta[c] * a.q[o];
+            double pi = a.z[o] + beta[c] * a.p[o];
+            a.q[o] = qi;
+            a.p[o] = pi;
+            a.y[o] = pending_value();
+#pragma unroll
+            for (int cc = 0; cc < K; ++cc)
+                if (cc == c) acc[cc] += pi * qi;
+        }
+    }
+    block_partials<K>(acc, a.part + (size_t)blockIdx.x * K);
+    if (last_block(&a.sc->ticket[1])) {
+        sum_partials<K>(a.part, gridDim.x, a.sc->pq);
+        if (threadIdx.x < K) {
+            int c = threadIdx.x;
+            double pq = a.sc->pq[c];
+            a.sc->alpha[c] = (a.sc->active[c] && pq != 0.0) ? a.sc->rz[c] / pq : 0.0;
+        }
+        if (threadIdx.x == 0) a.sc->ticket[1] = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// fwd: x += alpha p; r -= alpha q; (r.r); y = L^{-1} r  (rows ascending)
+// ---------------------------------------------------------------------------
+template <int K, typename TV>
+__global__ void __launch_bounds__(kBlock) fwd_kernel(SolveArgs a) {
+    if (a.reduce && ld_relaxed(&a.sc->done)) return;
+    constexpr int G = (K == 1) ? 8 : K;
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % G;
+    const int64_t group = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const int64_t ngroups = (int64_t)gridDim.x * blockDim.x / G;
+    const unsigned gmask = (G == 32) ? kFull : (((1u << G) - 1u) << ((lane / G) * G));
+    const TV* __restrict__ lv = reinterpret_cast<const TV*>(a.lr_val);
+    double alpha[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) alpha[c] = a.update ? a.sc->alpha[c] : 0.0;
+    double acc[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    const unsigned long long t0 = global_timer_ns();
+    bool ok = true;
+    for (int64_t i = group; i < a.n && ok; i += ngroups) {
+        const int64_t s = a.lr_ptr[i], e = a.lr_ptr[i + 1];
+        if (K == 1) {
+            double ri = a.r[i];
+            if (a.update) {
+                double xi = a.x[i] + alpha[0] * a.p[i];
+                ri = ri - alpha[0] * a.q[i];
+                if (gl == 0) {
+                    a.x[i] = xi;
+                    a.r[i] = ri;
+                    acc[0] += ri * ri;
+                }
+            }
+            double sum = 0.0;
+            for (int64_t pp = s + gl; pp < e; pp += G) {
+                const double l = to_d(lv[pp]);
+                const double yj = wait_value(a.y + a.lr_idx[pp], t0, a.timeout_ns, &a.sc->status, ok);
+                sum += l * yj;
+            }
+#pragma unroll
+            for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(gmask, sum, o, G);
+            if (gl == 0) {
+                if (a.z) a.z[i] = pending_value();
+                st_relaxed_f64(a.y + i, ri - sum);
+            }
+        } else {
+            const int c = gl;
+            const size_t o = (size_t)i * K + c;
+            double ri = a.r[o];
+            if (a.update) {
+                double xi = a.x[o] + alpha[c] * a.p[o];
+                ri = ri - alpha[c] * a.q[o];
+                a.x[o] = xi;
+                a.r[o] = ri;
+#pragma unroll
+                for (int cc = 0; cc < K; ++cc)
+                    if (cc == c) acc[cc] += ri * ri;
+            }
+            double sum = 0.0;
+            for (int64_t pp = s; pp < e; ++pp) {
+                const double l = to_d(lv[pp]);
+                const double yj =
+                    wait_value(a.y + (size_t)a.lr_idx[pp] * K + c, t0, a.timeout_ns, &a.sc->status, ok);
+                sum += l * yj;
+            }
+            if (a.z) a.z[o] = pending_value();
+            st_relaxed_f64(a.y + o, ri - sum);
+        }
+    }
+    // a timed-out wait abandons the pass (block-uniform decision)
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) a.sc->done = 1;
+        return;
+    }
+    if (!a.reduce) return;
+    block_partials<K>(acc, a.part + (size_t)(a.grid_max + blockIdx.x) * K);
+    if (last_block(&a.sc->ticket[2])) {
+        if (a.update) {
+            sum_partials<K>(a.part + (size_t)a.grid_max * K, gridDim.x, a.sc->rr);
+            if (threadIdx.x == 0) {
+                const int it = a.sc->iter + 1;
+                a.sc->iter = it;
+                int any = 0;
+                for (int c = 0; c < K; ++c) {
+                    if (!a.sc->active[c]) continue;
+                    bool conv = false;
+                    if (a.stop_rule == 0) conv = sqrt(a.sc->rr[c]) <= a.tol * sqrt(a.sc->bnorm2[c]);
+                    else if (a.stop_rule == 2) conv = a.sc->rr[c] <= a.tol;
+                    if (conv) {
+                        a.sc->active[c] = 0;
+                        a.sc->iters[c] = it;
+                    } else {
+                        a.sc->iters[c] = it;
+                        any = 1;
+                    }
+                }
+                if (!any || it >= a.max_iter) a.sc->done = 1;
+            }
+        }
+        if (threadIdx.x == 0) a.sc->ticket[2] = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// bwd: z = L^{-T} D^+ y  (rows descending); (r.z) -> rz, beta
+// ---------------------------------------------------------------------------
+template <int K, typename TV>
+__global__ void __launch_bounds__(kBlock) bwd_kernel(SolveArgs a) {
+    if (a.reduce && ld_relaxed(&a.sc->done)) return;
+    constexpr int G = (K == 1) ? 8 : K;
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % G;
+    const int64_t group = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const int64_t ngroups = (int64_t)gridDim.x * blockDim.x / G;
+    const unsigned gmask = (G == 32) ? kFull : (((1u << G) - 1u) << ((lane / G) * G));
+    const TV* __restrict__ lv = reinterpret_cast<const TV*>(a.lc_val);
+    const TV* __restrict__ dv = reinterpret_cast<const TV*>(a.diag);
+    double acc[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    const unsigned long long t0 = global_timer_ns();
+    bool ok = true;
+    for (int64_t g = group; g < a.n && ok; g += ngroups) {
+        const int64_t j = a.n - 1 - g;
+        const int64_t s = a.lc_ptr[j], e = a.lc_ptr[j + 1];
+        const double dj = to_d(dv[j]);
+        if (K == 1) {
+            double t = a.y[j];
+            if (dj != 0.0) t = t / dj;
+            double sum = 0.0;
+            for (int64_t pp = s + gl; pp < e; pp += G) {
+                const double l = to_d(lv[pp]);
+                const double zi = wait_value(a.z + a.lc_idx[pp], t0, a.timeout_ns, &a.sc->status, ok);
+                sum += l * zi;
+            }
+#pragma unroll
+            for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(gmask, sum, o, G);
+            if (gl == 0) {
+                const double zj = t - sum;
+                st_relaxed_f64(a.z + j, zj);
+                acc[0] += a.r[j] * zj;
+            }
+        } else {
+            const int c = gl;
+            const size_t o = (size_t)j * K + c;
+            double t = a.y[o];
+            if (dj != 0.0) t = t / dj;
+            double sum = 0.0;
+            for (int64_t pp = s; pp < e; ++pp) {
+                const double l = to_d(lv[pp]);
+                const double zi =
+                    wait_value(a.z + (size_t)a.lc_idx[pp] * K + c, t0, a.timeout_ns, &a.sc->status, ok);
+                sum += l * zi;
+            }
+            const double zj = t - sum;
+            st_relaxed_f64(a.z + o, zj);
+#pragma unroll
+            for (int cc = 0; cc < K; ++cc)
+                if (cc == c) acc[cc] += a.r[o] * zj;
+        }
+    }
+    // a timed-out wait abandons the pass (block-uniform decision)
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) a.sc->done = 1;
+        return;
+    }
+    if (!a.reduce) return;
+    block_partials<K>(acc, a.part + (size_t)(2 * a.grid_max + blockIdx.x) * K);
+    if (last_block(&a.sc->ticket[3])) {
+        double* rzn = a.sc->pq;  // reuse pq storage for the new r.z (pq is consumed)
+        sum_partials<K>(a.part + (size_t)2 * a.grid_max * K, gridDim.x, rzn);
+        if (threadIdx.x == 0) {
+            const bool init = a.sc->phase == 0;
+            int any = 0;
+            for (int c = 0; c < K; ++c) {
+                const double rn = rzn[c];
+                if (init) {
+                    if (a.sc->active[c]) {
+                        a.sc->rz[c] = rn;
+                        a.sc->rz0[c] = rn;
+                        a.sc->beta[c] = 0.0;
+                    }
+                } else if (a.sc->active[c]) {
+                    const double ro = a.sc->rz[c];
+                    a.sc->beta[c] = ro != 0.0 ? rn / ro : 0.0;
+                    a.sc->rz[c] = rn;
+                    if (a.stop_rule == 1) {
+                        const double r0 = a.sc->rz0[c];
+                        if (!(sqrt(rn) / sqrt(r0) > a.tol)) a.sc->active[c] = 0;
+                    }
+                } else {
+                    a.sc->beta[c] = 0.0;
+                }
+                any |= a.sc->active[c];
+            }
+            if (init && a.stop_rule == 1) {
+                for (int c = 0; c < K; ++c)
+                    if (a.sc->active[c] && !(a.sc->rz[c] > a.tol)) a.sc->active[c] = 0;
+                any = 0;
+                for (int c = 0; c < K; ++c) any |= a.sc->active[c];
+            }
+            a.sc->phase = 1;
+            if (!any) a.sc->done = 1;
+            a.sc->ticket[3] = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// true residual: t = b - A x (written to r when `replace`), ||t||^2 -> tr2
+// ---------------------------------------------------------------------------
+template <int K>
+__global__ void __launch_bounds__(kBlock) true_residual_kernel(SolveArgs a, int replace, double* t_out) {
+    constexpr int G = (K == 1) ? 8 : K;
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % G;
+    const int64_t group = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const int64_t ngroups = (int64_t)gridDim.x * blockDim.x / G;
+    const unsigned gmask = (G == 32) ? kFull : (((1u << G) - 1u) << ((lane / G) * G));
+    double acc[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    for (int64_t i = group; i < a.n; i += ngroups) {
+        const int s = a.a_ptr[i], e = a.a_ptr[i + 1];
+        if (K == 1) {
+            double sum = 0.0;
+            for (int pp = s + gl; pp < e; pp += G) sum += a.a_val[pp] * a.x[a.a_idx[pp]];
+#pragma unroll
+            for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(gmask, sum, o, G);
+            if (gl == 0) {
+                double t = a.b[i] - sum;
+                if (t_out) t_out[i] = t;
+                if (replace) a.r[i] = t;
+                acc[0] += t * t;
+            }
+        } else {
+            const int c = gl;
+            double sum = 0.0;
+            for (int pp = s; pp < e; ++pp) sum += a.a_val[pp] * a.x[(size_t)a.a_idx[pp] * K + c];
+            size_t o = (size_t)i * K + c;
+            double t = a.b[o] - sum;
+            if (t_out) t_out[o] = t;
+            if (replace) a.r[o] = t;
+#pragma unroll
+            for (int cc = 0; cc < K; ++cc)
+                if (cc == c) acc[cc] += t * t;
+        }
+    }
+    block_partials<K>(acc, a.part + (size_t)blockIdx.x * K);
+    if (last_block(&a.sc->ticket[0])) {
+        sum_partials<K>(a.part, gridDim.x, a.sc->tr2);
+        if (threadIdx.x == 0) a.sc->ticket[0] = 0;
+    }
+}
+
+// restart of the columns that failed the true-residual test: p = q = 0,
+// y = pending, phase = 0 (the next fwd/bwd pair rebuilds z and rz)
+template <int K>
+__global__ void restart_kernel(SolveArgs a, const int* reactivate) {
+    const int64_t total = (int64_t)a.n * K;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        int c = (int)(t % K);
+        if (reactivate[c]) {
+            a.p[t] = 0.0;
+            a.q[t] = 0.0;
+        }
+        a.y[t] = pending_value();
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int c = 0; c < K; ++c) {
+            if (reactivate[c]) a.sc->active[c] = 1;
+            a.sc->alpha[c] = 0.0;
+        }
+        a.sc->phase = 0;
+        a.sc->done = 0;
+    }
+}
+
+__global__ void fill_pending_kernel(double* y, int64_t total) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) y[t] = pending_value();
+}
+
+__global__ void spmv_plain_kernel(int32_t n, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                  const double* __restrict__ val, const double* __restrict__ x, double* y, int K) {
+    const int64_t total = (int64_t)n * K;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        int64_t i = t / K;
+        int c = (int)(t % K);
+        double s = 0.0;
+        for (int p = ptr[i]; p < ptr[i + 1]; ++p) s += val[p] * x[(size_t)idx[p] * K + c];
+        y[t] = s;
+    }
+}
+
+// ---- launch plumbing ------------------------------------------------------
+
+template <int K, typename TV>
+struct Kernels {
+    static void* fwd() { return (void*)fwd_kernel<K, TV>; }
+    static void* bwd() { return (void*)bwd_kernel<K, TV>; }
+};
+
+int resident_blocks(const void* fn, int device) {
+    int per_sm = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return per_sm * sms;
+}
+
+}  // namespace
+
+// ===========================================================================
+
+class PcgSolver {
+   public:
+    DevCsc A;
+    DevFactor F;
+    SolveConfig cfg;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int K = 1;
+    double *r = nullptr, *p = nullptr, *q = nullptr, *y = nullptr, *z = nullptr;
+    double* part = nullptr;
+    int grid_max = 0;
+    int grid_spmv = 0, grid_fwd = 0, grid_bwd = 0, grid_vec = 0;
+    PcgScalars* sc = nullptr;
+    PcgScalars* sc_host = nullptr;  // pinned
+    int* react = nullptr;          // device [kMaxK]
+    cudaGraphExec_t graph_exec = nullptr;
+    const double* graph_b = nullptr;
+    double* graph_x = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+    void *k_init = nullptr, *k_spmv = nullptr, *k_fwd = nullptr, *k_bwd = nullptr, *k_true = nullptr,
+         *k_restart = nullptr;
+
+    SolveArgs args(const double* b, double* x) const {
+        SolveArgs a;
+        a.n = A.n;
+        a.a_ptr = A.colptr;
+        a.a_idx = A.rowind;
+        a.a_val = A.val;
+        a.lr_ptr = F.lr_ptr;
+        a.lr_idx = F.lr_idx;
+        a.lr_val = cfg.fp32_factor ? (const void*)F.lr_val32 : (const void*)F.lr_val;
+        a.lc_ptr = F.lc_ptr;
+        a.lc_idx = F.lc_idx;
+        a.lc_val = cfg.fp32_factor ? (const void*)F.lc_val32 : (const void*)F.lc_val;
+        a.diag = cfg.fp32_factor ? (const void*)F.diag32 : (const void*)F.diag;
+        a.b = b;
+        a.x = x;
+        a.r = r;
+        a.p = p;
+        a.q = q;
+        a.y = y;
+        a.z = z;
+        a.part = part;
+        a.grid_max = grid_max;
+        a.sc = sc;
+        a.tol = cfg.tol;
+        a.max_iter = cfg.max_iter;
+        a.stop_rule = cfg.stop_rule;
+        a.update = 1;
+        a.reduce = 1;
+        a.timeout_ns = (unsigned long long)(cfg.timeout_s * 1e9);
+        return a;
+    }
+
+    cudaError_t launch(void* fn, int grid, SolveArgs& a) {
+        void* params[] = {&a};
+        return cudaLaunchKernel(fn, dim3(grid), dim3(kBlock), params, 0, stream);
+    }
+
+    cudaError_t launch_iteration(const double* b, double* x) {
+        SolveArgs a = args(b, x);
+        cudaError_t e;
+        if ((e = launch(k_spmv, grid_spmv, a)) != cudaSuccess) return e;
+        if ((e = launch(k_fwd, grid_fwd, a)) != cudaSuccess) return e;
+        return launch(k_bwd, grid_bwd, a);
+    }
+
+    // fwd (no update) + bwd with phase 0: z = M r, rz = rz0 = r.z
+    cudaError_t launch_start(const double* b, double* x) {
+        SolveArgs a = args(b, x);
+        a.update = 0;
+        a.reduce = 1;
+        cudaError_t e;
+        // fwd with reduce=1 but update=0: no x/r change, no rr test
+        if ((e = launch(k_fwd, grid_fwd, a)) != cudaSuccess) return e;
+        return launch(k_bwd, grid_bwd, a);
+    }
+};
+
+template <int K, typename TV>
+static void bind_kernels(PcgSolver* s) {
+    s->k_init = (void*)init_kernel<K>;
+    s->k_spmv = (void*)spmv_update_kernel<K>;
+    s->k_fwd = (void*)fwd_kernel<K, TV>;
+    s->k_bwd = (void*)bwd_kernel<K, TV>;
+    s->k_true = (void*)true_residual_kernel<K>;
+    s->k_restart = (void*)restart_kernel<K>;
+}
+
+template <typename TV>
+static bool bind_for_k(PcgSolver* s, int K) {
+    switch (K) {
+        case 1: bind_kernels<1, TV>(s); return true;
+        case 2: bind_kernels<2, TV>(s); return true;
+        case 4: bind_kernels<4, TV>(s); return true;
+        case 8: bind_kernels<8, TV>(s); return true;
+        case 16: bind_kernels<16, TV>(s); return true;
+        case 32: bind_kernels<32, TV>(s); return true;
+        default: return false;
+    }
+}
+
+PcgSolver* pcg_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cfg, int device, cudaStream_t stream,
+                      cudaError_t* err) {
+    *err = cudaSuccess;
+    if (A.n != F.n) {
+        *err = cudaErrorInvalidValue;
+        return nullptr;
+    }
+    PcgSolver* s = new PcgSolver();
+    s->A = A;
+    s->F = F;
+    s->cfg = cfg;
+    s->device = device;
+    s->stream = stream;
+    s->K = cfg.k;
+    bool okk = cfg.fp32_factor ? bind_for_k<float>(s, cfg.k) : bind_for_k<double>(s, cfg.k);
+    if (!okk || (cfg.fp32_factor && !F.lr_val32)) {
+        delete s;
+        *err = cudaErrorInvalidValue;
+        return nullptr;
+    }
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    s->grid_fwd = resident_blocks(s->k_fwd, device);
+    s->grid_bwd = resident_blocks(s->k_bwd, device);
+    s->grid_spmv = sms * 8;
+    s->grid_vec = sms * 8;
+    s->grid_max = std::max(std::max(s->grid_fwd, s->grid_bwd), std::max(s->grid_spmv, s->grid_vec));
+    const size_t nv = (size_t)A.n * (size_t)cfg.k;
+    cudaError_t e = cudaSuccess;
+    e = cudaMalloc(&s->r, sizeof(double) * std::max<size_t>(nv, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&s->p, sizeof(double) * std::max<size_t>(nv, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&s->q, sizeof(double) * std::max<size_t>(nv, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&s->y, sizeof(double) * std::max<size_t>(nv, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&s->z, sizeof(double) * std::max<size_t>(nv, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&s->part, sizeof(double) * (size_t)3 * s->grid_max * cfg.k);
+    if (e == cudaSuccess) e = cudaMalloc(&s->sc, sizeof(PcgScalars));
+    if (e == cudaSuccess) e = cudaMemset(s->sc, 0, sizeof(PcgScalars));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->sc_host, sizeof(PcgScalars));
+    if (e == cudaSuccess) e = cudaMalloc(&s->react, sizeof(int) * kMaxK);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev1);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev2);
+    if (e != cudaSuccess || s->grid_fwd <= 0 || s->grid_bwd <= 0) {
+        *err = e != cudaSuccess ? e : cudaErrorLaunchOutOfResources;
+        pcg_destroy(s);
+        return nullptr;
+    }
+    return s;
+}
+
+void pcg_destroy(PcgSolver* s) {
+    if (!s) return;
+    if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+    cudaFree(s->r);
+    cudaFree(s->p);
+    cudaFree(s->q);
+    cudaFree(s->y);
+    cudaFree(s->z);
+    cudaFree(s->part);
+    cudaFree(s->sc);
+    cudaFree(s->react);
+    if (s->sc_host) cudaFreeHost(s->sc_host);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->ev2) cudaEventDestroy(s->ev2);
+    delete s;
+}
+
+static cudaError_t build_graph(PcgSolver* s, const double* b, double* x) {
+    if (s->graph_exec && s->graph_b == b && s->graph_x == x) return cudaSuccess;
+    if (s->graph_exec) {
+        cudaGraphExecDestroy(s->graph_exec);
+        s->graph_exec = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    for (int u = 0; u < s->cfg.unroll; ++u) {
+        e = s->launch_iteration(b, x);
+        if (e != cudaSuccess) break;
+    }
+    cudaError_t e2 = cudaStreamEndCapture(s->stream, &g);
+    if (e != cudaSuccess) return e;
+    if (e2 != cudaSuccess) return e2;
+    e = cudaGraphInstantiate(&s->graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    s->graph_b = b;
+    s->graph_x = x;
+    return e;
+}
+
+cudaError_t pcg_solve(PcgSolver* s, const double* dB, double* dX, SolveResult* res) {
+    *res = SolveResult();
+    const int K = s->K;
+    cudaError_t e;
+    if (s->cfg.use_graph && (e = build_graph(s, dB, dX)) != cudaSuccess) return e;
+    e = cudaEventRecord(s->ev0, s->stream);
+    if (e != cudaSuccess) return e;
+    SolveArgs a = s->args(dB, dX);
+    if ((e = s->launch(s->k_init, s->grid_vec, a)) != cudaSuccess) return e;
+    if ((e = s->launch_start(dB, dX)) != cudaSuccess) return e;
+    res->kernel_launches += 3;
+    if ((e = cudaEventRecord(s->ev1, s->stream)) != cudaSuccess) return e;
+    int restarts = 0;
+    while (true) {
+        // iterate until the device says stop
+        while (true) {
+            if (s->cfg.use_graph) {
+                if ((e = cudaGraphLaunch(s->graph_exec, s->stream)) != cudaSuccess) return e;
+                res->graph_launches++;
+                res->kernel_launches += 3 * s->cfg.unroll;
+            } else {
+                for (int u = 0; u < s->cfg.unroll; ++u)
+                    if ((e = s->launch_iteration(dB, dX)) != cudaSuccess) return e;
+                res->kernel_launches += 3 * s->cfg.unroll;
+            }
+            if ((e = cudaMemcpyAsync(s->sc_host, s->sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s->stream)) !=
+                cudaSuccess)
+                return e;
+            if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return e;
+            if (s->sc_host->done) break;
+        }
+        // confirm on the true residual b - A x
+        SolveArgs t = s->args(dB, dX);
+        void* params[] = {&t, nullptr, nullptr};
+        int replace = 0;
+        double* tout = nullptr;
+        params[1] = &replace;
+        params[2] = &tout;
+        if ((e = cudaLaunchKernel(s->k_true, dim3(s->grid_vec), dim3(kBlock), params, 0, s->stream)) != cudaSuccess)
+            return e;
+        res->kernel_launches++;
+        if ((e = cudaMemcpyAsync(s->sc_host, s->sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s->stream)) !=
+            cudaSuccess)
+            return e;
+        if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return e;
+        const PcgScalars& h = *s->sc_host;
+        if (h.status != 0 || s->cfg.stop_rule != 0 || h.iter >= s->cfg.max_iter || restarts >= 3) break;
+        int react[kMaxK] = {0};
+        int any = 0;
+        for (int c = 0; c < K; ++c) {
+            double bn = std::sqrt(h.bnorm2[c]);
+            if (bn > 0 && std::sqrt(h.tr2[c]) > s->cfg.tol * bn) {
+                react[c] = 1;
+                any = 1;
+            }
+        }
+        if (!any) break;
+        // residual replacement and restart for the failing columns
+        ++restarts;
+        replace = 1;
+        if ((e = cudaMemcpyAsync(s->react, react, sizeof(react), cudaMemcpyHostToDevice, s->stream)) != cudaSuccess)
+            return e;
+        if ((e = cudaLaunchKernel(s->k_true, dim3(s->grid_vec), dim3(kBlock), params, 0, s->stream)) != cudaSuccess)
+            return e;
+        SolveArgs ra = s->args(dB, dX);
+        void* rparams[] = {&ra, &s->react};
+        if ((e = cudaLaunchKernel(s->k_restart, dim3(s->grid_vec), dim3(kBlock), rparams, 0, s->stream)) !=
+            cudaSuccess)
+            return e;
+        if ((e = s->launch_start(dB, dX)) != cudaSuccess) return e;
+        res->kernel_launches += 4;
+    }
+    if ((e = cudaEventRecord(s->ev2, s->stream)) != cudaSuccess) return e;
+    if ((e = cudaEventSynchronize(s->ev2)) != cudaSuccess) return e;
+    cudaEventElapsedTime(&res->ms_total, s->ev0, s->ev2);
+    cudaEventElapsedTime(&res->ms_iterations, s->ev1, s->ev2);
+    const PcgScalars& h = *s->sc_host;
+    res->status = h.status;
+    res->iterations = 0;
+    res->converged = 1;
+    for (int c = 0; c < K; ++c) {
+        res->iterations = std::max(res->iterations, h.iters[c]);
+        double bn = std::sqrt(h.bnorm2[c]);
+        double tr = bn > 0 ? std::sqrt(h.tr2[c]) / bn : 0.0;
+        double rr = bn > 0 ? std::sqrt(h.rr[c]) / bn : 0.0;
+        res->relres_true = std::max(res->relres_true, tr);
+        res->relres_rec = std::max(res->relres_rec, rr);
+        double pr = h.rz0[c] > 0 ? std::sqrt(h.rz[c] / h.rz0[c]) : 0.0;
+        res->precond_ratio = std::max(res->precond_ratio, pr);
+        bool conv;
+        if (s->cfg.stop_rule == 0) conv = tr <= s->cfg.tol;
+        else conv = !h.active[c];
+        if (!conv) res->converged = 0;
+    }
+    if (h.status != 0) res->converged = 0;
+    return cudaSuccess;
+}
+
+// ---- single operator applications ----------------------------------------
+
+namespace {
+__global__ void cm_to_rm_kernel(const double* __restrict__ cm, int ld, double* rm, int32_t n, int k) {
+    const int64_t total = (int64_t)n * k;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        int64_t i = t / k;
+        int c = (int)(t % k);
+        rm[t] = cm[(size_t)c * ld + i];
+    }
+}
+__global__ void rm_to_cm_kernel(const double* __restrict__ rm, double* cm, int ld, int32_t n, int k) {
+    const int64_t total = (int64_t)n * k;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        int64_t i = t / k;
+        int c = (int)(t % k);
+        cm[(size_t)c * ld + i] = rm[t];
+    }
+}
+}  // namespace
+
+cudaError_t cm_to_rm(const double* cm, int ld, double* rm, int32_t n, int k, cudaStream_t s) {
+    int64_t total = (int64_t)n * k;
+    int grid = (int)std::min<int64_t>(std::max<int64_t>(ceil_div(total, kBlock), 1), 148 * 16);
+    cm_to_rm_kernel<<<grid, kBlock, 0, s>>>(cm, ld, rm, n, k);
+    return cudaGetLastError();
+}
+
+cudaError_t rm_to_cm(const double* rm, double* cm, int ld, int32_t n, int k, cudaStream_t s) {
+    int64_t total = (int64_t)n * k;
+    int grid = (int)std::min<int64_t>(std::max<int64_t>(ceil_div(total, kBlock), 1), 148 * 16);
+    rm_to_cm_kernel<<<grid, kBlock, 0, s>>>(rm, cm, ld, n, k);
+    return cudaGetLastError();
+}
+
+cudaError_t spmv_f64(const DevCsc& A, const double* x, double* y, int k, cudaStream_t s) {
+    int64_t total = (int64_t)A.n * k;
+    int grid = (int)std::min<int64_t>(std::max<int64_t>(ceil_div(total, kBlock), 1), 148 * 16);
+    spmv_plain_kernel<<<grid, kBlock, 0, s>>>(A.n, A.colptr, A.rowind, A.val, x, y, k);
+    return cudaGetLastError();
+}
+
+template <int K, typename TV>
+static cudaError_t precond_apply_t(const DevFactor& F, const double* r, double* z, double* y, int* status,
+                                   double timeout_s, cudaStream_t s, int device) {
+    PcgScalars* sc = nullptr;
+    cudaError_t e = cudaMalloc(&sc, sizeof(PcgScalars));
+    if (e != cudaSuccess) return e;
+    cudaMemsetAsync(sc, 0, sizeof(PcgScalars), s);
+    SolveArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = F.n;
+    a.lr_ptr = F.lr_ptr;
+    a.lr_idx = F.lr_idx;
+    a.lr_val = std::is_same<TV, float>::value ? (const void*)F.lr_val32 : (const void*)F.lr_val;
+    a.lc_ptr = F.lc_ptr;
+    a.lc_idx = F.lc_idx;
+    a.lc_val = std::is_same<TV, float>::value ? (const void*)F.lc_val32 : (const void*)F.lc_val;
+    a.diag = std::is_same<TV, float>::value ? (const void*)F.diag32 : (const void*)F.diag;
+    a.r = const_cast<double*>(r);
+    a.y = y;
+    a.z = z;
+    a.sc = sc;
+    a.update = 0;
+    a.reduce = 0;
+    a.timeout_ns = (unsigned long long)(timeout_s * 1e9);
+    const int64_t total = (int64_t)F.n * K;
+    fill_pending_kernel<<<148 * 8, kBlock, 0, s>>>(y, total);
+    int gf = resident_blocks((void*)fwd_kernel<K, TV>, device);
+    int gb = resident_blocks((void*)bwd_kernel<K, TV>, device);
+    fwd_kernel<K, TV><<<gf, kBlock, 0, s>>>(a);
+    bwd_kernel<K, TV><<<gb, kBlock, 0, s>>>(a);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(status, &sc->status, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(sc);
+    return e;
+}
+
+cudaError_t precond_apply(const DevFactor& F, const double* r, double* z, double* ywork, int k, bool fp32,
+                          int* status, double timeout_s, cudaStream_t s) {
+    int device = 0;
+    cudaGetDevice(&device);
+#define RCHOL_PA(KK)                                                                                     \
+    case KK:                                                                                             \
+        return fp32 ? precond_apply_t<KK, float>(F, r, z, ywork, status, timeout_s, s, device)           \
+                    : precond_apply_t<KK, double>(F, r, z, ywork, status, timeout_s, s, device);
+    switch (k) {
+        RCHOL_PA(1)
+        RCHOL_PA(2)
+        RCHOL_PA(4)
+        RCHOL_PA(8)
+        RCHOL_PA(16)
+        RCHOL_PA(32)
+        default:
+            return cudaErrorInvalidValue;
+    }
+#undef RCHOL_PA
+}
+
+}  // namespace rchol

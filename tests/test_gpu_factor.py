@@ -1,0 +1,135 @@
+"""CUDA factor (through the C-ABI) against the oracle, bit-exact.
+
+The GPU eliminates vertices in whatever order the ready queue serves them;
+with Philox uniforms keyed by (seed, vertex, slot) and total orders for the
+merge and the value sort, the factor must equal the oracle's ORC_MODE_B200
+factor exactly: same pattern, same FP64 bits in L and D.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as O
+import rchol_b200 as R
+from helpers import OracleProblem, grid_laplacian
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "grid32_logw": dict(dims=(32, 32), seed=1),
+    "grid40_unit": dict(dims=(40, 40), seed=2, log_weights=False),
+    "cube10_sddm": dict(dims=(10, 10, 10), seed=3, excess_frac=0.05, wlo=1e-3, whi=1e3),
+    "cube24_logw": dict(dims=(24, 24, 24), seed=4, wlo=1e-3, whi=1e3),
+}
+
+
+def _gpu_factor(n, r, c, v, trim, seed, **opts):
+    ctx = R.Context(seed=seed, **opts)
+    try:
+        ctx.set_triplets(n, r, c, v, trim_ground=trim)
+        f = ctx.factor()
+        out = f.to_host()
+        info = f.info()
+        f.free()
+        return out, info
+    finally:
+        ctx.close()
+
+
+def _compare(gpu, orc):
+    cp, ri, val, d = gpu
+    assert np.array_equal(cp, orc["colptr"])
+    assert np.array_equal(ri, orc["rowind"])
+    assert np.array_equal(val, orc["val"])  # bit-exact FP64
+    assert np.array_equal(d, orc["diag"])
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_factor_bitexact_vs_oracle(name):
+    spec = dict(CASES[name])
+    dims = spec.pop("dims")
+    seed = spec.pop("seed")
+    n, r, c, v, ground = grid_laplacian(dims, seed=seed, **spec)
+    P = OracleProblem(n, r, c, v, trim=ground)
+    orc = P.factor(seed=seed + 100)
+    gpu, info = _gpu_factor(n, r, c, v, ground, seed + 100)
+    _compare(gpu, orc)
+    assert info.nnz_strict == orc["stats"]["nnz_strict"] or ground
+    assert info.attempts >= 1
+
+
+def test_factor_config1_bitexact():
+    n, r, c, v, g = R.generate("grid2d", [256, 256], seed=0)
+    P = OracleProblem(n, r, c, v)
+    orc = P.factor(seed=1)
+    gpu, info = _gpu_factor(n, r, c, v, False, 1)
+    _compare(gpu, orc)
+    assert info.fills == orc["stats"]["fills"]
+
+
+@pytest.mark.parametrize("opts", [dict(warps_per_block=1, num_blocks=1), dict(num_blocks=64),
+                                  dict(bucket_cap=1, slab_entries=32), dict(bucket_cap=2, pool_mult=1.0)])
+def test_factor_independent_of_launch_shape_and_pools(opts):
+    """One warp, a few warps, tiny buckets (overflow chunks), tiny shared
+    slabs (global slab path), a tiny pool (capacity retry): same bits."""
+    n, r, c, v, _ = grid_laplacian((20, 20, 6), seed=5, wlo=1e-3, whi=1e3)
+    P = OracleProblem(n, r, c, v)
+    orc = P.factor(seed=7)
+    gpu, info = _gpu_factor(n, r, c, v, False, 7, **opts)
+    _compare(gpu, orc)
+    if opts.get("bucket_cap", 32) <= 2:
+        assert info.overflow_fills > 0 and info.chunks_used > 0
+    if opts.get("slab_entries", 256) == 32:
+        assert info.big_vertices > 0
+    if opts.get("pool_mult", 6.0) == 1.0:
+        assert info.attempts >= 1
+
+
+def test_factor_repeatable_in_one_context():
+    n, r, c, v, _ = grid_laplacian((30, 30), seed=8)
+    ctx = R.Context(seed=3)
+    try:
+        ctx.set_triplets(n, r, c, v)
+        a = ctx.factor()
+        b = ctx.factor()
+        A, B = a.to_host(), b.to_host()
+        for x, y in zip(A, B):
+            assert np.array_equal(x, y)
+        a.free()
+        b.free()
+    finally:
+        ctx.close()
+
+
+def test_factor_write_read_roundtrip(tmp_path):
+    n, r, c, v, g = grid_laplacian((9, 9, 9), seed=9, excess_frac=0.1)
+    ctx = R.Context(seed=2)
+    try:
+        ctx.set_triplets(n, r, c, v, trim_ground=g)
+        f = ctx.factor()
+        prefix = str(tmp_path) + "/"
+        f.write(prefix)
+        f2 = ctx.factor_read(prefix)
+        A, B = f.to_host(), f2.to_host()
+        assert np.array_equal(A[0], B[0]) and np.array_equal(A[1], B[1])
+        np.testing.assert_allclose(A[2], B[2], rtol=1e-15)
+        np.testing.assert_array_equal(A[3], B[3])
+        # the file is the reference's format: unit diagonal, rows >= cols, 1-based
+        rows, cols, vals, diag = O.read_factor_files(prefix, f.info().n)
+        assert np.all(rows >= cols) and np.all(vals[rows == cols] == 1.0)
+    finally:
+        ctx.close()
+
+
+def test_invalid_inputs_report_status():
+    ctx = R.Context()
+    try:
+        with pytest.raises(R.RcholError) as e:
+            ctx.factor()
+        assert e.value.status == 9
+        n, r, c, v, _ = grid_laplacian((4, 4), seed=1)
+        v = v.copy()
+        v[0] = np.inf
+        with pytest.raises(R.RcholError):
+            ctx.set_triplets(n, r, c, v)
+    finally:
+        ctx.close()

