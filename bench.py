@@ -1,0 +1,470 @@
+#!/usr/bin/env python
+"""Benchmark: randomized-Cholesky factor + PCG time to a true FP64 relative
+residual of 1e-6 on one B200, FP32-factor/FP64-PCG ("mixed", the headline
+`value`) beside the plain FP64 form, on the 128^3 random-coefficient SDDM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = factorization of the resident matrix (setup, elimination,
+assembly) + one PCG solve of a resident zero-mean N(0,1) right-hand side.
+Inputs live in HBM before the timed region; the matrix and the factor work
+(~2 GB) exceed the 126 MB L2, and a 256 MiB buffer is also rewritten between
+timed steps.  Each step is bracketed by CUDA events; the timed region by a
+barrier and device synchronisation; the reported time is the max over ranks.
+With --gpus N > 1 every rank solves its own replica (the path does not shard).
+
+--impl reference times the reference's own CPU implementation on this host:
+the reference CPU factor (cpu_implementation/driver_local.cpp built from its
+sources under oracle/_ref/) plus the CPU PCG the reference would run, whose
+MKL dependency is absent here, so the oracle's FP64 port of
+experiment/custom_cg.hpp stands in for it.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "parallel-randomized-cholesky_b200"))
+
+METRIC = "factor+PCG time to rel. residual 1e-6 (s); FP32-mixed vs FP64 form, same B200"
+
+CONFIGS = {
+    "c2": dict(kind="grid3d", dims=[128, 128, 128], wlo=1e-3, whi=1e3, log_weights=True, excess_frac=0.05,
+               excess_lo=0.0, excess_hi=1e-2, seed=2, tol=1e-6,
+               workload="SDDM 3D 7-point 128^3 (2,097,152 unknowns), log-uniform conductances [1e-3,1e3] (seed 2), "
+                        "diagonal excess U[0,1e-2]*degree on 5% of rows, ground vertex appended and trimmed, "
+                        "ascending-nnz order, 1 zero-mean N(0,1) RHS"),
+    "c1": dict(kind="grid2d", dims=[256, 256], wlo=1.0, whi=1.0, log_weights=False, excess_frac=0.0, excess_lo=0.0,
+               excess_hi=0.0, seed=0, tol=1e-6,
+               workload="Laplacian 2D 5-point 256^2 unit weights, ascending-nnz order (seed 0), factor seed 1, "
+                        "1 zero-mean N(0,1) RHS"),
+}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------
+
+def dist_init(n_gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return rank, world, local
+
+
+def max_over_ranks(x, world):
+    """Max of a float over ranks (the driver's rule for multi-GPU timings)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl" else torch.device("cpu")
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, val in zip(names, parts[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        busy = [s for s in sm if s > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+
+def build_workload(cfg):
+    import rchol_b200 as R
+    n, r, c, v, g = R.generate(cfg["kind"], cfg["dims"], wlo=cfg["wlo"], whi=cfg["whi"],
+                               log_weights=cfg["log_weights"], excess_frac=cfg["excess_frac"],
+                               excess_lo=cfg["excess_lo"], excess_hi=cfg["excess_hi"], seed=cfg["seed"])
+    colptr, rowind, val = R.csc_from_triplets(n, r, c, v)
+    return dict(n=n, colptr=colptr, rowind=rowind, val=val, ground=g, triplets=(r, c, v))
+
+
+def algorithmic_bytes(n, nnz_a, nnz_l, lnnz_a, fills, k, sv):
+    """Bytes each kernel must move once (no cache reuse credit).
+    spmv_update: A in CSR (int32 index + FP64 value), row pointers, one read
+      of z, p and q read+write, y reset;
+    fwd: L in CSR (int32 + sv), int64 row pointers, level order, one read of
+      each y_j it consumes (counted once per row), x/r read+write, p/q read,
+      y write, z reset;
+    bwd: L in CSC, pointers, order, D, y and r read, z write;
+    factor: strict lower A read (12 B), every fill gathered and emitted
+      (16 B each way), every original entry gathered (16 B), L written (12 B)
+      and D (8 B)."""
+    vec = 8 * k
+    spmv = nnz_a * 12 + (n + 1) * 4 + n * vec * (1 + 2 + 2 + 1)
+    fwd = nnz_l * (4 + sv) + (n + 1) * 8 + n * 4 + n * vec * (1 + 2 + 2 + 1 + 1 + 1 + 1)
+    bwd = nnz_l * (4 + sv) + (n + 1) * 8 + n * 4 + n * sv + n * vec * 3
+    factor = 12 * lnnz_a + (fills + lnnz_a) * 16 + fills * 16 + 12 * nnz_l + 8 * n
+    return dict(spmv_update=spmv, fwd_solve=fwd, bwd_solve=bwd, factor=factor)
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "of measured"
+    return 6650.0, "of fallback"
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of each kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {}
+
+
+def run_b200(args, cfg, rank, world, local):
+    import torch
+    import rchol_b200 as R
+
+    dev = torch.device("cuda", local)
+    W = build_workload(cfg)
+    n, ground = W["n"], W["ground"]
+    ns = n - 1 if ground else n
+    ctx = {}
+    for form, prec in (("mixed", R.PREC_FP32_FACTOR), ("fp64", R.PREC_FP64)):
+        c = R.Context(device=local, seed=1, precision=prec, tol=cfg["tol"], stop_rule=R.STOP_RELRES)
+        c.set_csc(n, W["colptr"], W["rowind"], W["val"], trim_ground=ground)
+        ctx[form] = c
+    rng = np.random.default_rng(1000 + rank)
+    b = rng.standard_normal(ns)
+    b -= b.mean()
+    b_dev = torch.as_tensor(b, device=dev)
+    x_dev = torch.zeros(ns, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step(form):
+        c = ctx[form]
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        f = c.factor()
+        info = c.pcg_solve_device(f, 1, b_dev.data_ptr(), x_dev.data_ptr(), ns)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        fi = f.info()
+        return ms, f, fi, info
+
+    for _ in range(args.warmup):
+        for form in ("mixed", "fp64"):
+            ms, f, fi, info = step(form)
+            f.free()
+            flush.random_()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    times = {"mixed": [], "fp64": []}
+    last = {}
+    launches = 0
+    for _ in range(args.steps):
+        for form in ("mixed", "fp64"):
+            flush.random_()
+            ms, f, fi, info = step(form)
+            times[form].append(ms)
+            launches += fi.kernel_launches + info["kernel_launches"]
+            if form in last:
+                last[form][0].free()
+            last[form] = (f, fi, info)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    mixed_s = max_over_ranks(sum(times["mixed"]) / 1000.0 / args.steps, world)
+    fp64_s = max_over_ranks(sum(times["fp64"]) / 1000.0 / args.steps, world)
+
+    # per-kernel profile of the mixed form, for the roofline
+    f32, fi32, si32 = last["mixed"]
+    prof = ctx["mixed"].profile_solve(f32, 1, reps=5)
+    iters = si32["iterations"]
+    per_step = {"factor": fi32.ms_factor, "spmv_update": prof[0] * iters, "fwd_solve": prof[1] * iters,
+                "bwd_solve": prof[2] * iters}
+    per_launch = {"factor": fi32.ms_factor, "spmv_update": prof[0], "fwd_solve": prof[1], "bwd_solve": prof[2]}
+    A_nnz = int(W["colptr"][-1])
+    # the solve matrix is trimmed: nnz without the ground row/column
+    a_nnz_solve = A_nnz - (int(np.diff(W["colptr"])[-1]) * 2 - 1 if ground else 0)
+    ab = algorithmic_bytes(ns, a_nnz_solve, fi32.nnz_strict, fi32.nnz_lower_a, fi32.fills, 1, 4)
+    dom = max(per_step, key=per_step.get)
+    peak, peak_src = measured_peaks()
+    achieved = ab[dom] / (per_launch[dom] / 1000.0) / 1e9
+    traffic = committed_traffic().get(dom)
+
+    # e2e through the public API with host buffers (pinned)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    hcp, hri, hv, hb = pin(W["colptr"]), pin(W["rowind"]), pin(W["val"]), pin(b)
+    hx = torch.zeros(ns, dtype=torch.float64).pin_memory()
+    e2e_ms = []
+    c = ctx["mixed"]
+    import ctypes as C
+    for it in range(max(1, min(args.steps, 3)) + 1):
+        flush.random_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        R._check(R.lib().rchol_set_csc(c.h, n, C.c_void_p(hcp.data_ptr()), C.c_void_p(hri.data_ptr()),
+                                       C.c_void_p(hv.data_ptr()), 0, int(ground)), c.h)
+        f = c.factor()
+        si = R.SolveInfo()
+        st = R.lib().rchol_pcg_solve(c.h, f.h, 1, C.c_void_p(hb.data_ptr()), C.c_void_p(hx.data_ptr()), ns, 0,
+                                     C.byref(si))
+        e1.record()
+        e1.synchronize()
+        f.free()
+        if st not in (0, 6):
+            R._check(st, c.h)
+        if it > 0:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_s = max_over_ranks(sum(e2e_ms) / len(e2e_ms) / 1000.0, world)
+    relres = float(np.linalg.norm(b - spmv_host(W, ns, hx.numpy())) / np.linalg.norm(b))
+
+    out = {
+        "metric": METRIC, "value": round(mixed_s, 6), "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(mixed_s * 1000.0, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 factor / f64 PCG", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "n": ns, "nnz_A": a_nnz_solve, "tol": cfg["tol"], "rhs": 1,
+                   "parallelism": f"replicas x{args.gpus}", "l2": "inputs larger than L2 and a 256 MiB L2 flush "
+                                                               "between timed steps"},
+        "fp64_s": round(fp64_s, 6), "speedup_mixed_vs_fp64": round(fp64_s / mixed_s, 3),
+        "iterations": {"mixed": last["mixed"][2]["iterations"], "fp64": last["fp64"][2]["iterations"]},
+        "relres_true": {"mixed": last["mixed"][2]["relres_true"], "fp64": last["fp64"][2]["relres_true"],
+                        "e2e_host_check": relres},
+        "phase_ms": {"setup": round(fi32.ms_setup, 3), "factor": round(fi32.ms_factor, 3),
+                     "assemble": round(fi32.ms_assemble, 3), "pcg": round(last["mixed"][2]["ms_total"], 3)},
+        "kernel_ms_per_launch": {k: round(v, 4) for k, v in per_launch.items()},
+        "factor_stats": {"nnz_L": fi32.nnz_strict + fi32.n, "nnz_ratio": round((fi32.nnz_strict + fi32.n) /
+                                                                                 fi32.nnz_lower_a, 4),
+                         "solve_depth": fi32.solve_depth, "max_gather": fi32.max_gather},
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_src,
+                     "traffic": traffic, "algorithmic_bytes": ab[dom],
+                     "all_kernels_GBps": {k: round(ab[k] / (per_launch[k] / 1000.0) / 1e9, 1) for k in ab}},
+        "e2e": {"value": round(e2e_s, 6), "unit": "s",
+                "h2d_bytes_per_step": int(W["colptr"].nbytes + W["rowind"].nbytes + W["val"].nbytes + b.nbytes),
+                "d2h_bytes_per_step": int(ns * 8)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    for c in ctx.values():
+        for form in last:
+            pass
+    for form in last:
+        last[form][0].free()
+    return out, W, last["fp64"][2]["iterations"]
+
+
+def spmv_host(W, ns, x):
+    """y = A x on the host for the trimmed matrix (residual check only)."""
+    cp, ri, v = W["colptr"], W["rowind"], W["val"]
+    cols = np.repeat(np.arange(len(cp) - 1), np.diff(cp))
+    m = (ri < ns) & (cols < ns)
+    y = np.zeros(ns)
+    np.add.at(y, ri[m], v[m] * x[cols[m]])
+    return y
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (reference factor + oracle PCG port)
+# ---------------------------------------------------------------------------
+
+def reference_cpu_step(W, mtx_path, threads, iters_hint, pcg_sample_iters, factor_cache):
+    """One bounded sample of the reference CPU implementation: a full run of
+    the reference CPU factor (its own printed factor time) and `pcg_sample_iters`
+    iterations of the FP64 CPU PCG on its factor, scaled to the iteration count
+    of the full solve."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    n, ground = W["n"], W["ground"]
+    ns = n - 1 if ground else n
+    want = factor_cache.get("L") is None
+    out = O.run_reference(mtx_path, threads=threads, physics=ground, want_factor=want, timeout=1800)
+    if want:
+        rows, cols, vals, diag = out["rows"], out["cols"], out["vals"], out["diag"]
+        m = (rows != cols) & (rows < ns) & (cols < ns)
+        order = np.lexsort((rows[m], cols[m]))
+        r, c, v = rows[m][order], cols[m][order], vals[m][order]
+        cp = np.concatenate([[0], np.cumsum(np.bincount(c, minlength=ns))]).astype(np.int64)
+        acp, arow, aval = O.trim_last(n, W["colptr"], W["rowind"], W["val"]) if ground else \
+            (W["colptr"], W["rowind"], W["val"])
+        factor_cache["L"] = (cp, r.astype(np.int32), v, diag[:ns].copy())
+        factor_cache["A"] = (acp, arow, aval)
+    cp, r, v, d = factor_cache["L"]
+    acp, arow, aval = factor_cache["A"]
+    rng = np.random.default_rng(7)
+    b = rng.standard_normal(ns)
+    b -= b.mean()
+    if "iters" not in factor_cache:
+        if iters_hint is None:
+            _, info = O.pcg(ns, acp, arow, aval, cp, r, v, d, b, tol=1e-6, max_iter=1000, nthreads=threads)
+            factor_cache["iters"] = info["iterations"]
+        else:
+            factor_cache["iters"] = iters_hint
+    t0 = time.perf_counter()
+    O.pcg(ns, acp, arow, aval, cp, r, v, d, b, tol=1e-300, max_iter=pcg_sample_iters, nthreads=threads)
+    per_iter = (time.perf_counter() - t0) / pcg_sample_iters
+    solve_s = per_iter * factor_cache["iters"]
+    return out["factor_time"] + solve_s, out["factor_time"], solve_s, factor_cache["iters"]
+
+
+def run_reference_arm(args, cfg):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    if not os.path.exists(O.REF_BIN):
+        return {"impl": "reference", "unavailable": "reference CPU factor not built (oracle/_ref/rchol_ref_cpu)"}
+    import rchol_b200 as R
+    W = build_workload(cfg)
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as td:
+        mtx = os.path.join(td, "input.mtx")
+        R.write_mtx(mtx, W["n"], *W["triplets"])
+        cache = {}
+        for _ in range(args.warmup):
+            reference_cpu_step(W, mtx, threads, None, 2, cache)
+        vals, facs, sols = [], [], []
+        for _ in range(args.steps):
+            tot, fac, sol, iters = reference_cpu_step(W, mtx, threads, None, 3, cache)
+            vals.append(tot)
+            facs.append(fac)
+            sols.append(sol)
+    v = statistics.mean(vals)
+    sample = (f"reference CPU factor (cpu_implementation/driver_local.cpp, unmodified) full run on {threads} threads "
+              f"+ 3 iterations of the FP64 CPU PCG port on the reference's factor (MKL absent), scaled to the "
+              f"{cache['iters']} iterations of its full solve")
+    return {"metric": METRIC, "value": round(v, 6), "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(v * 1000, 3), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": cfg["workload"], "tol": cfg["tol"], "rhs": 1, "parallelism": "cpu"},
+            "factor_s": round(statistics.mean(facs), 6), "pcg_s": round(statistics.mean(sols), 6),
+            "cpu_baseline": {"value": round(v, 6), "unit": "s", "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": round(v, 6), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return
+        print(json.dumps(run_reference_arm(args, cfg)))
+        return
+    rank, world, local = dist_init(args.gpus)
+    out, W, iters64 = run_b200(args, cfg, rank, world, local)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as O
+        if os.path.exists(O.REF_BIN):
+            import rchol_b200 as R
+            threads = os.cpu_count() or 1
+            with tempfile.TemporaryDirectory() as td:
+                mtx = os.path.join(td, "input.mtx")
+                R.write_mtx(mtx, W["n"], *W["triplets"])
+                tot, fac, sol, iters = reference_cpu_step(W, mtx, threads, iters64, 3, {})
+            out["cpu_baseline"] = {"value": round(tot, 6), "unit": "s", "cores": threads, "kind": "reference",
+                                   "sample": f"reference CPU factor (cpu_implementation/driver_local.cpp) full run on "
+                                             f"{threads} threads ({fac:.3f} s) + 3 iterations of the FP64 CPU PCG "
+                                             f"port on its factor scaled to {iters} iterations ({sol:.3f} s)"}
+        else:
+            out["cpu_baseline"] = None
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -63,6 +63,7 @@ typedef struct rchol_opts {
     int device;               /* CUDA device ordinal */
     double timeout_s;         /* bound on every device-side wait */
     int verbose;              /* print phase timings (the reference's stdout) */
+    int poll_ns;              /* back-off (ns) between polls in the triangular solves */
 } rchol_opts;
 
 typedef struct rchol_factor_info {
@@ -80,6 +81,8 @@ typedef struct rchol_factor_info {
     float ms_factor;          /* the elimination kernel */
     float ms_assemble;        /* pool -> CSC/CSR, trim, FP32 copies */
     int attempts;             /* capacity retries + 1 */
+    int solve_depth;          /* levels of the triangular-solve dependency DAG */
+    int kernel_launches;      /* device kernels launched by this factorization */
     /* device pointers (valid while the factor lives) */
     const long long* lc_ptr;  /* strict CSC of L  [n+1] */
     const int* lc_idx;
@@ -166,6 +169,10 @@ rchol_status rchol_pcg_solve(rchol_ctx* ctx, const rchol_factor_t* f, int k, con
 /* One preconditioner application Z = L^-T D^+ L^-1 R (same layout rules). */
 rchol_status rchol_precond_apply(rchol_ctx* ctx, const rchol_factor_t* f, int k, const double* R, double* Z,
                                  int ldb, int on_device, int fp32);
+/* Mean device time (ms) of the three PCG iteration kernels over `reps`
+ * iterations on this factor with k right-hand sides: ms_out[0] SpMV +
+ * vector update, ms_out[1] forward solve, ms_out[2] backward solve. */
+rchol_status rchol_profile_solve(rchol_ctx* ctx, const rchol_factor_t* f, int k, int reps, float* ms_out);
 /* Y = A X with the (trimmed) matrix of the context. */
 rchol_status rchol_spmv(rchol_ctx* ctx, int k, const double* X, double* Y, int ldb, int on_device);
 

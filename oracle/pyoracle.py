@@ -212,11 +212,24 @@ def read_factor_files(prefix, n):
         while line.startswith("%"):
             line = f.readline()
         nr, nc, nnz = map(int, line.split())
-        data = np.loadtxt(f, dtype=np.float64, ndmin=2) if nnz else np.zeros((0, 3))
+        if nnz == 0:
+            data = np.zeros((0, 3))
+        else:
+            try:
+                import pandas as pd
+                data = pd.read_csv(f, sep=" ", header=None, dtype=np.float64, engine="c",
+                                   float_precision="round_trip").to_numpy()
+            except ImportError:
+                data = np.loadtxt(f, dtype=np.float64, ndmin=2)
     rows = data[:, 0].astype(np.int64) - 1
     cols = data[:, 1].astype(np.int64) - 1
     vals = data[:, 2]
-    diag = np.loadtxt(prefix + "sol_diag.txt", dtype=np.float64, ndmin=1)
+    try:
+        import pandas as pd
+        diag = pd.read_csv(prefix + "sol_diag.txt", header=None, dtype=np.float64, engine="c",
+                           float_precision="round_trip")[0].to_numpy()
+    except ImportError:
+        diag = np.loadtxt(prefix + "sol_diag.txt", dtype=np.float64, ndmin=1)
     return rows, cols, vals, diag
 
 

@@ -5,6 +5,7 @@
 //   D   the pivots,
 // with the ground vertex (the last one) removed when the input was an SDDM
 // converted to a Laplacian.  FP32 copies feed the mixed-precision solve.
+#include <algorithm>
 #include <climits>
 
 #include "device_common.cuh"
@@ -65,7 +66,7 @@ __global__ void transpose_kernel(int32_t nout, const int64_t* __restrict__ lc_pt
 // over a padded power of two in a shared slab, or in a per-warp global slab
 // for rows longer than the shared one.
 __global__ void sort_rows_kernel(int32_t nrows, const int64_t* __restrict__ ptr, int32_t* idx, double* val,
-                                 int32_t* gkey, double* gval, int64_t gcap, int32_t* status) {
+                                 int32_t* long_rows, int32_t* nlong) {
     __shared__ int32_t skey[8][kSortSlab];
     __shared__ double sval[8][kSortSlab];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -81,16 +82,12 @@ __global__ void sort_rows_kernel(int32_t nrows, const int64_t* __restrict__ ptr,
         if (__all_sync(kFull, sorted)) continue;
         int P = 1;
         while (P < len) P <<= 1;
+        if (P > kSortSlab) {  // left to the block-level sort
+            if (lane == 0) long_rows[atomicAdd(nlong, 1)] = (int32_t)r;
+            continue;
+        }
         int32_t* key = skey[wib];
         double* v = sval[wib];
-        if (P > kSortSlab) {
-            if (P > gcap) {
-                if (lane == 0) raise_error(status, kDevCapacity);
-                continue;
-            }
-            key = gkey + gw * gcap;
-            v = gval + gw * gcap;
-        }
         for (int t = lane; t < P; t += 32) {
             key[t] = t < len ? idx[o + t] : INT_MAX;
             v[t] = t < len ? val[o + t] : 0.0;
@@ -120,6 +117,79 @@ __global__ void sort_rows_kernel(int32_t nrows, const int64_t* __restrict__ ptr,
             val[o + t] = v[t];
         }
         __syncwarp();
+    }
+}
+
+// One CTA per long row: bitonic sort over a padded power of two held in
+// dynamic shared memory (up to kBlockSortCap entries) or, beyond that, in a
+// per-CTA global slab.
+constexpr int kBlockSortCap = 8192;
+
+__global__ void sort_long_rows_kernel(const int32_t* __restrict__ rows, int32_t nlong, const int64_t* __restrict__ ptr,
+                                      int32_t* idx, double* val, int32_t* gkey, double* gval, int64_t gcap,
+                                      int32_t* status) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    double* sv = reinterpret_cast<double*>(sm);
+    int32_t* sk = reinterpret_cast<int32_t*>(sv + kBlockSortCap);
+    for (int t = blockIdx.x; t < nlong; t += gridDim.x) {
+        const int32_t r = rows[t];
+        const int64_t o = ptr[r];
+        const int len = (int)(ptr[r + 1] - o);
+        int P = 1;
+        while (P < len) P <<= 1;
+        int32_t* key = sk;
+        double* v = sv;
+        if (P > kBlockSortCap) {
+            if (P > gcap) {
+                if (threadIdx.x == 0) raise_error(status, kDevCapacity);
+                continue;
+            }
+            key = gkey + (int64_t)blockIdx.x * gcap;
+            v = gval + (int64_t)blockIdx.x * gcap;
+        }
+        for (int q = threadIdx.x; q < P; q += blockDim.x) {
+            key[q] = q < len ? idx[o + q] : INT_MAX;
+            v[q] = q < len ? val[o + q] : 0.0;
+        }
+        __syncthreads();
+        for (int k = 2; k <= P; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = threadIdx.x; i < P; i += blockDim.x) {
+                    int l = i ^ j;
+                    if (l > i) {
+                        bool asc = (i & k) == 0;
+                        if ((key[i] > key[l]) == asc) {
+                            int32_t tk = key[i];
+                            key[i] = key[l];
+                            key[l] = tk;
+                            double tv = v[i];
+                            v[i] = v[l];
+                            v[l] = tv;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (int q = threadIdx.x; q < len; q += blockDim.x) {
+            idx[o + q] = key[q];
+            val[o + q] = v[q];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void level_hist_kernel(const int32_t* __restrict__ level, int32_t n, int32_t* hist) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) atomicAdd(hist + level[i], 1);
+}
+
+__global__ void level_scatter_kernel(const int32_t* __restrict__ level, int32_t n, const int32_t* __restrict__ start,
+                                     int32_t* cursor, int32_t* order) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        int l = level[i];
+        order[start[l] + atomicAdd(cursor + l, 1)] = (int32_t)i;
     }
 }
 
@@ -222,29 +292,51 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
     transpose_kernel<<<grid_for((int64_t)nout * 32, 256), 256, 0, s>>>(nout, f.lc_ptr, f.lc_idx, f.lc_val, f.lr_ptr,
                                                                        cnt, f.lr_idx, f.lr_val);
     RCHOL_TRY(cudaGetLastError());
-    // rows longer than the shared slab sort in a per-warp global slab sized
-    // for the longest row
+    // deterministic row order: warp sort for short rows, CTA sort for long ones
     const int sort_block = 256;
     const int sort_grid = 148 * 4;
-    const int64_t warps = (int64_t)sort_grid * (sort_block / 32);
-    int32_t* dmax = nullptr;
-    RCHOL_TRY(dmalloc(&dmax, 1));
-    RCHOL_TRY(cudaMemsetAsync(dmax, 0, sizeof(int32_t), s));
-    max_kernel<<<grid_for(nout, 256), 256, 0, s>>>(cnt, nout, dmax);
+    int32_t* dsc = nullptr;  // [0] long-row count, [1] max row length, [2] max level
+    int32_t* long_rows = nullptr;
+    RCHOL_TRY(dmalloc(&dsc, 4));
+    RCHOL_TRY(dmalloc(&long_rows, nout));
+    RCHOL_TRY(cudaMemsetAsync(dsc, 0, sizeof(int32_t) * 4, s));
+    max_kernel<<<grid_for(nout, 256), 256, 0, s>>>(cnt, nout, dsc + 1);
+    max_kernel<<<grid_for(nout, 256), 256, 0, s>>>(w.level, nout, dsc + 2);
+    sort_rows_kernel<<<sort_grid, sort_block, 0, s>>>(nout, f.lr_ptr, f.lr_idx, f.lr_val, long_rows, dsc);
     RCHOL_TRY(cudaGetLastError());
-    int32_t maxrow = 0;
-    RCHOL_TRY(cudaMemcpyAsync(&maxrow, dmax, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    int32_t hs[4] = {0, 0, 0, 0};
+    RCHOL_TRY(cudaMemcpyAsync(hs, dsc, sizeof(hs), cudaMemcpyDeviceToHost, s));
     RCHOL_TRY(cudaStreamSynchronize(s));
-    cudaFree(dmax);
-    int64_t gcap = 1;
-    while (gcap < maxrow) gcap <<= 1;
-    if (gcap <= kSortSlab) gcap = 1;
     int32_t* gkey = nullptr;
     double* gval = nullptr;
-    RCHOL_TRY(dmalloc(&gkey, warps * gcap));
-    RCHOL_TRY(dmalloc(&gval, warps * gcap));
-    sort_rows_kernel<<<sort_grid, sort_block, 0, s>>>(nout, f.lr_ptr, f.lr_idx, f.lr_val, gkey, gval, gcap,
-                                                      w.counters + 3);
+    int64_t gcap = 1;
+    const int lgrid = hs[0] > 0 ? std::min(hs[0], 148 * 2) : 1;
+    if (hs[1] > kBlockSortCap) {
+        while (gcap < hs[1]) gcap <<= 1;
+        RCHOL_TRY(dmalloc(&gkey, (int64_t)lgrid * gcap));
+        RCHOL_TRY(dmalloc(&gval, (int64_t)lgrid * gcap));
+    }
+    if (hs[0] > 0) {
+        const size_t smem = (size_t)kBlockSortCap * 12;
+        RCHOL_TRY(cudaFuncSetAttribute(sort_long_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        sort_long_rows_kernel<<<lgrid, 512, smem, s>>>(long_rows, hs[0], f.lr_ptr, f.lr_idx, f.lr_val, gkey, gval,
+                                                        gcap, w.counters + 3);
+        RCHOL_TRY(cudaGetLastError());
+    }
+    // rows in non-decreasing forward level
+    const int32_t depth = hs[2] + 1;
+    f.depth = depth;
+    int32_t *hist = nullptr, *lstart = nullptr;
+    RCHOL_TRY(dmalloc(&hist, depth));
+    RCHOL_TRY(dmalloc(&lstart, (int64_t)depth + 1));
+    RCHOL_TRY(dmalloc(&f.order, nout));
+    void* tmp2 = nullptr;
+    RCHOL_TRY(cudaMalloc(&tmp2, scan_tmp_bytes(depth)));
+    RCHOL_TRY(cudaMemsetAsync(hist, 0, sizeof(int32_t) * (size_t)depth, s));
+    level_hist_kernel<<<grid_for(nout, 256), 256, 0, s>>>(w.level, nout, hist);
+    RCHOL_TRY(exclusive_scan_i32_to_i32(hist, lstart, depth, tmp2, s));
+    RCHOL_TRY(cudaMemsetAsync(hist, 0, sizeof(int32_t) * (size_t)depth, s));
+    level_scatter_kernel<<<grid_for(nout, 256), 256, 0, s>>>(w.level, nout, lstart, hist, f.order);
     RCHOL_TRY(cudaGetLastError());
     RCHOL_TRY(cudaMemcpyAsync(f.diag, w.diag, sizeof(double) * (size_t)nout, cudaMemcpyDeviceToDevice, s));
     if (make_fp32) {
@@ -261,6 +353,11 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
     cudaFree(gval);
     cudaFree(cnt);
     cudaFree(tmp);
+    cudaFree(tmp2);
+    cudaFree(hist);
+    cudaFree(lstart);
+    cudaFree(dsc);
+    cudaFree(long_rows);
     return cudaSuccess;
 }
 

@@ -35,7 +35,7 @@ struct rchol_ctx {
     // solver cache
     rchol::PcgSolver* solver = nullptr;
     const rchol_factor_t* solver_f = nullptr;
-    int solver_k = 0, solver_fp32 = -1, solver_stop = -1, solver_maxit = -1;
+    int solver_k = 0, solver_fp32 = -1, solver_stop = -1, solver_maxit = -1, solver_poll = -1;
     double solver_tol = -1;
     // device staging for solves (row-major blocks)
     double* dB = nullptr;
@@ -81,14 +81,14 @@ void free_csc(DevCsc& a) {
 void free_work(FactorWork& w) {
     void* ps[] = {w.lcolptr, w.lrow,  w.lval, w.dep,  w.queue,  w.fcnt,   w.brow,     w.bval,       w.chead,
                   w.cnext,   w.crow,  w.cval, w.prow, w.pval,   w.pstart, w.pcnt,     w.diag,       w.gscratch,
-                  w.counters, w.counters64, w.scan_tmp};
+                  w.counters, w.counters64, w.scan_tmp, w.level};
     for (void* p : ps) cudaFree(p);
     w = FactorWork();
 }
 
 void free_factor(DevFactor& f) {
     void* ps[] = {f.lc_ptr, f.lc_idx, f.lc_val, f.lc_val32, f.lr_ptr, f.lr_idx, f.lr_val, f.lr_val32, f.diag,
-                  f.diag32};
+                  f.diag32, f.order};
     for (void* p : ps) cudaFree(p);
     f = DevFactor();
 }
@@ -139,6 +139,7 @@ rchol_status alloc_work(rchol_ctx* ctx, const PoolPlan& pp) {
     CK(dalloc(&w.pstart, n), "alloc pool starts");
     CK(dalloc(&w.pcnt, n), "alloc pool counts");
     CK(dalloc(&w.diag, n), "alloc diag");
+    CK(dalloc(&w.level, n), "alloc levels");
     CK(cudaMalloc((void**)&w.gscratch, (size_t)warps * (size_t)w.gscratch_entries * 32), "alloc slab scratch");
     CK(dalloc(&w.counters, 16), "alloc counters");
     CK(dalloc(&w.counters64, 4), "alloc counters64");
@@ -215,6 +216,7 @@ extern "C" rchol_status rchol_opts_default(rchol_opts* o) {
     o->device = 0;
     o->timeout_s = 30.0;
     o->verbose = 0;
+    o->poll_ns = 0;
     return RCHOL_OK;
 }
 
@@ -229,6 +231,7 @@ static rchol_status check_opts(const rchol_opts* o, std::string& why) {
     else if (o->stop_rule < 0 || o->stop_rule > 2) why = "stop_rule";
     else if (o->unroll < 1 || o->unroll > 64) why = "unroll must be 1..64";
     else if (!(o->timeout_s > 0.0)) why = "timeout_s must be positive";
+    else if (o->poll_ns < 0 || o->poll_ns > 100000) why = "poll_ns must be 0..100000";
     else return RCHOL_OK;
     return RCHOL_ERR_INVALID;
 }
@@ -311,14 +314,7 @@ extern "C" rchol_status rchol_set_csc(rchol_ctx* ctx, int n, const int* colptr, 
     if (!ctx || n <= 0 || !colptr || !rowind || !val) return fail(ctx, RCHOL_ERR_INVALID, "bad CSC arguments");
     if (trim_ground && n < 2) return fail(ctx, RCHOL_ERR_INVALID, "trim_ground needs n >= 2");
     cudaSetDevice(ctx->device);
-    drop_solver(ctx);
-    free_work(ctx->w);
-    ctx->w_ready = false;
-    if (ctx->trim) free_csc(ctx->At);
-    free_csc(ctx->A);
-    ctx->have = false;
     int32_t nnz32 = 0;
-    std::vector<int32_t> hptr;
     if (on_device) {
         CK(cudaMemcpy(&nnz32, colptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost), "read nnz");
     } else {
@@ -327,12 +323,27 @@ extern "C" rchol_status rchol_set_csc(rchol_ctx* ctx, int n, const int* colptr, 
             if (colptr[i + 1] < colptr[i]) return fail(ctx, RCHOL_ERR_INVALID, "colptr is not monotone");
     }
     if (nnz32 < 0) return fail(ctx, RCHOL_ERR_INVALID, "negative nnz");
+    // a matrix of the same shape reuses every device buffer (new values or a
+    // new pattern of the same size); the factor work is kept when the strict
+    // lower triangle keeps its size
+    const bool same = ctx->have && ctx->A.n == n && ctx->A.nnz == nnz32 && ctx->trim == (trim_ground != 0);
+    const int64_t old_lnnz = ctx->w.lnnz;
+    drop_solver(ctx);
+    if (ctx->trim) free_csc(ctx->At);
     DevCsc A;
-    A.n = n;
-    A.nnz = nnz32;
-    CK(dalloc(&A.colptr, (int64_t)n + 1), "alloc colptr");
-    CK(dalloc(&A.rowind, A.nnz), "alloc rowind");
-    CK(dalloc(&A.val, A.nnz), "alloc val");
+    if (same) {
+        A = ctx->A;
+    } else {
+        free_work(ctx->w);
+        ctx->w_ready = false;
+        free_csc(ctx->A);
+        A.n = n;
+        A.nnz = nnz32;
+        CK(dalloc(&A.colptr, (int64_t)n + 1), "alloc colptr");
+        CK(dalloc(&A.rowind, A.nnz), "alloc rowind");
+        CK(dalloc(&A.val, A.nnz), "alloc val");
+    }
+    ctx->have = false;
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     CK(cudaMemcpyAsync(A.colptr, colptr, sizeof(int32_t) * ((size_t)n + 1), kind, ctx->stream), "copy colptr");
     CK(cudaMemcpyAsync(A.rowind, rowind, sizeof(int32_t) * (size_t)A.nnz, kind, ctx->stream), "copy rowind");
@@ -346,12 +357,26 @@ extern "C" rchol_status rchol_set_csc(rchol_ctx* ctx, int n, const int* colptr, 
     }
     CK(cudaStreamSynchronize(ctx->stream), "sync upload");
     // largest column (bounds the gather of early vertices)
-    std::vector<int32_t> cp((size_t)n + 1);
-    CK(cudaMemcpy(cp.data(), ctx->A.colptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyDeviceToHost), "read colptr");
     int32_t mx = 0;
-    for (int i = 0; i < n; ++i) mx = std::max(mx, cp[(size_t)i + 1] - cp[(size_t)i]);
+    if (on_device) {
+        std::vector<int32_t> cp((size_t)n + 1);
+        CK(cudaMemcpy(cp.data(), ctx->A.colptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyDeviceToHost),
+           "read colptr");
+        for (int i = 0; i < n; ++i) mx = std::max(mx, cp[(size_t)i + 1] - cp[(size_t)i]);
+    } else {
+        for (int i = 0; i < n; ++i) mx = std::max(mx, colptr[i + 1] - colptr[i]);
+    }
     ctx->max_col = mx;
     ctx->have = true;
+    if (same && ctx->w_ready) {
+        int64_t lnnz = 0;
+        rchol_status s = lower_nnz(ctx, &lnnz);
+        if (s != RCHOL_OK) return s;
+        if (lnnz != old_lnnz || 4 * (int64_t)mx > ctx->w.gscratch_entries) {
+            free_work(ctx->w);
+            ctx->w_ready = false;
+        }
+    }
     return RCHOL_OK;
 }
 
@@ -507,6 +532,11 @@ extern "C" rchol_status rchol_factor(rchol_ctx* ctx, rchol_factor_t** out) {
     info.chunks_used = counters[2];
     info.factor_grid = grid;
     info.attempts = attempt + 1;
+    info.solve_depth = f->F.depth;
+    // setup (count, 3-pass scan, scatter, queue) + elimination + assembly
+    // (counts, scans, scatter, transpose, maxima, row sorts, level order)
+    info.kernel_launches = 6 + 1 + 1 + 3 + 1 + 3 + 1 + 2 + 1 + 1 + 1 + 3 + 1 +
+                           (o.precision == RCHOL_PREC_FP32_FACTOR ? 3 : 0);
     info.lc_ptr = reinterpret_cast<const long long*>(f->F.lc_ptr);
     info.lc_idx = f->F.lc_idx;
     info.lc_val = f->F.lc_val;
@@ -579,6 +609,17 @@ rchol_status factor_from_host_csc(rchol_ctx* ctx, int32_t n, const std::vector<i
     F.n = n;
     F.nnz = nnz;
     std::vector<float> v32(v.begin(), v.end()), cv32(cv.begin(), cv.end()), d32(d.begin(), d.end());
+    // forward levels of the solve DAG and the rows sorted by level
+    std::vector<int32_t> lev((size_t)n, 0);
+    for (int32_t j = 0; j < n; ++j)
+        for (int64_t p = cp[(size_t)j]; p < cp[(size_t)j + 1]; ++p)
+            lev[(size_t)ri[(size_t)p]] = std::max(lev[(size_t)ri[(size_t)p]], lev[(size_t)j] + 1);
+    int32_t depth = 0;
+    for (int32_t x : lev) depth = std::max(depth, x + 1);
+    std::vector<int32_t> lstart((size_t)depth + 1, 0), order((size_t)n);
+    for (int32_t x : lev) lstart[(size_t)x + 1]++;
+    for (int32_t l = 0; l < depth; ++l) lstart[(size_t)l + 1] += lstart[(size_t)l];
+    for (int32_t i = 0; i < n; ++i) order[(size_t)lstart[(size_t)lev[(size_t)i]]++] = i;
     auto up = [&](auto** dst, const auto& src) -> cudaError_t {
         using T = typename std::remove_reference<decltype(src)>::type::value_type;
         cudaError_t e = cudaMalloc((void**)dst, sizeof(T) * std::max<size_t>(src.size(), 1));
@@ -596,6 +637,8 @@ rchol_status factor_from_host_csc(rchol_ctx* ctx, int32_t n, const std::vector<i
     if (e == cudaSuccess) e = up(&F.lr_val32, cv32);
     if (e == cudaSuccess) e = up(&F.diag, d);
     if (e == cudaSuccess) e = up(&F.diag32, d32);
+    if (e == cudaSuccess) e = up(&F.order, order);
+    F.depth = depth;
     if (e != cudaSuccess) {
         free_factor(F);
         delete f;
@@ -612,6 +655,7 @@ rchol_status factor_from_host_csc(rchol_ctx* ctx, int32_t n, const std::vector<i
     f->info.lr_idx = F.lr_idx;
     f->info.lr_val = F.lr_val;
     f->info.diag = F.diag;
+    f->info.solve_depth = depth;
     *out = f;
     return RCHOL_OK;
 }
@@ -714,7 +758,8 @@ rchol_status get_solver(rchol_ctx* ctx, const rchol_factor_t* f, int k) {
     const rchol_opts& o = ctx->o;
     const int fp32 = o.precision == RCHOL_PREC_FP32_FACTOR;
     if (ctx->solver && ctx->solver_f == f && ctx->solver_k == k && ctx->solver_fp32 == fp32 &&
-        ctx->solver_stop == o.stop_rule && ctx->solver_maxit == o.max_iter && ctx->solver_tol == o.tol)
+        ctx->solver_stop == o.stop_rule && ctx->solver_maxit == o.max_iter && ctx->solver_tol == o.tol &&
+        ctx->solver_poll == o.poll_ns)
         return RCHOL_OK;
     drop_solver(ctx);
     rchol::SolveConfig cfg;
@@ -726,6 +771,7 @@ rchol_status get_solver(rchol_ctx* ctx, const rchol_factor_t* f, int k) {
     cfg.unroll = o.unroll;
     cfg.use_graph = o.use_graph != 0;
     cfg.timeout_s = o.timeout_s;
+    cfg.poll_ns = o.poll_ns;
     if (cfg.fp32_factor && !f->F.lr_val32)
         return fail(ctx, RCHOL_ERR_INVALID, "factor has no FP32 copy (factor with RCHOL_PREC_FP32_FACTOR)");
     cudaError_t e = cudaSuccess;
@@ -737,6 +783,7 @@ rchol_status get_solver(rchol_ctx* ctx, const rchol_factor_t* f, int k) {
     ctx->solver_stop = o.stop_rule;
     ctx->solver_maxit = o.max_iter;
     ctx->solver_tol = o.tol;
+    ctx->solver_poll = o.poll_ns;
     return RCHOL_OK;
 }
 
@@ -845,6 +892,32 @@ extern "C" rchol_status rchol_precond_apply(rchol_ctx* ctx, const rchol_factor_t
     if (status != 0) return fail(ctx, RCHOL_ERR_TIMEOUT, "precond apply: a device wait timed out");
     s = stage_out(ctx, ctx->dX, Z, ldb, k, on_device);
     if (s != RCHOL_OK) return s;
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    return RCHOL_OK;
+}
+
+extern "C" rchol_status rchol_profile_solve(rchol_ctx* ctx, const rchol_factor_t* f, int k, int reps,
+                                            float* ms_out) {
+    if (!ctx || !f || !ms_out || reps < 1) return fail(ctx, RCHOL_ERR_INVALID, "bad argument");
+    if (!valid_k(k)) return fail(ctx, RCHOL_ERR_INVALID, "k must be 1, 2, 4, 8, 16 or 32");
+    if (!ctx->have || ctx->At.n != f->F.n) return fail(ctx, RCHOL_ERR_INVALID, "factor does not match the matrix");
+    cudaSetDevice(ctx->device);
+    rchol_status s = get_solver(ctx, f, k);
+    if (s != RCHOL_OK) return s;
+    const size_t elems = (size_t)f->F.n * (size_t)k;
+    s = ensure_stage(ctx, elems);
+    if (s != RCHOL_OK) return s;
+    std::vector<double> b(elems);
+    std::mt19937_64 g(12345);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    for (int c = 0; c < k; ++c) {
+        double mean = 0;
+        for (int32_t i = 0; i < f->F.n; ++i) mean += (b[(size_t)i * k + c] = nd(g));
+        mean /= f->F.n;
+        for (int32_t i = 0; i < f->F.n; ++i) b[(size_t)i * k + c] -= mean;
+    }
+    CK(cudaMemcpyAsync(ctx->dB, b.data(), sizeof(double) * elems, cudaMemcpyHostToDevice, ctx->stream), "upload");
+    CK(rchol::pcg_profile(ctx->solver, ctx->dB, ctx->dX, reps, ms_out), "profile");
     CK(cudaStreamSynchronize(ctx->stream), "sync");
     return RCHOL_OK;
 }

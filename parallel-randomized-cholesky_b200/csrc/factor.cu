@@ -135,6 +135,7 @@ struct FactorArgs {
     int64_t* pstart;
     int32_t* pcnt;
     double* diag;
+    int32_t* level;  // forward level of each row of L (depth in the L-solve DAG)
     unsigned char* gscratch;
     int64_t gscratch_entries;
     int32_t* counters;
@@ -350,12 +351,18 @@ __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_glob
         if (lane == 0) fail(a, kDevCapacity);
         return false;
     }
-    // fills and pool writes must be visible before any neighbour is released
+    // row r of L depends on column k: level[r] >= level[k] + 1.  level[k]
+    // is final here: every column with an entry in row k was eliminated
+    // before k was released.
+    const int lk = ld_relaxed(a.level + k) + 1;
+    // fills, pool writes and levels must be visible before any neighbour is
+    // released
     __threadfence();
     __syncwarp();
     for (int i = lane; i < m; i += kWarp) {
         const int mult = (int)(s.b_aux[i] >> 32);
         const int32_t r = s.b_row[i];
+        atomicMax(a.level + r, lk);
         const int old = atom_add_acq_rel(a.dep + r, -mult);
         if (old == mult) push_ready(a, r);
     }
@@ -500,6 +507,7 @@ cudaError_t launch_init_factor_state(FactorWork& w, cudaStream_t s) {
     if ((e = cudaMemsetAsync(w.chead, 0xff, sizeof(int32_t) * (size_t)w.n, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.cnext, 0xff, sizeof(int32_t) * (size_t)w.nchunks, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.queue, 0xff, sizeof(int32_t) * (size_t)w.n, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(w.level, 0, sizeof(int32_t) * (size_t)w.n, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.counters, 0, sizeof(int32_t) * 16, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.counters64, 0, sizeof(unsigned long long) * 4, s)) != cudaSuccess) return e;
     init_queue_kernel<<<grid_for(w.n, 256), 256, 0, s>>>(w.n, w.dep, w.queue, w.counters);
@@ -544,6 +552,7 @@ cudaError_t launch_factor(FactorWork& w, const FactorLaunch& cfg, cudaStream_t s
     a.pstart = w.pstart;
     a.pcnt = w.pcnt;
     a.diag = w.diag;
+    a.level = w.level;
     a.gscratch = w.gscratch;
     a.gscratch_entries = w.gscratch_entries;
     a.counters = w.counters;

@@ -56,6 +56,7 @@ struct FactorWork {
     int64_t* pstart = nullptr;    // [n] column start in the pool
     int32_t* pcnt = nullptr;      // [n] merged neighbour count
     double* diag = nullptr;       // [n] D
+    int32_t* level = nullptr;     // [n] forward level (longest dependency chain) of each row of L
     // per-warp scratch for vertices that do not fit the shared-memory slab
     int64_t gscratch_entries = 0; // entries per warp
     unsigned char* gscratch = nullptr;
@@ -83,6 +84,10 @@ struct DevFactor {
     float* lr_val32 = nullptr;
     double* diag = nullptr;
     float* diag32 = nullptr;
+    // rows in non-decreasing forward level: the forward solve walks this
+    // order, the backward solve walks it reversed (both are topological)
+    int32_t* order = nullptr;
+    int32_t depth = 0;        // number of levels of the forward solve DAG
 };
 
 struct FactorLaunch {
@@ -128,6 +133,7 @@ struct SolveConfig {
     int stop_rule = 0;         // 0 relres (true residual), 1 precond ratio, 2 abs r^2
     int unroll = 4;            // iterations per captured graph launch
     bool use_graph = true;
+    int poll_ns = 0;           // back-off between polls in the triangular solves
     double timeout_s = 20.0;
 };
 
@@ -151,6 +157,8 @@ PcgSolver* pcg_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cf
                       cudaStream_t stream, cudaError_t* err);
 cudaError_t pcg_solve(PcgSolver* s, const double* dB, double* dX, SolveResult* res);
 void pcg_destroy(PcgSolver* s);
+// Mean device time of spmv_update / fwd / bwd over `reps` iterations.
+cudaError_t pcg_profile(PcgSolver* s, const double* dB, double* dX, int reps, float* ms_out);
 
 // Kernel-level entry points used by tests/bench (one operator application).
 cudaError_t spmv_f64(const DevCsc& A, const double* x, double* y, int k, cudaStream_t s);

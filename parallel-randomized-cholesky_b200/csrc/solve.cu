@@ -75,6 +75,7 @@ struct SolveArgs {
     const int32_t* __restrict__ lc_idx;
     const void* __restrict__ lc_val;
     const void* __restrict__ diag;
+    const int32_t* __restrict__ order;  // rows by non-decreasing forward level
     // vectors (n x K row-major)
     const double* __restrict__ b;
     double* x;
@@ -93,6 +94,7 @@ struct SolveArgs {
     int stop_rule;
     int update;              // fwd: apply the x/r update
     int reduce;              // compute reductions / scalars
+    int poll_ns;             // back-off between polls of a pending value
     unsigned long long timeout_ns;
 };
 
@@ -154,14 +156,15 @@ __device__ __forceinline__ bool timed_out(unsigned long long t0, unsigned long l
 
 // Poll a solution component until it has been produced.
 __device__ __forceinline__ double wait_value(const double* p, unsigned long long t0, unsigned long long limit,
-                                             int* status, bool& ok) {
+                                             int* status, bool& ok, int poll_ns) {
     double v = ld_relaxed_f64(p);
     if (!is_pending(v)) return v;
     unsigned spins = 0;
     while (true) {
+        if (poll_ns > 0) __nanosleep(poll_ns);
         v = ld_relaxed_f64(p);
         if (!is_pending(v)) return v;
-        if ((++spins & 1023u) == 0 && timed_out(t0, limit)) {
+        if ((++spins & 255u) == 0 && timed_out(t0, limit)) {
             raise_error(status, kDevTimeout);
             ok = false;
             return 0.0;
@@ -295,7 +298,8 @@ __global__ void __launch_bounds__(kBlock) fwd_kernel(SolveArgs a) {
     for (int c = 0; c < K; ++c) acc[c] = 0.0;
     const unsigned long long t0 = global_timer_ns();
     bool ok = true;
-    for (int64_t i = group; i < a.n && ok; i += ngroups) {
+    for (int64_t t = group; t < a.n && ok; t += ngroups) {
+        const int64_t i = a.order ? a.order[t] : t;
         const int64_t s = a.lr_ptr[i], e = a.lr_ptr[i + 1];
         if (K == 1) {
             double ri = a.r[i];
@@ -311,7 +315,7 @@ __global__ void __launch_bounds__(kBlock) fwd_kernel(SolveArgs a) {
             double sum = 0.0;
             for (int64_t pp = s + gl; pp < e; pp += G) {
                 const double l = to_d(lv[pp]);
-                const double yj = wait_value(a.y + a.lr_idx[pp], t0, a.timeout_ns, &a.sc->status, ok);
+                const double yj = wait_value(a.y + a.lr_idx[pp], t0, a.timeout_ns, &a.sc->status, ok, a.poll_ns);
                 sum += l * yj;
             }
 #pragma unroll
@@ -337,7 +341,7 @@ __global__ void __launch_bounds__(kBlock) fwd_kernel(SolveArgs a) {
             for (int64_t pp = s; pp < e; ++pp) {
                 const double l = to_d(lv[pp]);
                 const double yj =
-                    wait_value(a.y + (size_t)a.lr_idx[pp] * K + c, t0, a.timeout_ns, &a.sc->status, ok);
+                    wait_value(a.y + (size_t)a.lr_idx[pp] * K + c, t0, a.timeout_ns, &a.sc->status, ok, a.poll_ns);
                 sum += l * yj;
             }
             if (a.z) a.z[o] = pending_value();
@@ -398,7 +402,7 @@ __global__ void __launch_bounds__(kBlock) bwd_kernel(SolveArgs a) {
     const unsigned long long t0 = global_timer_ns();
     bool ok = true;
     for (int64_t g = group; g < a.n && ok; g += ngroups) {
-        const int64_t j = a.n - 1 - g;
+        const int64_t j = a.order ? a.order[a.n - 1 - g] : a.n - 1 - g;
         const int64_t s = a.lc_ptr[j], e = a.lc_ptr[j + 1];
         const double dj = to_d(dv[j]);
         if (K == 1) {
@@ -407,7 +411,7 @@ __global__ void __launch_bounds__(kBlock) bwd_kernel(SolveArgs a) {
             double sum = 0.0;
             for (int64_t pp = s + gl; pp < e; pp += G) {
                 const double l = to_d(lv[pp]);
-                const double zi = wait_value(a.z + a.lc_idx[pp], t0, a.timeout_ns, &a.sc->status, ok);
+                const double zi = wait_value(a.z + a.lc_idx[pp], t0, a.timeout_ns, &a.sc->status, ok, a.poll_ns);
                 sum += l * zi;
             }
 #pragma unroll
@@ -426,7 +430,7 @@ __global__ void __launch_bounds__(kBlock) bwd_kernel(SolveArgs a) {
             for (int64_t pp = s; pp < e; ++pp) {
                 const double l = to_d(lv[pp]);
                 const double zi =
-                    wait_value(a.z + (size_t)a.lc_idx[pp] * K + c, t0, a.timeout_ns, &a.sc->status, ok);
+                    wait_value(a.z + (size_t)a.lc_idx[pp] * K + c, t0, a.timeout_ns, &a.sc->status, ok, a.poll_ns);
                 sum += l * zi;
             }
             const double zj = t - sum;
@@ -626,6 +630,7 @@ class PcgSolver {
         a.lc_idx = F.lc_idx;
         a.lc_val = cfg.fp32_factor ? (const void*)F.lc_val32 : (const void*)F.lc_val;
         a.diag = cfg.fp32_factor ? (const void*)F.diag32 : (const void*)F.diag;
+        a.order = F.order;
         a.b = b;
         a.x = x;
         a.r = r;
@@ -641,6 +646,7 @@ class PcgSolver {
         a.stop_rule = cfg.stop_rule;
         a.update = 1;
         a.reduce = 1;
+        a.poll_ns = cfg.poll_ns;
         a.timeout_ns = (unsigned long long)(cfg.timeout_s * 1e9);
         return a;
     }
@@ -882,6 +888,42 @@ cudaError_t pcg_solve(PcgSolver* s, const double* dB, double* dX, SolveResult* r
     return cudaSuccess;
 }
 
+// Per-kernel device time of the iteration kernels: starts a solve of dB
+// (tolerance 0, so nothing converges), then times `reps` iterations with an
+// event between every launch.  ms_out[0..2] = mean spmv_update, fwd, bwd.
+cudaError_t pcg_profile(PcgSolver* s, const double* dB, double* dX, int reps, float* ms_out) {
+    SolveConfig keep = s->cfg;
+    s->cfg.tol = 0.0;
+    s->cfg.max_iter = 1 << 30;
+    SolveArgs a = s->args(dB, dX);
+    cudaError_t e;
+    if ((e = s->launch(s->k_init, s->grid_vec, a)) != cudaSuccess) return e;
+    if ((e = s->launch_start(dB, dX)) != cudaSuccess) return e;
+    cudaEvent_t ev[4];
+    for (auto& x : ev) cudaEventCreate(&x);
+    double acc[3] = {0, 0, 0};
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+        SolveArgs it = s->args(dB, dX);
+        cudaEventRecord(ev[0], s->stream);
+        e = s->launch(s->k_spmv, s->grid_spmv, it);
+        cudaEventRecord(ev[1], s->stream);
+        if (e == cudaSuccess) e = s->launch(s->k_fwd, s->grid_fwd, it);
+        cudaEventRecord(ev[2], s->stream);
+        if (e == cudaSuccess) e = s->launch(s->k_bwd, s->grid_bwd, it);
+        cudaEventRecord(ev[3], s->stream);
+        cudaEventSynchronize(ev[3]);
+        float m;
+        for (int q = 0; q < 3; ++q) {
+            cudaEventElapsedTime(&m, ev[q], ev[q + 1]);
+            acc[q] += m;
+        }
+    }
+    for (auto& x : ev) cudaEventDestroy(x);
+    for (int q = 0; q < 3; ++q) ms_out[q] = (float)(acc[q] / std::max(reps, 1));
+    s->cfg = keep;
+    return e;
+}
+
 // ---- single operator applications ----------------------------------------
 
 namespace {
@@ -943,6 +985,7 @@ static cudaError_t precond_apply_t(const DevFactor& F, const double* r, double* 
     a.lc_idx = F.lc_idx;
     a.lc_val = std::is_same<TV, float>::value ? (const void*)F.lc_val32 : (const void*)F.lc_val;
     a.diag = std::is_same<TV, float>::value ? (const void*)F.diag32 : (const void*)F.diag;
+    a.order = F.order;
     a.r = const_cast<double*>(r);
     a.y = y;
     a.z = z;

@@ -30,7 +30,7 @@ EXPORTS = [
     "rchol_last_error", "rchol_load_mtx", "rchol_set_triplets", "rchol_set_csc", "rchol_csc_from_triplets",
     "rchol_read_mtx", "rchol_matrix_info", "rchol_matrix_copy_to_host", "rchol_factor", "rchol_factor_get_info",
     "rchol_factor_copy_to_host", "rchol_factor_write", "rchol_factor_read", "rchol_factor_from_csr_upper",
-    "rchol_factor_free", "rchol_pcg_solve", "rchol_precond_apply", "rchol_spmv", "rchol_factorization_driver",
+    "rchol_factor_free", "rchol_pcg_solve", "rchol_precond_apply", "rchol_profile_solve", "rchol_spmv", "rchol_factorization_driver",
     "rchol_prepare_and_solve", "rchol_generate", "rchol_free_host", "rchol_write_mtx",
 ]
 
@@ -46,7 +46,7 @@ class Opts(C.Structure):
                 ("warps_per_block", C.c_int), ("slab_entries", C.c_int), ("bucket_cap", C.c_int),
                 ("pool_mult", C.c_double), ("max_iter", C.c_int), ("tol", C.c_double), ("stop_rule", C.c_int),
                 ("unroll", C.c_int), ("use_graph", C.c_int), ("device", C.c_int), ("timeout_s", C.c_double),
-                ("verbose", C.c_int)]
+                ("verbose", C.c_int), ("poll_ns", C.c_int)]
 
 
 class FactorInfo(C.Structure):
@@ -55,6 +55,7 @@ class FactorInfo(C.Structure):
                 ("big_vertices", C.c_int), ("overflow_fills", C.c_int), ("chunks_used", C.c_int),
                 ("factor_grid", C.c_int), ("ms_setup", C.c_float), ("ms_factor", C.c_float),
                 ("ms_assemble", C.c_float), ("attempts", C.c_int),
+                ("solve_depth", C.c_int), ("kernel_launches", C.c_int),
                 ("lc_ptr", C.c_void_p), ("lc_idx", C.c_void_p), ("lc_val", C.c_void_p),
                 ("lr_ptr", C.c_void_p), ("lr_idx", C.c_void_p), ("lr_val", C.c_void_p), ("diag", C.c_void_p)]
 
@@ -112,6 +113,7 @@ def lib():
         L.rchol_pcg_solve.argtypes = [vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, C.POINTER(SolveInfo)]
         L.rchol_precond_apply.argtypes = [vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int]
         L.rchol_spmv.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.c_int]
+        L.rchol_profile_solve.argtypes = [vp, vp, C.c_int, C.c_int, C.POINTER(C.c_float)]
         L.rchol_factorization_driver.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_int]
         L.rchol_prepare_and_solve.argtypes = [C.c_int, C.c_longlong, vp, vp, vp, vp, vp, vp, vp, C.c_double,
                                               C.c_int, C.c_longlong, C.c_int, vp, C.POINTER(SolveInfo)]
@@ -366,6 +368,12 @@ class Context:
         _check(lib().rchol_precond_apply(self.h, factor.h, k, Rf.ctypes.data_as(C.c_void_p),
                                          Z.ctypes.data_as(C.c_void_p), n, 0, int(fp32)), self.h)
         return Z[:, 0].copy() if vec else np.ascontiguousarray(Z)
+
+    def profile_solve(self, factor, k=1, reps=5):
+        """Mean ms of (spmv_update, fwd, bwd) per iteration."""
+        ms = (C.c_float * 3)()
+        _check(lib().rchol_profile_solve(self.h, factor.h, k, reps, ms), self.h)
+        return list(ms)
 
     def spmv(self, X):
         X = np.asarray(X, np.float64)
