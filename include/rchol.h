@@ -64,6 +64,8 @@ typedef struct rchol_opts {
     double timeout_s;         /* bound on every device-side wait */
     int verbose;              /* print phase timings (the reference's stdout) */
     int poll_ns;              /* back-off (ns) between polls in the triangular solves */
+    int sched_epl;            /* triangular-solve schedule: matrix entries per lane (1..64) */
+    int exact_bwd_levels;     /* order the backward solve by its true DAG levels */
 } rchol_opts;
 
 typedef struct rchol_factor_info {

@@ -179,17 +179,125 @@ __global__ void sort_long_rows_kernel(const int32_t* __restrict__ rows, int32_t 
     }
 }
 
-__global__ void level_hist_kernel(const int32_t* __restrict__ level, int32_t n, int32_t* hist) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) atomicAdd(hist + level[i], 1);
+// lane class of a row (log2 of its lane-group size) and its bucket
+__device__ __forceinline__ int lane_class(int64_t len, int epl) {
+    int64_t need = (len + epl - 1) / epl;
+    int c = 0;
+    while (c < kLaneClasses - 1 && (1ll << c) < need) ++c;
+    return c;
+}
+__device__ __forceinline__ int sched_key(int level, int64_t len, int epl) {
+    return kLaneClasses * level + lane_class(len, epl);
 }
 
-__global__ void level_scatter_kernel(const int32_t* __restrict__ level, int32_t n, const int32_t* __restrict__ start,
+__global__ void sched_hist_kernel(const int32_t* __restrict__ level, const int64_t* __restrict__ ptr, int32_t n,
+                                  int32_t depth, int backward, int epl, int32_t* hist) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        int l = backward ? depth - 1 - level[i] : level[i];
+        atomicAdd(hist + sched_key(l, ptr[i + 1] - ptr[i], epl), 1);
+    }
+}
+
+// Longest path from each row to a sink of the L^T solve DAG:
+// levb[j] = 1 + max over i in column j of levb[i] (0 for an empty column).
+// Rows are visited in a topological order (`order`) by persistent warps
+// round-robin; each waits for the levels it needs (-1 = pending), bounded.
+__global__ void bwd_level_kernel(int32_t n, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                 const int32_t* __restrict__ order, int32_t* levb, int32_t* status,
+                                 unsigned long long timeout_ns) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const unsigned long long t0 = global_timer_ns();
+    bool ok = true;
+    for (int64_t t = warp; t < n && ok; t += nwarps) {
+        const int32_t j = order[t];
+        int m = -1;
+        for (int64_t p = ptr[j] + lane; p < ptr[j + 1]; p += 32) {
+            int v;
+            unsigned spins = 0;
+            while ((v = ld_relaxed(levb + idx[p])) < 0) {
+                if ((++spins & 255u) == 0 && global_timer_ns() - t0 > timeout_ns) {
+                    raise_error(status, kDevTimeout);
+                    ok = false;
+                    break;
+                }
+            }
+            m = max(m, v);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(kFull, m, o));
+        if (lane == 0) atomicExch(levb + j, m + 1);
+        ok = __all_sync(kFull, ok);
+    }
+}
+
+__global__ void sched_scatter_kernel(const int32_t* __restrict__ level, const int64_t* __restrict__ ptr, int32_t n,
+                                     int32_t depth, int backward, int epl, const int32_t* __restrict__ start,
                                      int32_t* cursor, int32_t* order) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        int l = level[i];
-        order[start[l] + atomicAdd(cursor + l, 1)] = (int32_t)i;
+        int l = backward ? depth - 1 - level[i] : level[i];
+        int k = sched_key(l, ptr[i + 1] - ptr[i], epl);
+        order[start[k] + atomicAdd(cursor + k, 1)] = (int32_t)i;
+    }
+}
+
+// tasks per bucket: rows of class c pack 32 >> c to a warp
+__global__ void sched_task_count_kernel(const int32_t* __restrict__ hist, int32_t nb, int32_t* tcount) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += stride) {
+        const int per = 32 >> (int)(b % kLaneClasses);
+        tcount[b] = (hist[b] + per - 1) / per;
+    }
+}
+
+__global__ void sched_task_emit_kernel(const int32_t* __restrict__ hist, const int32_t* __restrict__ start,
+                                       const int32_t* __restrict__ tstart, int32_t nb, int32_t ntasks, int2* tasks) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntasks; t += stride) {
+        int lo = 0, hi = nb - 1;  // last bucket with tstart <= t
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (tstart[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const int b = lo;
+        const int cls = b % kLaneClasses;
+        const int per = 32 >> cls;
+        const int q = (int)(t - tstart[b]);
+        int2 d;
+        d.x = start[b] + per * q;
+        d.y = min(per, hist[b] - per * q) | (cls << 8);
+        tasks[t] = d;
+    }
+}
+
+// rows in schedule order: position p copies row order[p] of (ptr, idx, val)
+__global__ void permute_len_kernel(int32_t n, const int32_t* __restrict__ order, const int64_t* __restrict__ ptr,
+                                   int32_t* len) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+        const int32_t i = order[p];
+        len[p] = (int32_t)(ptr[i + 1] - ptr[i]);
+    }
+}
+
+__global__ void permute_rows_kernel(int32_t n, const int32_t* __restrict__ order, const int64_t* __restrict__ ptr,
+                                    const int32_t* __restrict__ idx, const double* __restrict__ val,
+                                    const float* __restrict__ val32, const int64_t* __restrict__ optr, int32_t* oidx,
+                                    double* oval, float* oval32) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); p < n; p += warps) {
+        const int32_t i = order[p];
+        const int64_t s = ptr[i], len = ptr[i + 1] - s, o = optr[p];
+        for (int64_t q = lane; q < len; q += 32) {
+            oidx[o + q] = idx[s + q];
+            oval[o + q] = val[s + q];
+            if (val32) oval32[o + q] = val32[s + q];
+        }
     }
 }
 
@@ -261,15 +369,52 @@ cudaError_t dmalloc(T** p, int64_t n) {
         if (e__ != cudaSuccess) return e__; \
     } while (0)
 
-cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp32, DevFactor& f, cudaStream_t s) {
+// (Re)allocate a persistent buffer that shares the capacity `cap` with its
+// siblings: kept when present and the shared capacity did not grow.
+template <typename T>
+static cudaError_t realloc_if(T** p, bool grow, int64_t cap) {
+    if (*p && !grow) return cudaSuccess;
+    cudaFree(*p);
+    *p = nullptr;
+    return cudaMalloc((void**)p, sizeof(T) * (size_t)(cap > 0 ? cap : 1));
+}
+
+// Reuse a buffer with its own capacity when it suffices, else reallocate.
+template <typename T>
+static cudaError_t ensure(T** p, int64_t& cap, int64_t need) {
+    if (*p && cap >= need) return cudaSuccess;
+    cudaFree(*p);
+    *p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * (size_t)(need > 0 ? need : 1));
+    if (e == cudaSuccess) cap = need;
+    return e;
+}
+
+cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp32, int epl, bool exact_bwd,
+                            double timeout_s, Scratch& sc, DevFactor& f, cudaStream_t s) {
     const int32_t nout = trim_ground ? w.n - 1 : w.n;
     const int32_t ground = trim_ground ? w.n - 1 : -1;
     f.n = nout;
-    int32_t* cnt = nullptr;
+    sc.reset();
+    // temporaries of this call: counts, scan scratch, long-row list, status
+    RCHOL_TRY(sc.reserve((size_t)nout * 40 + 4 * scan_tmp_bytes(nout) + (16u << 20)));
+    int32_t *cnt = nullptr, *dsc = nullptr, *long_rows = nullptr;
     void* tmp = nullptr;
-    RCHOL_TRY(dmalloc(&cnt, nout));
-    RCHOL_TRY(cudaMalloc(&tmp, scan_tmp_bytes(nout)));
-    RCHOL_TRY(dmalloc(&f.lc_ptr, (int64_t)nout + 1));
+    RCHOL_TRY(sc.get(&cnt, nout));
+    RCHOL_TRY(sc.get(&long_rows, nout));
+    RCHOL_TRY(sc.get(&dsc, 4));
+    RCHOL_TRY(sc.get((char**)&tmp, (int64_t)scan_tmp_bytes(nout)));
+    // per-row arrays share cap_n (n+1 entries)
+    const bool grow_n = f.cap_n < (int64_t)nout + 1;
+    const int64_t capn = std::max<int64_t>(f.cap_n, (int64_t)nout + 1);
+    RCHOL_TRY(realloc_if(&f.lc_ptr, grow_n, capn));
+    RCHOL_TRY(realloc_if(&f.lr_ptr, grow_n, capn));
+    RCHOL_TRY(realloc_if(&f.diag, grow_n, capn));
+    RCHOL_TRY(realloc_if(&f.order_f, grow_n, capn));
+    RCHOL_TRY(realloc_if(&f.order_b, grow_n, capn));
+    if (make_fp32) RCHOL_TRY(realloc_if(&f.diag32, grow_n, capn));
+    f.cap_n = capn;
     col_counts_kernel<<<grid_for(nout, 256), 256, 0, s>>>(nout, ground, w.pcnt, w.pstart, w.prow, cnt);
     RCHOL_TRY(cudaGetLastError());
     RCHOL_TRY(exclusive_scan_i32_to_i64(cnt, f.lc_ptr, nout, tmp, s));
@@ -277,12 +422,24 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
     RCHOL_TRY(cudaMemcpyAsync(&nnz, f.lc_ptr + nout, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     RCHOL_TRY(cudaStreamSynchronize(s));
     f.nnz = nnz;
-    RCHOL_TRY(dmalloc(&f.lc_idx, nnz));
-    RCHOL_TRY(dmalloc(&f.lc_val, nnz));
-    RCHOL_TRY(dmalloc(&f.lr_idx, nnz));
-    RCHOL_TRY(dmalloc(&f.lr_val, nnz));
-    RCHOL_TRY(dmalloc(&f.lr_ptr, (int64_t)nout + 1));
-    RCHOL_TRY(dmalloc(&f.diag, nout));
+    // per-entry arrays share cap_nnz
+    const bool grow_z = f.cap_nnz < nnz;
+    const int64_t capz = std::max<int64_t>(f.cap_nnz, nnz);
+    RCHOL_TRY(realloc_if(&f.lc_idx, grow_z, capz));
+    RCHOL_TRY(realloc_if(&f.lc_val, grow_z, capz));
+    RCHOL_TRY(realloc_if(&f.lr_idx, grow_z, capz));
+    RCHOL_TRY(realloc_if(&f.lr_val, grow_z, capz));
+    if (make_fp32) {
+        RCHOL_TRY(realloc_if(&f.lc_val32, grow_z, capz));
+        RCHOL_TRY(realloc_if(&f.lr_val32, grow_z, capz));
+    } else {
+        cudaFree(f.lc_val32);
+        cudaFree(f.lr_val32);
+        cudaFree(f.diag32);
+        f.lc_val32 = f.lr_val32 = nullptr;
+        f.diag32 = nullptr;
+    }
+    f.cap_nnz = capz;
     RCHOL_TRY(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (size_t)(nout > 0 ? nout : 1), s));
     scatter_cols_kernel<<<grid_for((int64_t)nout * 32, 256), 256, 0, s>>>(nout, f.lc_ptr, w.pstart, w.prow, w.pval,
                                                                           f.lc_idx, f.lc_val, cnt);
@@ -295,11 +452,7 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
     // deterministic row order: warp sort for short rows, CTA sort for long ones
     const int sort_block = 256;
     const int sort_grid = 148 * 4;
-    int32_t* dsc = nullptr;  // [0] long-row count, [1] max row length, [2] max level
-    int32_t* long_rows = nullptr;
-    RCHOL_TRY(dmalloc(&dsc, 4));
-    RCHOL_TRY(dmalloc(&long_rows, nout));
-    RCHOL_TRY(cudaMemsetAsync(dsc, 0, sizeof(int32_t) * 4, s));
+    RCHOL_TRY(cudaMemsetAsync(dsc, 0, sizeof(int32_t) * 4, s));  // long rows, max row, max level
     max_kernel<<<grid_for(nout, 256), 256, 0, s>>>(cnt, nout, dsc + 1);
     max_kernel<<<grid_for(nout, 256), 256, 0, s>>>(w.level, nout, dsc + 2);
     sort_rows_kernel<<<sort_grid, sort_block, 0, s>>>(nout, f.lr_ptr, f.lr_idx, f.lr_val, long_rows, dsc);
@@ -313,8 +466,8 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
     const int lgrid = hs[0] > 0 ? std::min(hs[0], 148 * 2) : 1;
     if (hs[1] > kBlockSortCap) {
         while (gcap < hs[1]) gcap <<= 1;
-        RCHOL_TRY(dmalloc(&gkey, (int64_t)lgrid * gcap));
-        RCHOL_TRY(dmalloc(&gval, (int64_t)lgrid * gcap));
+        RCHOL_TRY(sc.get(&gkey, (int64_t)lgrid * gcap));
+        RCHOL_TRY(sc.get(&gval, (int64_t)lgrid * gcap));
     }
     if (hs[0] > 0) {
         const size_t smem = (size_t)kBlockSortCap * 12;
@@ -323,42 +476,138 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
                                                         gcap, w.counters + 3);
         RCHOL_TRY(cudaGetLastError());
     }
-    // rows in non-decreasing forward level
-    const int32_t depth = hs[2] + 1;
-    f.depth = depth;
-    int32_t *hist = nullptr, *lstart = nullptr;
-    RCHOL_TRY(dmalloc(&hist, depth));
-    RCHOL_TRY(dmalloc(&lstart, (int64_t)depth + 1));
-    RCHOL_TRY(dmalloc(&f.order, nout));
-    void* tmp2 = nullptr;
-    RCHOL_TRY(cudaMalloc(&tmp2, scan_tmp_bytes(depth)));
-    RCHOL_TRY(cudaMemsetAsync(hist, 0, sizeof(int32_t) * (size_t)depth, s));
-    level_hist_kernel<<<grid_for(nout, 256), 256, 0, s>>>(w.level, nout, hist);
-    RCHOL_TRY(exclusive_scan_i32_to_i32(hist, lstart, depth, tmp2, s));
-    RCHOL_TRY(cudaMemsetAsync(hist, 0, sizeof(int32_t) * (size_t)depth, s));
-    level_scatter_kernel<<<grid_for(nout, 256), 256, 0, s>>>(w.level, nout, lstart, hist, f.order);
-    RCHOL_TRY(cudaGetLastError());
+    f.depth = hs[2] + 1;
     RCHOL_TRY(cudaMemcpyAsync(f.diag, w.diag, sizeof(double) * (size_t)nout, cudaMemcpyDeviceToDevice, s));
     if (make_fp32) {
-        RCHOL_TRY(dmalloc(&f.lc_val32, nnz));
-        RCHOL_TRY(dmalloc(&f.lr_val32, nnz));
-        RCHOL_TRY(dmalloc(&f.diag32, nout));
         to_f32_kernel<<<grid_for(nnz, 256), 256, 0, s>>>(f.lc_val, f.lc_val32, nnz);
         to_f32_kernel<<<grid_for(nnz, 256), 256, 0, s>>>(f.lr_val, f.lr_val32, nnz);
         to_f32_kernel<<<grid_for(nout, 256), 256, 0, s>>>(f.diag, f.diag32, nout);
         RCHOL_TRY(cudaGetLastError());
     }
+    RCHOL_TRY(build_solve_schedule(f, w.level, epl, exact_bwd, timeout_s, sc, s));
     RCHOL_TRY(cudaStreamSynchronize(s));
-    cudaFree(gkey);
-    cudaFree(gval);
-    cudaFree(cnt);
-    cudaFree(tmp);
-    cudaFree(tmp2);
-    cudaFree(hist);
-    cudaFree(lstart);
-    cudaFree(dsc);
-    cudaFree(long_rows);
+    sc.reset();
     return cudaSuccess;
+}
+
+// Orders the rows by (level, lane class) into `order` (capacity n, owned by
+// the factor) and emits the task list into `*tasks` (grown as needed).
+static cudaError_t build_one_schedule(const int32_t* level, const int64_t* ptr, int32_t n, int32_t depth, int backward,
+                                      int epl, Scratch& sc, int32_t* order, int2** tasks, int64_t& tcap,
+                                      int32_t* ntasks, cudaStream_t s) {
+    const int32_t nb = kLaneClasses * depth;
+    int32_t *hist = nullptr, *start = nullptr, *tcount = nullptr, *tstart = nullptr;
+    void* tmp = nullptr;
+    RCHOL_TRY(sc.get(&hist, nb));
+    RCHOL_TRY(sc.get(&start, (int64_t)nb + 1));
+    RCHOL_TRY(sc.get(&tcount, nb));
+    RCHOL_TRY(sc.get(&tstart, (int64_t)nb + 1));
+    RCHOL_TRY(sc.get((char**)&tmp, (int64_t)scan_tmp_bytes(nb)));
+    RCHOL_TRY(cudaMemsetAsync(hist, 0, sizeof(int32_t) * (size_t)nb, s));
+    sched_hist_kernel<<<grid_for(n, 256), 256, 0, s>>>(level, ptr, n, depth, backward, epl, hist);
+    RCHOL_TRY(exclusive_scan_i32_to_i32(hist, start, nb, tmp, s));
+    sched_task_count_kernel<<<grid_for(nb, 256), 256, 0, s>>>(hist, nb, tcount);
+    RCHOL_TRY(exclusive_scan_i32_to_i32(tcount, tstart, nb, tmp, s));
+    int32_t nt = 0;
+    RCHOL_TRY(cudaMemcpyAsync(&nt, tstart + nb, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    RCHOL_TRY(cudaStreamSynchronize(s));
+    *ntasks = nt;
+    RCHOL_TRY(ensure(tasks, tcap, (int64_t)nt));
+    sched_task_emit_kernel<<<grid_for(nt, 256), 256, 0, s>>>(hist, start, tstart, nb, nt, *tasks);
+    RCHOL_TRY(cudaMemsetAsync(tcount, 0, sizeof(int32_t) * (size_t)nb, s));
+    sched_scatter_kernel<<<grid_for(n, 256), 256, 0, s>>>(level, ptr, n, depth, backward, epl, start, tcount, order);
+    return cudaGetLastError();
+}
+
+static cudaError_t build_layout(int32_t n, const int32_t* order, const int64_t* ptr, const int32_t* idx,
+                                const double* val, const float* val32, int64_t* optr, int32_t* oidx, double* oval,
+                                float* oval32, Scratch& sc, cudaStream_t s) {
+    int32_t* len = nullptr;
+    void* tmp = nullptr;
+    RCHOL_TRY(sc.get(&len, n));
+    RCHOL_TRY(sc.get((char**)&tmp, (int64_t)scan_tmp_bytes(n)));
+    permute_len_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, order, ptr, len);
+    RCHOL_TRY(exclusive_scan_i32_to_i64(len, optr, n, tmp, s));
+    permute_rows_kernel<<<grid_for((int64_t)n * 32, 256), 256, 0, s>>>(n, order, ptr, idx, val, val32, optr, oidx,
+                                                                        oval, oval32);
+    return cudaGetLastError();
+}
+
+// The solve layouts (schedule-ordered copies of Lr and Lc) for the orders
+// already built; FP32 values are copied when the factor has them.
+static cudaError_t build_layouts(DevFactor& f, Scratch& sc, cudaStream_t s) {
+    const bool grow_n = f.cap_ln < (int64_t)f.n + 1;
+    const int64_t capn = std::max<int64_t>(f.cap_ln, (int64_t)f.n + 1);
+    RCHOL_TRY(realloc_if(&f.sf_ptr, grow_n, capn));
+    RCHOL_TRY(realloc_if(&f.sb_ptr, grow_n, capn));
+    f.cap_ln = capn;
+    const bool fp32 = f.lr_val32 != nullptr;
+    const bool grow_z = f.cap_lz < f.nnz || (fp32 && !f.sf_val32);
+    const int64_t capz = std::max<int64_t>(f.cap_lz, f.nnz);
+    RCHOL_TRY(realloc_if(&f.sf_idx, grow_z, capz));
+    RCHOL_TRY(realloc_if(&f.sf_val, grow_z, capz));
+    RCHOL_TRY(realloc_if(&f.sb_idx, grow_z, capz));
+    RCHOL_TRY(realloc_if(&f.sb_val, grow_z, capz));
+    if (fp32) {
+        RCHOL_TRY(realloc_if(&f.sf_val32, grow_z, capz));
+        RCHOL_TRY(realloc_if(&f.sb_val32, grow_z, capz));
+    } else {
+        cudaFree(f.sf_val32);
+        cudaFree(f.sb_val32);
+        f.sf_val32 = f.sb_val32 = nullptr;
+    }
+    f.cap_lz = capz;
+    RCHOL_TRY(build_layout(f.n, f.order_f, f.lr_ptr, f.lr_idx, f.lr_val, f.lr_val32, f.sf_ptr, f.sf_idx, f.sf_val,
+                           f.sf_val32, sc, s));
+    RCHOL_TRY(build_layout(f.n, f.order_b, f.lc_ptr, f.lc_idx, f.lc_val, f.lc_val32, f.sb_ptr, f.sb_idx, f.sb_val,
+                           f.sb_val32, sc, s));
+    return cudaSuccess;
+}
+
+cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bool exact_bwd, double timeout_s,
+                                 Scratch& sc, cudaStream_t s) {
+    if (epl < 1) epl = 1;
+    {
+        const bool grow_n = f.cap_n < (int64_t)f.n + 1;
+        const int64_t capn = std::max<int64_t>(f.cap_n, (int64_t)f.n + 1);
+        RCHOL_TRY(realloc_if(&f.order_f, grow_n, capn));
+        RCHOL_TRY(realloc_if(&f.order_b, grow_n, capn));
+        if (grow_n && f.cap_n > 0) return cudaErrorInvalidValue;  // siblings would be undersized
+        f.cap_n = capn;
+    }
+    // forward: rows of Lr; backward: rows of L^T = columns of Lc
+    RCHOL_TRY(build_one_schedule(level, f.lr_ptr, f.n, f.depth, 0, epl, sc, f.order_f, &f.tasks_f, f.cap_tf,
+                                 &f.ntasks_f, s));
+    RCHOL_TRY(build_one_schedule(level, f.lc_ptr, f.n, f.depth, 1, epl, sc, f.order_b, &f.tasks_b, f.cap_tb,
+                                 &f.ntasks_b, s));
+    f.depth_b = f.depth;
+    if (!exact_bwd || f.n == 0) {
+        RCHOL_TRY(build_layouts(f, sc, s));
+        return cudaStreamSynchronize(s);
+    }
+    // true backward levels, visited in the reversed-forward order just built
+    int32_t *levb = nullptr, *st = nullptr;
+    RCHOL_TRY(sc.get(&levb, f.n));
+    RCHOL_TRY(sc.get(&st, 2));
+    RCHOL_TRY(cudaMemsetAsync(levb, 0xff, sizeof(int32_t) * (size_t)f.n, s));
+    RCHOL_TRY(cudaMemsetAsync(st, 0, sizeof(int32_t) * 2, s));
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bwd_level_kernel, 256, 0);
+    bwd_level_kernel<<<std::max(1, per_sm * sms), 256, 0, s>>>(f.n, f.lc_ptr, f.lc_idx, f.order_b, levb, st,
+                                                              (unsigned long long)(timeout_s * 1e9));
+    RCHOL_TRY(cudaGetLastError());
+    max_kernel<<<grid_for(f.n, 256), 256, 0, s>>>(levb, f.n, st + 1);
+    int32_t hs[2] = {0, 0};
+    RCHOL_TRY(cudaMemcpyAsync(hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s));
+    RCHOL_TRY(cudaStreamSynchronize(s));
+    if (hs[0] != 0) return cudaErrorLaunchTimeout;
+    f.depth_b = hs[1] + 1;
+    RCHOL_TRY(build_one_schedule(levb, f.lc_ptr, f.n, f.depth_b, 0, epl, sc, f.order_b, &f.tasks_b, f.cap_tb,
+                                 &f.ntasks_b, s));
+    RCHOL_TRY(build_layouts(f, sc, s));
+    return cudaStreamSynchronize(s);
 }
 
 cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, cudaStream_t s) {

@@ -37,6 +37,9 @@ struct rchol_ctx {
     const rchol_factor_t* solver_f = nullptr;
     int solver_k = 0, solver_fp32 = -1, solver_stop = -1, solver_maxit = -1, solver_poll = -1;
     double solver_tol = -1;
+    // assembly temporaries and the buffers of the last released factor
+    rchol::Scratch scratch;
+    DevFactor spare;
     // device staging for solves (row-major blocks)
     double* dB = nullptr;
     double* dX = nullptr;
@@ -87,8 +90,9 @@ void free_work(FactorWork& w) {
 }
 
 void free_factor(DevFactor& f) {
-    void* ps[] = {f.lc_ptr, f.lc_idx, f.lc_val, f.lc_val32, f.lr_ptr, f.lr_idx, f.lr_val, f.lr_val32, f.diag,
-                  f.diag32, f.order};
+    void* ps[] = {f.lc_ptr, f.lc_idx,  f.lc_val,  f.lc_val32, f.lr_ptr,  f.lr_idx, f.lr_val,
+                  f.lr_val32, f.diag, f.diag32, f.order_f, f.order_b, f.tasks_f, f.tasks_b,
+                  f.sf_ptr, f.sf_idx, f.sf_val, f.sf_val32, f.sb_ptr, f.sb_idx, f.sb_val, f.sb_val32};
     for (void* p : ps) cudaFree(p);
     f = DevFactor();
 }
@@ -217,6 +221,8 @@ extern "C" rchol_status rchol_opts_default(rchol_opts* o) {
     o->timeout_s = 30.0;
     o->verbose = 0;
     o->poll_ns = 0;
+    o->sched_epl = 2;
+    o->exact_bwd_levels = 0;
     return RCHOL_OK;
 }
 
@@ -232,6 +238,7 @@ static rchol_status check_opts(const rchol_opts* o, std::string& why) {
     else if (o->unroll < 1 || o->unroll > 64) why = "unroll must be 1..64";
     else if (!(o->timeout_s > 0.0)) why = "timeout_s must be positive";
     else if (o->poll_ns < 0 || o->poll_ns > 100000) why = "poll_ns must be 0..100000";
+    else if (o->sched_epl < 1 || o->sched_epl > 64) why = "sched_epl must be 1..64";
     else return RCHOL_OK;
     return RCHOL_ERR_INVALID;
 }
@@ -262,6 +269,8 @@ extern "C" void rchol_destroy(rchol_ctx* ctx) {
     cudaSetDevice(ctx->device);
     drop_solver(ctx);
     free_work(ctx->w);
+    free_factor(ctx->spare);
+    ctx->scratch.release();
     if (ctx->trim) free_csc(ctx->At);
     free_csc(ctx->A);
     cudaFree(ctx->dB);
@@ -503,7 +512,10 @@ extern "C" rchol_status rchol_factor(rchol_ctx* ctx, rchol_factor_t** out) {
     }
     rchol_factor_t* f = new rchol_factor_t();
     f->ctx = ctx;
-    cudaError_t e = rchol::assemble_factor(w, ctx->trim, o.precision == RCHOL_PREC_FP32_FACTOR, f->F, ctx->stream);
+    f->F = ctx->spare;  // reuse the buffers of the last released factor
+    ctx->spare = DevFactor();
+    cudaError_t e = rchol::assemble_factor(w, ctx->trim, o.precision == RCHOL_PREC_FP32_FACTOR, o.sched_epl,
+                                           o.exact_bwd_levels != 0, o.timeout_s, ctx->scratch, f->F, ctx->stream);
     if (e != cudaSuccess) {
         free_factor(f->F);
         delete f;
@@ -616,10 +628,6 @@ rchol_status factor_from_host_csc(rchol_ctx* ctx, int32_t n, const std::vector<i
             lev[(size_t)ri[(size_t)p]] = std::max(lev[(size_t)ri[(size_t)p]], lev[(size_t)j] + 1);
     int32_t depth = 0;
     for (int32_t x : lev) depth = std::max(depth, x + 1);
-    std::vector<int32_t> lstart((size_t)depth + 1, 0), order((size_t)n);
-    for (int32_t x : lev) lstart[(size_t)x + 1]++;
-    for (int32_t l = 0; l < depth; ++l) lstart[(size_t)l + 1] += lstart[(size_t)l];
-    for (int32_t i = 0; i < n; ++i) order[(size_t)lstart[(size_t)lev[(size_t)i]]++] = i;
     auto up = [&](auto** dst, const auto& src) -> cudaError_t {
         using T = typename std::remove_reference<decltype(src)>::type::value_type;
         cudaError_t e = cudaMalloc((void**)dst, sizeof(T) * std::max<size_t>(src.size(), 1));
@@ -637,8 +645,16 @@ rchol_status factor_from_host_csc(rchol_ctx* ctx, int32_t n, const std::vector<i
     if (e == cudaSuccess) e = up(&F.lr_val32, cv32);
     if (e == cudaSuccess) e = up(&F.diag, d);
     if (e == cudaSuccess) e = up(&F.diag32, d32);
-    if (e == cudaSuccess) e = up(&F.order, order);
     F.depth = depth;
+    int32_t* dlev = nullptr;
+    if (e == cudaSuccess) e = up(&dlev, lev);
+    if (e == cudaSuccess) {
+        ctx->scratch.reset();
+        e = rchol::build_solve_schedule(F, dlev, ctx->o.sched_epl, ctx->o.exact_bwd_levels != 0, ctx->o.timeout_s,
+                                        ctx->scratch, ctx->stream);
+        ctx->scratch.reset();
+    }
+    cudaFree(dlev);
     if (e != cudaSuccess) {
         free_factor(F);
         delete f;
@@ -741,6 +757,10 @@ extern "C" void rchol_factor_free(rchol_factor_t* f) {
     if (ctx) {
         cudaSetDevice(ctx->device);
         if (ctx->solver_f == f) drop_solver(ctx);
+        if (!ctx->spare.lc_ptr && f->F.cap_n > 0) {  // keep the buffers for the next factor
+            ctx->spare = f->F;
+            f->F = DevFactor();
+        }
     }
     free_factor(f->F);
     delete f;

@@ -31,7 +31,7 @@ constexpr unsigned long long kInfBits = 0x7ff0000000000000ull;
 constexpr int kSlabBytesPerEntry = 32;     // 8 (a_val) + 8 (b_val) + 8 (b_aux) + 4 + 4
 
 enum Counter { kQHead = 0, kQTail = 1, kChunkCursor = 2, kStatus = 3, kAbort = 4, kBigCount = 5,
-               kMaxGather = 6, kOverflowFills = 7 };
+               kMaxGather = 6, kOverflowFills = 7, kDone = 8 };
 
 __device__ __forceinline__ int pow2_at_least(int x) {
     int p = 1;
@@ -184,15 +184,11 @@ __device__ bool append_fill(const FactorArgs& a, int32_t col, int32_t row, doubl
     return true;
 }
 
-__device__ __forceinline__ void push_ready(const FactorArgs& a, int32_t r) {
-    int t = atomicAdd(a.counters + kQTail, 1);
-    if (t < a.n) st_release(a.queue + t, r);
-    else fail(a, kDevBadInput);
-}
-
 // Eliminate vertex k with one warp.  Returns false if the kernel must stop.
+// `next` receives one neighbour this elimination released (or stays -1);
+// the other released neighbours go to the global queue.
 __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_global, int lane,
-                          int64_t& pool_cur, int64_t& pool_end, long long& fills) {
+                          int64_t& pool_cur, int64_t& pool_end, long long& fills, int32_t& next) {
     const int nf = ld_relaxed(a.fcnt + k);
     const int o0 = a.lcolptr[k];
     const int no = a.lcolptr[k + 1] - o0;
@@ -359,12 +355,33 @@ __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_glob
     // released
     __threadfence();
     __syncwarp();
-    for (int i = lane; i < m; i += kWarp) {
-        const int mult = (int)(s.b_aux[i] >> 32);
-        const int32_t r = s.b_row[i];
-        atomicMax(a.level + r, lk);
-        const int old = atom_add_acq_rel(a.dep + r, -mult);
-        if (old == mult) push_ready(a, r);
+    const unsigned lt = (1u << lane) - 1u;
+    for (int base = 0; base < m; base += kWarp) {
+        const int i = base + lane;
+        bool ready = false;
+        int32_t r = -1;
+        if (i < m) {
+            const int mult = (int)(s.b_aux[i] >> 32);
+            r = s.b_row[i];
+            atomicMax(a.level + r, lk);
+            ready = atom_add_acq_rel(a.dep + r, -mult) == mult;
+        }
+        unsigned bal = __ballot_sync(kFull, ready);
+        if (bal && next < 0) {  // keep the first released neighbour for this warp
+            const int leader = __ffs(bal) - 1;
+            next = __shfl_sync(kFull, r, leader);
+            if (lane == leader) ready = false;
+            bal &= bal - 1u;
+        }
+        if (bal) {  // the rest go to the global queue, one reservation per warp
+            int slot = 0;
+            if (lane == 0) slot = atomicAdd(a.counters + kQTail, __popc(bal));
+            slot = __shfl_sync(kFull, slot, 0) + __popc(bal & lt);
+            if (ready) {
+                if (slot < a.n) st_release(a.queue + slot, r);
+                else fail(a, kDevBadInput);
+            }
+        }
     }
     __syncwarp();
     return true;
@@ -379,28 +396,37 @@ __global__ void __launch_bounds__(256) factor_kernel(FactorArgs a) {
     const unsigned long long t0 = global_timer_ns();
     int64_t pool_cur = 0, pool_end = 0;
     long long fills = 0;
+    int32_t next = -1;
     while (true) {
-        int idx = 0;
-        if (lane == 0) idx = atomicAdd(a.counters + kQHead, 1);
-        idx = __shfl_sync(kFull, idx, 0);
-        if (idx >= a.n) break;
-        int k = -1;
-        if (lane == 0) {
-            unsigned spins = 0;
-            while ((k = ld_acquire(a.queue + idx)) < 0) {
-                if ((++spins & 255u) == 0) {
-                    if (aborted(a)) break;
-                    if (global_timer_ns() - t0 > a.timeout_ns) {
-                        fail(a, kDevTimeout);
-                        break;
+        int k = next;
+        next = -1;
+        if (k < 0) {
+            // pop: reserve the next queue slot and wait for its vertex.  A
+            // slot may never be filled (vertices released to the warp that
+            // freed them skip the queue), so the wait also ends once every
+            // vertex has been eliminated.
+            int idx = 0;
+            if (lane == 0) idx = atomicAdd(a.counters + kQHead, 1);
+            idx = __shfl_sync(kFull, idx, 0);
+            if (idx >= a.n) break;
+            if (lane == 0) {
+                unsigned spins = 0;
+                while ((k = ld_acquire(a.queue + idx)) < 0) {
+                    if ((++spins & 63u) == 0) {
+                        if (ld_relaxed(a.counters + kDone) >= a.n || aborted(a)) break;
+                        if (global_timer_ns() - t0 > a.timeout_ns) {
+                            fail(a, kDevTimeout);
+                            break;
+                        }
                     }
                 }
             }
+            k = __shfl_sync(kFull, k, 0);
+            if (k < 0) break;
         }
-        k = __shfl_sync(kFull, k, 0);
-        if (k < 0) break;
         __threadfence();
-        if (!eliminate(a, k, sm, warp_global, lane, pool_cur, pool_end, fills)) break;
+        if (!eliminate(a, k, sm, warp_global, lane, pool_cur, pool_end, fills, next)) break;
+        if (lane == 0) atomicAdd(a.counters + kDone, 1);
         if (aborted(a)) break;
     }
     if (lane == 0 && fills) atomicAdd(a.pool_cursor + 1, (unsigned long long)fills);

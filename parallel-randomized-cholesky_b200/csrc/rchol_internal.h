@@ -7,6 +7,50 @@
 
 namespace rchol {
 
+// Bump allocator for the temporaries of one assembly (reset per call):
+// avoids a cudaMalloc/cudaFree (and the device sync of cudaFree) per
+// temporary.  Requests beyond the arena fall back to cudaMalloc and are
+// released at the next reset.
+struct Scratch {
+    char* base = nullptr;
+    size_t cap = 0, used = 0;
+    void* overflow[64] = {};
+    int noverflow = 0;
+    cudaError_t reserve(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        cudaFree(base);
+        base = nullptr;
+        cap = 0;
+        cudaError_t e = cudaMalloc((void**)&base, bytes);
+        if (e == cudaSuccess) cap = bytes;
+        return e;
+    }
+    void reset() {
+        used = 0;
+        for (int i = 0; i < noverflow; ++i) cudaFree(overflow[i]);
+        noverflow = 0;
+    }
+    template <typename T>
+    cudaError_t get(T** p, int64_t n) {
+        size_t bytes = (sizeof(T) * (size_t)(n > 0 ? n : 1) + 255) & ~(size_t)255;
+        if (used + bytes <= cap) {
+            *p = reinterpret_cast<T*>(base + used);
+            used += bytes;
+            return cudaSuccess;
+        }
+        if (noverflow == 64) return cudaErrorMemoryAllocation;
+        cudaError_t e = cudaMalloc((void**)p, bytes);
+        if (e == cudaSuccess) overflow[noverflow++] = *p;
+        return e;
+    }
+    void release() {
+        reset();
+        cudaFree(base);
+        base = nullptr;
+        cap = 0;
+    }
+};
+
 // Error codes written to the device status word (first writer wins).
 enum DeviceError : int {
     kDevOk = 0,
@@ -84,11 +128,46 @@ struct DevFactor {
     float* lr_val32 = nullptr;
     double* diag = nullptr;
     float* diag32 = nullptr;
-    // rows in non-decreasing forward level: the forward solve walks this
-    // order, the backward solve walks it reversed (both are topological)
-    int32_t* order = nullptr;
+    // Solve schedules.  order_f lists the rows by (forward level, lane
+    // class); order_b by (backward level = depth-1-forward level, class), a
+    // topological order of the L^T solve.  A row of length len gets
+    // G = pow2 >= ceil(len / epl) lanes (1..32); a task packs
+    // 32/G rows of one level and one class into a warp: int2 {first position
+    // in the order, row count | log2(G) << 8}.
+    int32_t* order_f = nullptr;
+    int32_t* order_b = nullptr;
+    int2* tasks_f = nullptr;
+    int2* tasks_b = nullptr;
+    int32_t ntasks_f = 0, ntasks_b = 0;
+    // Solve layouts: the rows of Lr (forward) and of L^T = columns of Lc
+    // (backward) stored in schedule order, so that position p of order_f
+    // owns entries sf_ptr[p]..sf_ptr[p+1] (same for the backward side).
+    int64_t* sf_ptr = nullptr;
+    int32_t* sf_idx = nullptr;
+    double* sf_val = nullptr;
+    float* sf_val32 = nullptr;
+    int64_t* sb_ptr = nullptr;
+    int32_t* sb_idx = nullptr;
+    double* sb_val = nullptr;
+    float* sb_val32 = nullptr;
     int32_t depth = 0;        // number of levels of the forward solve DAG
+    int32_t depth_b = 0;      // levels of the backward schedule
+    // allocated capacities (buffers of a released factor are reused)
+    int64_t cap_n = 0, cap_nnz = 0, cap_tf = 0, cap_tb = 0, cap_ln = 0, cap_lz = 0;
 };
+
+// Lane classes of the K = 1 solves: a row gets G = 1, 2, 4, ..., 32 lanes,
+// the smallest G that leaves at most `epl` entries per lane (rows longer
+// than 32*epl still get one warp).
+constexpr int kLaneClasses = 6;
+
+// Builds order_f/order_b/tasks_f/tasks_b of `f` (device arrays allocated
+// here) from the forward level of every row (device array, n entries).
+// With exact_bwd the backward order uses the true longest-path levels of
+// the L^T solve (one extra sync-free pass); otherwise the reversed forward
+// levels, which are also topological.
+cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bool exact_bwd, double timeout_s,
+                                 Scratch& sc, cudaStream_t s);
 
 struct FactorLaunch {
     int grid = 0;
@@ -108,8 +187,10 @@ size_t factor_smem_bytes(int block, int smem_slab);
 
 // Assemble Lc/Lr (and FP32 copies) from the pool; drop the last vertex when
 // trim_ground is set.  The device arrays of `f` are allocated here.
-cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp32, DevFactor& f,
-                            cudaStream_t s);
+// `f` may hold the buffers of a released factor; they are reused when large
+// enough.
+cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp32, int epl, bool exact_bwd,
+                            double timeout_s, Scratch& sc, DevFactor& f, cudaStream_t s);
 // Drop the last row/column of A (ground vertex) into a new DevCsc.
 cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, cudaStream_t s);
 

@@ -68,6 +68,8 @@ struct SolveArgs {
     const int32_t* __restrict__ a_idx;
     const double* __restrict__ a_val;
     // factor
+    // forward / backward solve layouts: position p of order_f / order_b
+    // owns entries lr_ptr[p]..lr_ptr[p+1] / lc_ptr[p]..lc_ptr[p+1]
     const int64_t* __restrict__ lr_ptr;
     const int32_t* __restrict__ lr_idx;
     const void* __restrict__ lr_val;
@@ -75,7 +77,11 @@ struct SolveArgs {
     const int32_t* __restrict__ lc_idx;
     const void* __restrict__ lc_val;
     const void* __restrict__ diag;
-    const int32_t* __restrict__ order;  // rows by non-decreasing forward level
+    const int32_t* __restrict__ order_f;  // forward-solve row order
+    const int32_t* __restrict__ order_b;  // backward-solve row order
+    const int2* __restrict__ tasks_f;
+    const int2* __restrict__ tasks_b;
+    int32_t ntasks_f, ntasks_b;
     // vectors (n x K row-major)
     const double* __restrict__ b;
     double* x;
@@ -112,6 +118,24 @@ __device__ void block_partials(const double (&v)[K], double* out_block /* [K] */
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
         if (lane == 0) red[w][c] = s;
     }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double s = 0.0;
+        for (int i = 0; i < kBlock / 32; ++i) s += red[i][threadIdx.x];
+        out_block[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+// Block-wide sum per column when every thread carries the partial of column
+// (lane % K): lanes of the same column in a warp are combined first.
+template <int K>
+__device__ void block_partials_lane(double v, double* out_block /* [K] */) {
+    __shared__ double red[kBlock / 32][K];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o >= K; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    if (lane < K) red[w][lane] = v;
     __syncthreads();
     if (threadIdx.x < K) {
         double s = 0.0;
@@ -172,14 +196,115 @@ __device__ __forceinline__ double wait_value(const double* p, unsigned long long
     }
 }
 
+
+// Last-block bookkeeping after the x/r update (fwd): iteration count and the
+// residual-based stop rules.
+__device__ void fwd_convergence(SolveArgs& a, int K = 1) {
+    const int it = a.sc->iter + 1;
+    a.sc->iter = it;
+    int any = 0;
+    for (int c = 0; c < K; ++c) {
+        if (!a.sc->active[c]) continue;
+        bool conv = false;
+        if (a.stop_rule == 0) conv = sqrt(a.sc->rr[c]) <= a.tol * sqrt(a.sc->bnorm2[c]);
+        else if (a.stop_rule == 2) conv = a.sc->rr[c] <= a.tol;
+        a.sc->iters[c] = it;
+        if (conv) a.sc->active[c] = 0;
+        else any = 1;
+    }
+    if (!any || it >= a.max_iter) a.sc->done = 1;
+}
+
+// Last-block bookkeeping after z = M^-1 r (bwd): the new r.z sits in pq;
+// beta, rz and the preconditioned stop rule.  phase 0 (start or restart)
+// initialises rz and rz0.
+__device__ void bwd_scalars(SolveArgs& a, int K) {
+    const bool init = a.sc->phase == 0;
+    int any = 0;
+    for (int c = 0; c < K; ++c) {
+        const double rn = a.sc->pq[c];
+        if (init) {
+            if (a.sc->active[c]) {
+                a.sc->rz[c] = rn;
+                a.sc->rz0[c] = rn;
+                a.sc->beta[c] = 0.0;
+                if (a.stop_rule == 1 && !(rn > a.tol)) a.sc->active[c] = 0;
+            }
+        } else if (a.sc->active[c]) {
+            const double ro = a.sc->rz[c];
+            a.sc->beta[c] = ro != 0.0 ? rn / ro : 0.0;
+            a.sc->rz[c] = rn;
+            if (a.stop_rule == 1 && !(sqrt(rn) / sqrt(a.sc->rz0[c]) > a.tol)) a.sc->active[c] = 0;
+        } else {
+            a.sc->beta[c] = 0.0;
+        }
+        any |= a.sc->active[c];
+    }
+    a.sc->phase = 1;
+    if (!any) a.sc->done = 1;
+    a.sc->ticket[3] = 0;
+}
+
+// sum_p val[p] * vec[idx[p] * K + c] over entries s..e, waiting on pending
+// components; entries are fetched four at a time so their gathers overlap.
+template <typename TV, int K = 1>
+__device__ __forceinline__ double row_dot(const int32_t* __restrict__ idx, const TV* __restrict__ val, int64_t s,
+                                          int64_t e, const double* vec, unsigned long long t0,
+                                          unsigned long long limit, int* status, bool& ok, int poll_ns, int c = 0) {
+    double sum = 0.0;
+    int64_t p = s;
+    for (; p + 4 <= e; p += 4) {
+        const double* q0 = vec + (size_t)idx[p] * K + c;
+        const double* q1 = vec + (size_t)idx[p + 1] * K + c;
+        const double* q2 = vec + (size_t)idx[p + 2] * K + c;
+        const double* q3 = vec + (size_t)idx[p + 3] * K + c;
+        const double l0 = to_d(val[p]), l1 = to_d(val[p + 1]), l2 = to_d(val[p + 2]), l3 = to_d(val[p + 3]);
+        double v0 = ld_relaxed_f64(q0), v1 = ld_relaxed_f64(q1);
+        double v2 = ld_relaxed_f64(q2), v3 = ld_relaxed_f64(q3);
+        if (is_pending(v0)) v0 = wait_value(q0, t0, limit, status, ok, poll_ns);
+        if (is_pending(v1)) v1 = wait_value(q1, t0, limit, status, ok, poll_ns);
+        if (is_pending(v2)) v2 = wait_value(q2, t0, limit, status, ok, poll_ns);
+        if (is_pending(v3)) v3 = wait_value(q3, t0, limit, status, ok, poll_ns);
+        sum += l0 * v0;
+        sum += l1 * v1;
+        sum += l2 * v2;
+        sum += l3 * v3;
+    }
+    for (; p < e; ++p) {
+        const double* q = vec + (size_t)idx[p] * K + c;
+        double v = ld_relaxed_f64(q);
+        if (is_pending(v)) v = wait_value(q, t0, limit, status, ok, poll_ns);
+        sum += to_d(val[p]) * v;
+    }
+    return sum;
+}
+
+// sum_p val[p] * vec[idx[p] * K + c] for final (non-pending) vectors
+template <int K = 1>
+__device__ __forceinline__ double row_dot_plain(const int32_t* __restrict__ idx, const double* __restrict__ val,
+                                                int64_t s, int64_t e, const double* __restrict__ vec, int c = 0) {
+    double sum = 0.0;
+    int64_t p = s;
+    for (; p + 4 <= e; p += 4) {
+        const double v0 = vec[(size_t)idx[p] * K + c], v1 = vec[(size_t)idx[p + 1] * K + c];
+        const double v2 = vec[(size_t)idx[p + 2] * K + c], v3 = vec[(size_t)idx[p + 3] * K + c];
+        sum += val[p] * v0;
+        sum += val[p + 1] * v1;
+        sum += val[p + 2] * v2;
+        sum += val[p + 3] * v3;
+    }
+    for (; p < e; ++p) sum += val[p] * vec[(size_t)idx[p] * K + c];
+    return sum;
+}
+
 // ---------------------------------------------------------------------------
 // init: x = 0, r = b, p = q = 0, y = pending; ||b||^2
 // ---------------------------------------------------------------------------
 template <int K>
 __global__ void __launch_bounds__(kBlock) init_kernel(SolveArgs a) {
-    double acc[K];
-#pragma unroll
-    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    // the grid stride is a multiple of K, so every element a thread touches
+    // belongs to column (lane % K)
+    double acc = 0.0;
     const int64_t total = (int64_t)a.n * K;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
@@ -189,12 +314,9 @@ __global__ void __launch_bounds__(kBlock) init_kernel(SolveArgs a) {
         a.p[t] = 0.0;
         a.q[t] = 0.0;
         a.y[t] = pending_value();
-        int c = (int)(t % K);
-#pragma unroll
-        for (int cc = 0; cc < K; ++cc)
-            if (cc == c) acc[cc] += bv * bv;
+        acc += bv * bv;
     }
-    block_partials<K>(acc, a.part + (size_t)blockIdx.x * K);
+    block_partials_lane<K>(acc, a.part + (size_t)blockIdx.x * K);
     if (last_block(&a.sc->ticket[0])) {
         sum_partials<K>(a.part, gridDim.x, a.sc->bnorm2);
         if (threadIdx.x < K) {
@@ -223,49 +345,26 @@ __global__ void __launch_bounds__(kBlock) init_kernel(SolveArgs a) {
 template <int K>
 __global__ void __launch_bounds__(kBlock) spmv_update_kernel(SolveArgs a) {
     if (ld_relaxed(&a.sc->done)) return;
-    constexpr int G = (K == 1) ? 8 : K;           // lanes per row
+    // one RHS: a thread per row; K RHS: K lanes per row, lane c owns column c
+    constexpr int G = K;
     const int lane = threadIdx.x & 31;
-    const int gl = lane % G;
+    const int c = lane % G;
     const int64_t group = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
     const int64_t ngroups = (int64_t)gridDim.x * blockDim.x / G;
-    double acc[K];
-#pragma unroll
-    for (int c = 0; c < K; ++c) acc[c] = 0.0;
-    double beta[K];
-#pragma unroll
-    for (int c = 0; c < K; ++c) beta[c] = a.sc->beta[c];
-    const unsigned gmask = (G == 32) ? kFull : (((1u << G) - 1u) << ((lane / G) * G));
+    const double beta = a.sc->beta[c];
+    double acc = 0.0;
     for (int64_t i = group; i < a.n; i += ngroups) {
         const int s = a.a_ptr[i], e = a.a_ptr[i + 1];
-        if (K == 1) {
-            double sum = 0.0;
-            for (int pp = s + gl; pp < e; pp += G) sum += a.a_val[pp] * a.z[a.a_idx[pp]];
-#pragma unroll
-            for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(gmask, sum, o, G);
-            if (gl == 0) {
-                double qi = sum + beta[0] * a.q[i];
-                double pi = a.z[i] + beta[0] * a.p[i];
-                a.q[i] = qi;
-                a.p[i] = pi;
-                a.y[i] = pending_value();
-                acc[0] += pi * qi;
-            }
-        } else {
-            const int c = gl;  // G == K
-            double sum = 0.0;
-            for (int pp = s; pp < e; ++pp) sum += a.a_val[pp] * a.z[(size_t)a.a_idx[pp] * K + c];
-            size_t o = (size_t)i * K + c;
-            double qi = sum + beta[c] * a.q[o];
-            double pi = a.z[o] + beta[c] * a.p[o];
-            a.q[o] = qi;
-            a.p[o] = pi;
-            a.y[o] = pending_value();
-#pragma unroll
-            for (int cc = 0; cc < K; ++cc)
-                if (cc == c) acc[cc] += pi * qi;
-        }
+        const double sum = row_dot_plain<K>(a.a_idx, a.a_val, s, e, a.z, c);
+        const size_t o = (size_t)i * K + c;
+        const double qi = sum + beta * a.q[o];
+        const double pi = a.z[o] + beta * a.p[o];
+        a.q[o] = qi;
+        a.p[o] = pi;
+        a.y[o] = pending_value();
+        acc += pi * qi;
     }
-    block_partials<K>(acc, a.part + (size_t)blockIdx.x * K);
+    block_partials_lane<K>(acc, a.part + (size_t)blockIdx.x * K);
     if (last_block(&a.sc->ticket[1])) {
         sum_partials<K>(a.part, gridDim.x, a.sc->pq);
         if (threadIdx.x < K) {
@@ -282,71 +381,33 @@ __global__ void __launch_bounds__(kBlock) spmv_update_kernel(SolveArgs a) {
 // ---------------------------------------------------------------------------
 template <int K, typename TV>
 __global__ void __launch_bounds__(kBlock) fwd_kernel(SolveArgs a) {
+    // K >= 2 right-hand sides: K lanes per row, lane c owns column c
     if (a.reduce && ld_relaxed(&a.sc->done)) return;
-    constexpr int G = (K == 1) ? 8 : K;
+    constexpr int G = K;
     const int lane = threadIdx.x & 31;
-    const int gl = lane % G;
+    const int c = lane % G;
     const int64_t group = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
     const int64_t ngroups = (int64_t)gridDim.x * blockDim.x / G;
-    const unsigned gmask = (G == 32) ? kFull : (((1u << G) - 1u) << ((lane / G) * G));
     const TV* __restrict__ lv = reinterpret_cast<const TV*>(a.lr_val);
-    double alpha[K];
-#pragma unroll
-    for (int c = 0; c < K; ++c) alpha[c] = a.update ? a.sc->alpha[c] : 0.0;
-    double acc[K];
-#pragma unroll
-    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    const double alpha = a.update ? a.sc->alpha[c] : 0.0;
+    double acc = 0.0;
     const unsigned long long t0 = global_timer_ns();
     bool ok = true;
     for (int64_t t = group; t < a.n && ok; t += ngroups) {
-        const int64_t i = a.order ? a.order[t] : t;
-        const int64_t s = a.lr_ptr[i], e = a.lr_ptr[i + 1];
-        if (K == 1) {
-            double ri = a.r[i];
-            if (a.update) {
-                double xi = a.x[i] + alpha[0] * a.p[i];
-                ri = ri - alpha[0] * a.q[i];
-                if (gl == 0) {
-                    a.x[i] = xi;
-                    a.r[i] = ri;
-                    acc[0] += ri * ri;
-                }
-            }
-            double sum = 0.0;
-            for (int64_t pp = s + gl; pp < e; pp += G) {
-                const double l = to_d(lv[pp]);
-                const double yj = wait_value(a.y + a.lr_idx[pp], t0, a.timeout_ns, &a.sc->status, ok, a.poll_ns);
-                sum += l * yj;
-            }
-#pragma unroll
-            for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(gmask, sum, o, G);
-            if (gl == 0) {
-                if (a.z) a.z[i] = pending_value();
-                st_relaxed_f64(a.y + i, ri - sum);
-            }
-        } else {
-            const int c = gl;
-            const size_t o = (size_t)i * K + c;
-            double ri = a.r[o];
-            if (a.update) {
-                double xi = a.x[o] + alpha[c] * a.p[o];
-                ri = ri - alpha[c] * a.q[o];
-                a.x[o] = xi;
-                a.r[o] = ri;
-#pragma unroll
-                for (int cc = 0; cc < K; ++cc)
-                    if (cc == c) acc[cc] += ri * ri;
-            }
-            double sum = 0.0;
-            for (int64_t pp = s; pp < e; ++pp) {
-                const double l = to_d(lv[pp]);
-                const double yj =
-                    wait_value(a.y + (size_t)a.lr_idx[pp] * K + c, t0, a.timeout_ns, &a.sc->status, ok, a.poll_ns);
-                sum += l * yj;
-            }
-            if (a.z) a.z[o] = pending_value();
-            st_relaxed_f64(a.y + o, ri - sum);
+        const int64_t i = a.order_f[t];
+        const int64_t s = a.lr_ptr[t], e = a.lr_ptr[t + 1];
+        const size_t o = (size_t)i * K + c;
+        double ri = a.r[o];
+        if (a.update) {
+            a.x[o] = a.x[o] + alpha * a.p[o];
+            ri = ri - alpha * a.q[o];
+            a.r[o] = ri;
+            acc += ri * ri;
         }
+        const double sum = row_dot<TV, K>(a.lr_idx, lv, s, e, a.y, t0, a.timeout_ns, &a.sc->status, ok,
+                                          a.poll_ns, c);
+        if (a.z) a.z[o] = pending_value();
+        st_relaxed_f64(a.y + o, ri - sum);
     }
     // a timed-out wait abandons the pass (block-uniform decision)
     if (__syncthreads_or(!ok)) {
@@ -354,29 +415,11 @@ __global__ void __launch_bounds__(kBlock) fwd_kernel(SolveArgs a) {
         return;
     }
     if (!a.reduce) return;
-    block_partials<K>(acc, a.part + (size_t)(a.grid_max + blockIdx.x) * K);
+    block_partials_lane<K>(acc, a.part + (size_t)(a.grid_max + blockIdx.x) * K);
     if (last_block(&a.sc->ticket[2])) {
         if (a.update) {
             sum_partials<K>(a.part + (size_t)a.grid_max * K, gridDim.x, a.sc->rr);
-            if (threadIdx.x == 0) {
-                const int it = a.sc->iter + 1;
-                a.sc->iter = it;
-                int any = 0;
-                for (int c = 0; c < K; ++c) {
-                    if (!a.sc->active[c]) continue;
-                    bool conv = false;
-                    if (a.stop_rule == 0) conv = sqrt(a.sc->rr[c]) <= a.tol * sqrt(a.sc->bnorm2[c]);
-                    else if (a.stop_rule == 2) conv = a.sc->rr[c] <= a.tol;
-                    if (conv) {
-                        a.sc->active[c] = 0;
-                        a.sc->iters[c] = it;
-                    } else {
-                        a.sc->iters[c] = it;
-                        any = 1;
-                    }
-                }
-                if (!any || it >= a.max_iter) a.sc->done = 1;
-            }
+            if (threadIdx.x == 0) fwd_convergence(a, K);
         }
         if (threadIdx.x == 0) a.sc->ticket[2] = 0;
     }
@@ -387,58 +430,30 @@ __global__ void __launch_bounds__(kBlock) fwd_kernel(SolveArgs a) {
 // ---------------------------------------------------------------------------
 template <int K, typename TV>
 __global__ void __launch_bounds__(kBlock) bwd_kernel(SolveArgs a) {
+    // K >= 2 right-hand sides: K lanes per row, lane c owns column c
     if (a.reduce && ld_relaxed(&a.sc->done)) return;
-    constexpr int G = (K == 1) ? 8 : K;
+    constexpr int G = K;
     const int lane = threadIdx.x & 31;
-    const int gl = lane % G;
+    const int c = lane % G;
     const int64_t group = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
     const int64_t ngroups = (int64_t)gridDim.x * blockDim.x / G;
-    const unsigned gmask = (G == 32) ? kFull : (((1u << G) - 1u) << ((lane / G) * G));
     const TV* __restrict__ lv = reinterpret_cast<const TV*>(a.lc_val);
     const TV* __restrict__ dv = reinterpret_cast<const TV*>(a.diag);
-    double acc[K];
-#pragma unroll
-    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    double acc = 0.0;
     const unsigned long long t0 = global_timer_ns();
     bool ok = true;
     for (int64_t g = group; g < a.n && ok; g += ngroups) {
-        const int64_t j = a.order ? a.order[a.n - 1 - g] : a.n - 1 - g;
-        const int64_t s = a.lc_ptr[j], e = a.lc_ptr[j + 1];
+        const int64_t j = a.order_b[g];
+        const int64_t s = a.lc_ptr[g], e = a.lc_ptr[g + 1];
         const double dj = to_d(dv[j]);
-        if (K == 1) {
-            double t = a.y[j];
-            if (dj != 0.0) t = t / dj;
-            double sum = 0.0;
-            for (int64_t pp = s + gl; pp < e; pp += G) {
-                const double l = to_d(lv[pp]);
-                const double zi = wait_value(a.z + a.lc_idx[pp], t0, a.timeout_ns, &a.sc->status, ok, a.poll_ns);
-                sum += l * zi;
-            }
-#pragma unroll
-            for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(gmask, sum, o, G);
-            if (gl == 0) {
-                const double zj = t - sum;
-                st_relaxed_f64(a.z + j, zj);
-                acc[0] += a.r[j] * zj;
-            }
-        } else {
-            const int c = gl;
-            const size_t o = (size_t)j * K + c;
-            double t = a.y[o];
-            if (dj != 0.0) t = t / dj;
-            double sum = 0.0;
-            for (int64_t pp = s; pp < e; ++pp) {
-                const double l = to_d(lv[pp]);
-                const double zi =
-                    wait_value(a.z + (size_t)a.lc_idx[pp] * K + c, t0, a.timeout_ns, &a.sc->status, ok, a.poll_ns);
-                sum += l * zi;
-            }
-            const double zj = t - sum;
-            st_relaxed_f64(a.z + o, zj);
-#pragma unroll
-            for (int cc = 0; cc < K; ++cc)
-                if (cc == c) acc[cc] += a.r[o] * zj;
-        }
+        const size_t o = (size_t)j * K + c;
+        double t = a.y[o];
+        if (dj != 0.0) t = t / dj;
+        const double sum = row_dot<TV, K>(a.lc_idx, lv, s, e, a.z, t0, a.timeout_ns, &a.sc->status, ok,
+                                          a.poll_ns, c);
+        const double zj = t - sum;
+        st_relaxed_f64(a.z + o, zj);
+        acc += a.r[o] * zj;
     }
     // a timed-out wait abandons the pass (block-uniform decision)
     if (__syncthreads_or(!ok)) {
@@ -446,44 +461,167 @@ __global__ void __launch_bounds__(kBlock) bwd_kernel(SolveArgs a) {
         return;
     }
     if (!a.reduce) return;
-    block_partials<K>(acc, a.part + (size_t)(2 * a.grid_max + blockIdx.x) * K);
+    block_partials_lane<K>(acc, a.part + (size_t)(2 * a.grid_max + blockIdx.x) * K);
     if (last_block(&a.sc->ticket[3])) {
-        double* rzn = a.sc->pq;  // reuse pq storage for the new r.z (pq is consumed)
-        sum_partials<K>(a.part + (size_t)2 * a.grid_max * K, gridDim.x, rzn);
-        if (threadIdx.x == 0) {
-            const bool init = a.sc->phase == 0;
-            int any = 0;
-            for (int c = 0; c < K; ++c) {
-                const double rn = rzn[c];
-                if (init) {
-                    if (a.sc->active[c]) {
-                        a.sc->rz[c] = rn;
-                        a.sc->rz0[c] = rn;
-                        a.sc->beta[c] = 0.0;
-                    }
-                } else if (a.sc->active[c]) {
-                    const double ro = a.sc->rz[c];
-                    a.sc->beta[c] = ro != 0.0 ? rn / ro : 0.0;
-                    a.sc->rz[c] = rn;
-                    if (a.stop_rule == 1) {
-                        const double r0 = a.sc->rz0[c];
-                        if (!(sqrt(rn) / sqrt(r0) > a.tol)) a.sc->active[c] = 0;
-                    }
-                } else {
-                    a.sc->beta[c] = 0.0;
-                }
-                any |= a.sc->active[c];
-            }
-            if (init && a.stop_rule == 1) {
-                for (int c = 0; c < K; ++c)
-                    if (a.sc->active[c] && !(a.sc->rz[c] > a.tol)) a.sc->active[c] = 0;
-                any = 0;
-                for (int c = 0; c < K; ++c) any |= a.sc->active[c];
-            }
-            a.sc->phase = 1;
-            if (!any) a.sc->done = 1;
-            a.sc->ticket[3] = 0;
+        sum_partials<K>(a.part + (size_t)2 * a.grid_max * K, gridDim.x, a.sc->pq);
+        if (threadIdx.x == 0) bwd_scalars(a, K);
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// K = 1 solves driven by the level-ordered task lists: a task is one long
+// row (the warp's lanes stride its entries) or a pack of up to 32 short rows
+// of one level (one row per lane, entries loaded four at a time so that the
+// row's gathers are in flight together).  Warps walk the task list in
+// order, so every dependency sits in an earlier task.
+// ---------------------------------------------------------------------------
+
+// Strided partial dot product of one lane of a G-lane row group: entries
+// s+gl, s+gl+G, ... fetched four at a time.
+template <typename TV>
+__device__ __forceinline__ double group_dot(const int32_t* __restrict__ idx, const TV* __restrict__ val, int64_t s,
+                                            int64_t e, int gl, int G, const double* vec, unsigned long long t0,
+                                            unsigned long long limit, int* status, bool& ok, int poll_ns) {
+    double sum = 0.0;
+    int64_t p = s + gl;
+    const int64_t G4 = 4ll * G;
+    for (; p + 3 * G < e; p += G4) {
+        const double* q0 = vec + idx[p];
+        const double* q1 = vec + idx[p + G];
+        const double* q2 = vec + idx[p + 2 * G];
+        const double* q3 = vec + idx[p + 3 * G];
+        const double l0 = to_d(val[p]), l1 = to_d(val[p + G]), l2 = to_d(val[p + 2 * G]), l3 = to_d(val[p + 3 * G]);
+        double v0 = ld_relaxed_f64(q0), v1 = ld_relaxed_f64(q1);
+        double v2 = ld_relaxed_f64(q2), v3 = ld_relaxed_f64(q3);
+        if (is_pending(v0)) v0 = wait_value(q0, t0, limit, status, ok, poll_ns);
+        if (is_pending(v1)) v1 = wait_value(q1, t0, limit, status, ok, poll_ns);
+        if (is_pending(v2)) v2 = wait_value(q2, t0, limit, status, ok, poll_ns);
+        if (is_pending(v3)) v3 = wait_value(q3, t0, limit, status, ok, poll_ns);
+        sum += l0 * v0;
+        sum += l1 * v1;
+        sum += l2 * v2;
+        sum += l3 * v3;
+    }
+    for (; p < e; p += G) {
+        const double* q = vec + idx[p];
+        double v = ld_relaxed_f64(q);
+        if (is_pending(v)) v = wait_value(q, t0, limit, status, ok, poll_ns);
+        sum += to_d(val[p]) * v;
+    }
+    return sum;
+}
+
+// Sum over the G lanes of each row group (all 32 lanes take part).
+__device__ __forceinline__ double group_sum(double v, int G) {
+    for (int o = 16; o > 0; o >>= 1)
+        if (o < G) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+template <typename TV>
+__global__ void __launch_bounds__(kBlock) fwd_task_kernel(SolveArgs a) {
+    if (a.reduce && ld_relaxed(&a.sc->done)) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const TV* __restrict__ lv = reinterpret_cast<const TV*>(a.lr_val);
+    const double alpha = a.update ? a.sc->alpha[0] : 0.0;
+    double acc[1] = {0.0};
+    const unsigned long long t0 = global_timer_ns();
+    bool ok = true;
+    int2 dn = warp < a.ntasks_f ? a.tasks_f[warp] : make_int2(0, 0);
+    for (int64_t t = warp; t < a.ntasks_f && ok; t += nwarps) {
+        const int2 d = dn;
+        if (t + nwarps < a.ntasks_f) dn = a.tasks_f[t + nwarps];  // next descriptor in flight
+        const int G = 1 << (d.y >> 8);
+        const int cnt = d.y & 0xff;
+        const int r = lane / G, gl = lane % G;
+        const bool active = r < cnt;
+        int64_t i = 0;
+        double sum = 0.0;
+        if (active) {
+            const int64_t p = d.x + r;
+            i = a.order_f[p];
+            sum = group_dot<TV>(a.lr_idx, lv, a.lr_ptr[p], a.lr_ptr[p + 1], gl, G, a.y, t0, a.timeout_ns,
+                                &a.sc->status, ok, a.poll_ns);
         }
+        sum = group_sum(sum, G);
+        if (active && gl == 0) {
+            double ri = a.r[i];
+            if (a.update) {
+                a.x[i] = a.x[i] + alpha * a.p[i];
+                ri = ri - alpha * a.q[i];
+                a.r[i] = ri;
+                acc[0] += ri * ri;
+            }
+            if (a.z) a.z[i] = pending_value();
+            st_relaxed_f64(a.y + i, ri - sum);
+        }
+        ok = __all_sync(kFull, ok);
+    }
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) a.sc->done = 1;
+        return;
+    }
+    if (!a.reduce) return;
+    block_partials<1>(acc, a.part + (size_t)(a.grid_max + blockIdx.x));
+    if (last_block(&a.sc->ticket[2])) {
+        if (a.update) {
+            sum_partials<1>(a.part + (size_t)a.grid_max, gridDim.x, a.sc->rr);
+            if (threadIdx.x == 0) fwd_convergence(a);
+        }
+        if (threadIdx.x == 0) a.sc->ticket[2] = 0;
+    }
+}
+
+template <typename TV>
+__global__ void __launch_bounds__(kBlock) bwd_task_kernel(SolveArgs a) {
+    if (a.reduce && ld_relaxed(&a.sc->done)) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const TV* __restrict__ lv = reinterpret_cast<const TV*>(a.lc_val);
+    const TV* __restrict__ dv = reinterpret_cast<const TV*>(a.diag);
+    double acc[1] = {0.0};
+    const unsigned long long t0 = global_timer_ns();
+    bool ok = true;
+    int2 dn = warp < a.ntasks_b ? a.tasks_b[warp] : make_int2(0, 0);
+    for (int64_t t = warp; t < a.ntasks_b && ok; t += nwarps) {
+        const int2 d = dn;
+        if (t + nwarps < a.ntasks_b) dn = a.tasks_b[t + nwarps];  // next descriptor in flight
+        const int G = 1 << (d.y >> 8);
+        const int cnt = d.y & 0xff;
+        const int r = lane / G, gl = lane % G;
+        const bool active = r < cnt;
+        int64_t j = 0;
+        double sum = 0.0;
+        if (active) {
+            const int64_t p = d.x + r;
+            j = a.order_b[p];
+            sum = group_dot<TV>(a.lc_idx, lv, a.lc_ptr[p], a.lc_ptr[p + 1], gl, G, a.z, t0, a.timeout_ns,
+                                &a.sc->status, ok, a.poll_ns);
+        }
+        sum = group_sum(sum, G);
+        if (active && gl == 0) {
+            const double dj = to_d(dv[j]);
+            double tj = a.y[j];
+            if (dj != 0.0) tj = tj / dj;
+            const double zj = tj - sum;
+            st_relaxed_f64(a.z + j, zj);
+            if (a.reduce) acc[0] += a.r[j] * zj;
+        }
+        ok = __all_sync(kFull, ok);
+    }
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) a.sc->done = 1;
+        return;
+    }
+    if (!a.reduce) return;
+    block_partials<1>(acc, a.part + (size_t)(2 * a.grid_max + blockIdx.x));
+    if (last_block(&a.sc->ticket[3])) {
+        sum_partials<1>(a.part + (size_t)2 * a.grid_max, gridDim.x, a.sc->pq);
+        if (threadIdx.x == 0) bwd_scalars(a, 1);
     }
 }
 
@@ -492,42 +630,21 @@ __global__ void __launch_bounds__(kBlock) bwd_kernel(SolveArgs a) {
 // ---------------------------------------------------------------------------
 template <int K>
 __global__ void __launch_bounds__(kBlock) true_residual_kernel(SolveArgs a, int replace, double* t_out) {
-    constexpr int G = (K == 1) ? 8 : K;
+    constexpr int G = K;
     const int lane = threadIdx.x & 31;
-    const int gl = lane % G;
+    const int c = lane % G;
     const int64_t group = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
     const int64_t ngroups = (int64_t)gridDim.x * blockDim.x / G;
-    const unsigned gmask = (G == 32) ? kFull : (((1u << G) - 1u) << ((lane / G) * G));
-    double acc[K];
-#pragma unroll
-    for (int c = 0; c < K; ++c) acc[c] = 0.0;
+    double acc = 0.0;
     for (int64_t i = group; i < a.n; i += ngroups) {
-        const int s = a.a_ptr[i], e = a.a_ptr[i + 1];
-        if (K == 1) {
-            double sum = 0.0;
-            for (int pp = s + gl; pp < e; pp += G) sum += a.a_val[pp] * a.x[a.a_idx[pp]];
-#pragma unroll
-            for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(gmask, sum, o, G);
-            if (gl == 0) {
-                double t = a.b[i] - sum;
-                if (t_out) t_out[i] = t;
-                if (replace) a.r[i] = t;
-                acc[0] += t * t;
-            }
-        } else {
-            const int c = gl;
-            double sum = 0.0;
-            for (int pp = s; pp < e; ++pp) sum += a.a_val[pp] * a.x[(size_t)a.a_idx[pp] * K + c];
-            size_t o = (size_t)i * K + c;
-            double t = a.b[o] - sum;
-            if (t_out) t_out[o] = t;
-            if (replace) a.r[o] = t;
-#pragma unroll
-            for (int cc = 0; cc < K; ++cc)
-                if (cc == c) acc[cc] += t * t;
-        }
+        const double sum = row_dot_plain<K>(a.a_idx, a.a_val, a.a_ptr[i], a.a_ptr[i + 1], a.x, c);
+        const size_t o = (size_t)i * K + c;
+        const double t = a.b[o] - sum;
+        if (t_out) t_out[o] = t;
+        if (replace) a.r[o] = t;
+        acc += t * t;
     }
-    block_partials<K>(acc, a.part + (size_t)blockIdx.x * K);
+    block_partials_lane<K>(acc, a.part + (size_t)blockIdx.x * K);
     if (last_block(&a.sc->ticket[0])) {
         sum_partials<K>(a.part, gridDim.x, a.sc->tr2);
         if (threadIdx.x == 0) a.sc->ticket[0] = 0;
@@ -623,14 +740,20 @@ class PcgSolver {
         a.a_ptr = A.colptr;
         a.a_idx = A.rowind;
         a.a_val = A.val;
-        a.lr_ptr = F.lr_ptr;
-        a.lr_idx = F.lr_idx;
-        a.lr_val = cfg.fp32_factor ? (const void*)F.lr_val32 : (const void*)F.lr_val;
-        a.lc_ptr = F.lc_ptr;
-        a.lc_idx = F.lc_idx;
-        a.lc_val = cfg.fp32_factor ? (const void*)F.lc_val32 : (const void*)F.lc_val;
+        // the solves read the schedule-ordered layouts (row ranges by position)
+        a.lr_ptr = F.sf_ptr;
+        a.lr_idx = F.sf_idx;
+        a.lr_val = cfg.fp32_factor ? (const void*)F.sf_val32 : (const void*)F.sf_val;
+        a.lc_ptr = F.sb_ptr;
+        a.lc_idx = F.sb_idx;
+        a.lc_val = cfg.fp32_factor ? (const void*)F.sb_val32 : (const void*)F.sb_val;
         a.diag = cfg.fp32_factor ? (const void*)F.diag32 : (const void*)F.diag;
-        a.order = F.order;
+        a.order_f = F.order_f;
+        a.order_b = F.order_b;
+        a.tasks_f = F.tasks_f;
+        a.tasks_b = F.tasks_b;
+        a.ntasks_f = F.ntasks_f;
+        a.ntasks_b = F.ntasks_b;
         a.b = b;
         a.x = x;
         a.r = r;
@@ -680,8 +803,8 @@ template <int K, typename TV>
 static void bind_kernels(PcgSolver* s) {
     s->k_init = (void*)init_kernel<K>;
     s->k_spmv = (void*)spmv_update_kernel<K>;
-    s->k_fwd = (void*)fwd_kernel<K, TV>;
-    s->k_bwd = (void*)bwd_kernel<K, TV>;
+    s->k_fwd = K == 1 ? (void*)fwd_task_kernel<TV> : (void*)fwd_kernel<K, TV>;
+    s->k_bwd = K == 1 ? (void*)bwd_task_kernel<TV> : (void*)bwd_kernel<K, TV>;
     s->k_true = (void*)true_residual_kernel<K>;
     s->k_restart = (void*)restart_kernel<K>;
 }
@@ -714,7 +837,7 @@ PcgSolver* pcg_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cf
     s->stream = stream;
     s->K = cfg.k;
     bool okk = cfg.fp32_factor ? bind_for_k<float>(s, cfg.k) : bind_for_k<double>(s, cfg.k);
-    if (!okk || (cfg.fp32_factor && !F.lr_val32)) {
+    if (!okk || (cfg.fp32_factor && !F.sf_val32)) {
         delete s;
         *err = cudaErrorInvalidValue;
         return nullptr;
@@ -978,14 +1101,19 @@ static cudaError_t precond_apply_t(const DevFactor& F, const double* r, double* 
     SolveArgs a;
     memset(&a, 0, sizeof(a));
     a.n = F.n;
-    a.lr_ptr = F.lr_ptr;
-    a.lr_idx = F.lr_idx;
-    a.lr_val = std::is_same<TV, float>::value ? (const void*)F.lr_val32 : (const void*)F.lr_val;
-    a.lc_ptr = F.lc_ptr;
-    a.lc_idx = F.lc_idx;
-    a.lc_val = std::is_same<TV, float>::value ? (const void*)F.lc_val32 : (const void*)F.lc_val;
+    a.lr_ptr = F.sf_ptr;
+    a.lr_idx = F.sf_idx;
+    a.lr_val = std::is_same<TV, float>::value ? (const void*)F.sf_val32 : (const void*)F.sf_val;
+    a.lc_ptr = F.sb_ptr;
+    a.lc_idx = F.sb_idx;
+    a.lc_val = std::is_same<TV, float>::value ? (const void*)F.sb_val32 : (const void*)F.sb_val;
     a.diag = std::is_same<TV, float>::value ? (const void*)F.diag32 : (const void*)F.diag;
-    a.order = F.order;
+    a.order_f = F.order_f;
+    a.order_b = F.order_b;
+    a.tasks_f = F.tasks_f;
+    a.tasks_b = F.tasks_b;
+    a.ntasks_f = F.ntasks_f;
+    a.ntasks_b = F.ntasks_b;
     a.r = const_cast<double*>(r);
     a.y = y;
     a.z = z;
@@ -995,10 +1123,17 @@ static cudaError_t precond_apply_t(const DevFactor& F, const double* r, double* 
     a.timeout_ns = (unsigned long long)(timeout_s * 1e9);
     const int64_t total = (int64_t)F.n * K;
     fill_pending_kernel<<<148 * 8, kBlock, 0, s>>>(y, total);
-    int gf = resident_blocks((void*)fwd_kernel<K, TV>, device);
-    int gb = resident_blocks((void*)bwd_kernel<K, TV>, device);
-    fwd_kernel<K, TV><<<gf, kBlock, 0, s>>>(a);
-    bwd_kernel<K, TV><<<gb, kBlock, 0, s>>>(a);
+    if (K == 1) {
+        int gf = resident_blocks((void*)fwd_task_kernel<TV>, device);
+        int gb = resident_blocks((void*)bwd_task_kernel<TV>, device);
+        fwd_task_kernel<TV><<<gf, kBlock, 0, s>>>(a);
+        bwd_task_kernel<TV><<<gb, kBlock, 0, s>>>(a);
+    } else {
+        int gf = resident_blocks((void*)fwd_kernel<K, TV>, device);
+        int gb = resident_blocks((void*)bwd_kernel<K, TV>, device);
+        fwd_kernel<K, TV><<<gf, kBlock, 0, s>>>(a);
+        bwd_kernel<K, TV><<<gb, kBlock, 0, s>>>(a);
+    }
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(status, &sc->status, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);

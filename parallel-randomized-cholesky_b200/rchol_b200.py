@@ -46,7 +46,8 @@ class Opts(C.Structure):
                 ("warps_per_block", C.c_int), ("slab_entries", C.c_int), ("bucket_cap", C.c_int),
                 ("pool_mult", C.c_double), ("max_iter", C.c_int), ("tol", C.c_double), ("stop_rule", C.c_int),
                 ("unroll", C.c_int), ("use_graph", C.c_int), ("device", C.c_int), ("timeout_s", C.c_double),
-                ("verbose", C.c_int), ("poll_ns", C.c_int)]
+                ("verbose", C.c_int), ("poll_ns", C.c_int),
+                ("sched_epl", C.c_int), ("exact_bwd_levels", C.c_int)]
 
 
 class FactorInfo(C.Structure):
