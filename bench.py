@@ -55,8 +55,12 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    p.add_argument("--config", default="c2", choices=sorted(CONFIGS) + ["c4"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile-run", action="store_true",
+                   help="one factorization + one PCG solve of the config (mixed form), for profilers")
+    p.add_argument("--size", type=int, default=0, help="grid side override for --profile-run (small ncu cases)")
+    p.add_argument("--max-iter", type=int, default=0, help="PCG iteration cap for --profile-run")
     return p.parse_args()
 
 
@@ -281,6 +285,14 @@ def run_b200(args, cfg, rank, world, local):
     achieved = ab[dom] / (per_launch[dom] / 1000.0) / 1e9
     traffic = committed_traffic().get(dom)
 
+    # 32 right-hand sides through one block solve vs the single-RHS solve
+    k32 = 32
+    B32 = np.random.default_rng(2000 + rank).standard_normal((ns, k32))
+    B32 -= B32.mean(axis=0)
+    ctx["mixed"].pcg_solve(f32, B32)  # warm (graph capture)
+    X32, si32k = ctx["mixed"].pcg_solve(f32, B32)
+    per_rhs_speedup = (si32["ms_total"] * k32) / si32k["ms_total"]
+
     # e2e through the public API with host buffers (pinned)
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
     hcp, hri, hv, hb = pin(W["colptr"]), pin(W["rowind"]), pin(W["val"]), pin(b)
@@ -334,6 +346,8 @@ def run_b200(args, cfg, rank, world, local):
         "e2e": {"value": round(e2e_s, 6), "unit": "s",
                 "h2d_bytes_per_step": int(W["colptr"].nbytes + W["rowind"].nbytes + W["val"].nbytes + b.nbytes),
                 "d2h_bytes_per_step": int(ns * 8)},
+        "rhs32": {"solve_ms": round(si32k["ms_total"], 3), "iterations": si32k["iterations"],
+                  "relres_true": si32k["relres_true"], "per_rhs_throughput_vs_single": round(per_rhs_speedup, 2)},
         "gpu_launches": int(launches),
         "clocks": clk,
     }
@@ -432,9 +446,135 @@ def run_reference_arm(args, cfg):
             "e2e": {"value": round(v, 6), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def c4_systems():
+    """64 uneven Laplacians: 32 2D 5-point grids with sides U{32..1024} and 32
+    3D 7-point grids with sides U{10..100} (seed 4), conductances log-uniform
+    [1e-2, 1e2], each in ascending-nnz order."""
+    import rchol_b200 as R
+    rng = np.random.default_rng(4)
+    sides2 = rng.integers(32, 1025, 32)
+    sides3 = rng.integers(10, 101, 32)
+    out = []
+    for q, s in enumerate(list(sides2) + list(sides3)):
+        dims = [int(s)] * (2 if q < 32 else 3)
+        n, r, c, v, g = R.generate("grid2d" if q < 32 else "grid3d", dims, wlo=1e-2, whi=1e2, log_weights=True,
+                                   seed=4000 + q)
+        cp, ri, val = R.csc_from_triplets(n, r, c, v)
+        out.append((n, cp, ri, val))
+    return out
+
+
+def run_c4(args):
+    """Batched uneven systems: one block-diagonal factor launch + one batched
+    PCG (8 RHS per system, FP32 factor / FP64 PCG, tol 1e-6) against looping
+    the single-system path over the same systems (factor + 8-RHS solve each)."""
+    import torch
+    import rchol_b200 as R
+    k = 8
+    systems = c4_systems()
+    ntot = sum(s[0] for s in systems)
+    rng = np.random.default_rng(44)
+    Bs = []
+    for n, *_ in systems:
+        B = rng.standard_normal((n, k))
+        Bs.append(B - B.mean(axis=0))
+    Bstack = np.concatenate(Bs, axis=0)
+    ctx = R.Context(seed=1, precision=R.PREC_FP32_FACTOR, tol=1e-6)
+    ctx.set_opts(max_iter=2000)
+    off = ctx.batch_set(systems)
+
+    def batched():
+        f = ctx.factor()
+        X, per, tot = ctx.batch_solve(f, Bstack)
+        f.free()
+        return tot, per
+
+    singles = []
+    for n, cp, ri, val in systems:
+        c = R.Context(seed=1, precision=R.PREC_FP32_FACTOR, tol=1e-6)
+        c.set_opts(max_iter=2000)
+        c.set_csc(n, cp, ri, val)
+        singles.append(c)
+
+    def looped():
+        its = []
+        for c, B in zip(singles, Bs):
+            f = c.factor()
+            X, info = c.pcg_solve(f, B)
+            its.append(info["iterations"])
+            f.free()
+        return its
+
+    for _ in range(max(1, args.warmup)):
+        batched()
+        looped()
+    tb, tl = [], []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tot, per = batched()
+        torch.cuda.synchronize()
+        tb.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        its = looped()
+        torch.cuda.synchronize()
+        tl.append(time.perf_counter() - t0)
+    solves = len(systems) * k
+    vb = solves / statistics.mean(tb)
+    vl = solves / statistics.mean(tl)
+    print(json.dumps({"metric": "batched solves/s: 64 uneven Laplacians x 8 RHS, factor + PCG to 1e-6",
+                      "value": round(vb, 2), "unit": "solves/s", "higher_is_better": True, "steps": args.steps,
+                      "warmup": args.warmup, "n_gpus": 1, "dtype": "f32 factor / f64 PCG", "data": "synthetic",
+                      "config": {"workload": "64 systems: 32 2D grids sides U{32..1024}, 32 3D grids sides "
+                                             "U{10..100} (seed 4), log-uniform conductances [1e-2,1e2]",
+                                 "unknowns": int(ntot), "rhs_per_system": k},
+                      "looped_single_system_solves_per_s": round(vl, 2),
+                      "speedup_vs_looped": round(vb / vl, 3),
+                      "batched_s": round(statistics.mean(tb), 4), "looped_s": round(statistics.mean(tl), 4),
+                      "max_iterations": tot["iterations"], "max_relres": tot["relres_true"],
+                      "looped_max_iterations": max(its), "wall_clock_timing": True}))
+    for c in singles:
+        c.close()
+    ctx.close()
+
+
+def profile_run(args, cfg):
+    """One factor + one solve through the C ABI: the workload the committed
+    ncu summaries under profiles/ were captured on."""
+    import rchol_b200 as R
+    cfg = dict(cfg)
+    if args.size:
+        cfg["dims"] = [args.size] * len(cfg["dims"])
+    W = build_workload(cfg)
+    n, ground = W["n"], W["ground"]
+    ns = n - 1 if ground else n
+    kw = dict(seed=1, precision=R.PREC_FP32_FACTOR, tol=cfg["tol"])
+    if args.max_iter:
+        kw["max_iter"] = args.max_iter
+    ctx = R.Context(**kw)
+    ctx.set_csc(n, W["colptr"], W["rowind"], W["val"], trim_ground=ground)
+    f = ctx.factor()
+    fi = f.info()
+    b = np.random.default_rng(0).standard_normal(ns)
+    b -= b.mean()
+    x, si = ctx.pcg_solve(f, b)
+    print(json.dumps({"profile_run": args.config, "dims": cfg["dims"], "n": ns, "nnz_L": fi.nnz_strict,
+                      "factor_ms": fi.ms_factor, "assemble_ms": fi.ms_assemble, "solve_ms": si["ms_total"],
+                      "iterations": si["iterations"], "relres": si["relres_true"]}))
+    f.free()
+    ctx.close()
+
+
 def main():
     args = parse()
+    if args.config == "c4":
+        dist_init(1)
+        run_c4(args)
+        return
     cfg = CONFIGS[args.config]
+    if args.profile_run:
+        profile_run(args, cfg)
+        return
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         if rank != 0:

@@ -178,6 +178,27 @@ rchol_status rchol_profile_solve(rchol_ctx* ctx, const rchol_factor_t* f, int k,
 /* Y = A X with the (trimmed) matrix of the context. */
 rchol_status rchol_spmv(rchol_ctx* ctx, int k, const double* X, double* Y, int ldb, int on_device);
 
+/* ---- batched independent systems (many uneven Laplacians at once) -------
+ * rchol_batch_set stacks nsys preprocessed systems (host CSC, diagonal
+ * included, each a Laplacian or SDDM without a ground vertex, at least 32
+ * vertices each) into one block-diagonal matrix of the context: system s owns
+ * rows offsets[s] .. offsets[s+1]-1 (offsets may be NULL).  rchol_factor then
+ * eliminates every system in one persistent launch, and rchol_batch_solve runs
+ * one PCG per (system, right-hand side) pair -- own step lengths, own stop
+ * test -- with one set of kernel launches per iteration for all of them.  B/X
+ * are (n_total x k) column-major with rows grouped by system.  per_system
+ * (nsys entries, may be NULL) receives each system's iterations (max over its
+ * right-hand sides) and true relative residual; total the whole batch. */
+typedef struct rchol_system {
+    int n;
+    const int* colptr;
+    const int* rowind;
+    const double* val;
+} rchol_system;
+rchol_status rchol_batch_set(rchol_ctx* ctx, int nsys, const rchol_system* systems, long long* offsets);
+rchol_status rchol_batch_solve(rchol_ctx* ctx, const rchol_factor_t* f, int k, const double* B, double* X, int ldb,
+                               int on_device, rchol_solve_info* per_system, rchol_solve_info* total);
+
 /* ---- reference drop-ins ---------------------------------------------------
  * The whole CLI path of driver.cu main (:2148-2160) / driver_physics.cu main:
  * load, factor with num_blocks squads, and when check_solve = 1 run PCG to

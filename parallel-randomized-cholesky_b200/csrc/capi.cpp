@@ -2,6 +2,7 @@
 // orchestration with capacity retries, PCG, the reference drop-ins.
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -37,6 +38,11 @@ struct rchol_ctx {
     const rchol_factor_t* solver_f = nullptr;
     int solver_k = 0, solver_fp32 = -1, solver_stop = -1, solver_maxit = -1, solver_poll = -1;
     double solver_tol = -1;
+    // batched systems (block-diagonal stacking)
+    std::vector<int64_t> batch_off;
+    rchol::BatchSolver* bsolver = nullptr;
+    const rchol_factor_t* bsolver_f = nullptr;
+    int bsolver_k = 0;
     // assembly temporaries and the buffers of the last released factor
     rchol::Scratch scratch;
     DevFactor spare;
@@ -182,6 +188,9 @@ void drop_solver(rchol_ctx* ctx) {
     if (ctx->solver) rchol::pcg_destroy(ctx->solver);
     ctx->solver = nullptr;
     ctx->solver_f = nullptr;
+    if (ctx->bsolver) rchol::batch_destroy(ctx->bsolver);
+    ctx->bsolver = nullptr;
+    ctx->bsolver_f = nullptr;
 }
 
 rchol_status ensure_stage(rchol_ctx* ctx, size_t elems) {
@@ -338,6 +347,7 @@ extern "C" rchol_status rchol_set_csc(rchol_ctx* ctx, int n, const int* colptr, 
     const bool same = ctx->have && ctx->A.n == n && ctx->A.nnz == nnz32 && ctx->trim == (trim_ground != 0);
     const int64_t old_lnnz = ctx->w.lnnz;
     drop_solver(ctx);
+    ctx->batch_off.clear();
     if (ctx->trim) free_csc(ctx->At);
     DevCsc A;
     if (same) {
@@ -756,7 +766,7 @@ extern "C" void rchol_factor_free(rchol_factor_t* f) {
     rchol_ctx* ctx = f->ctx;
     if (ctx) {
         cudaSetDevice(ctx->device);
-        if (ctx->solver_f == f) drop_solver(ctx);
+        if (ctx->solver_f == f || ctx->bsolver_f == f) drop_solver(ctx);
         if (!ctx->spare.lc_ptr && f->F.cap_n > 0) {  // keep the buffers for the next factor
             ctx->spare = f->F;
             f->F = DevFactor();
@@ -990,6 +1000,113 @@ void random_vec(std::vector<double>& v, size_t n, unsigned long seed) {
 }
 
 }  // namespace
+
+extern "C" rchol_status rchol_batch_set(rchol_ctx* ctx, int nsys, const rchol_system* sys, long long* offsets) {
+    if (!ctx || nsys < 1 || !sys) return fail(ctx, RCHOL_ERR_INVALID, "bad batch arguments");
+    std::vector<int64_t> off((size_t)nsys + 1, 0);
+    for (int s = 0; s < nsys; ++s) {
+        if (sys[s].n < 32 || !sys[s].colptr || !sys[s].rowind || !sys[s].val)
+            return fail(ctx, RCHOL_ERR_INVALID, "every batched system needs >= 32 vertices and CSC arrays");
+        off[(size_t)s + 1] = off[(size_t)s] + sys[s].n;
+    }
+    if (off[(size_t)nsys] > INT32_MAX) return fail(ctx, RCHOL_ERR_INVALID, "batch too large");
+    int64_t nnz = 0;
+    for (int s = 0; s < nsys; ++s) nnz += sys[s].colptr[sys[s].n];
+    if (nnz > INT32_MAX) return fail(ctx, RCHOL_ERR_INVALID, "batch has more than 2^31-1 entries");
+    const int32_t n = (int32_t)off[(size_t)nsys];
+    std::vector<int32_t> cp((size_t)n + 1), ri((size_t)nnz);
+    std::vector<double> v((size_t)nnz);
+    int64_t pos = 0;
+    for (int s = 0; s < nsys; ++s) {
+        const int32_t o = (int32_t)off[(size_t)s];
+        const int32_t ns = sys[s].n;
+        for (int32_t j = 0; j < ns; ++j) {
+            cp[(size_t)o + j] = (int32_t)pos;
+            for (int32_t p = sys[s].colptr[j]; p < sys[s].colptr[j + 1]; ++p) {
+                const int32_t r = sys[s].rowind[p];
+                if (r < 0 || r >= ns) return fail(ctx, RCHOL_ERR_INVALID, "row index out of range in a system");
+                ri[(size_t)pos] = o + r;
+                v[(size_t)pos] = sys[s].val[p];
+                ++pos;
+            }
+        }
+    }
+    cp[(size_t)n] = (int32_t)pos;
+    rchol_status st = rchol_set_csc(ctx, n, cp.data(), ri.data(), v.data(), 0, 0);
+    if (st != RCHOL_OK) return st;
+    ctx->batch_off = off;
+    if (offsets)
+        for (int s = 0; s <= nsys; ++s) offsets[s] = off[(size_t)s];
+    return RCHOL_OK;
+}
+
+extern "C" rchol_status rchol_batch_solve(rchol_ctx* ctx, const rchol_factor_t* f, int k, const double* B, double* X,
+                                          int ldb, int on_device, rchol_solve_info* per_system,
+                                          rchol_solve_info* total) {
+    if (!ctx || !f || !B || !X) return fail(ctx, RCHOL_ERR_INVALID, "null argument");
+    if (ctx->batch_off.empty()) return fail(ctx, RCHOL_ERR_NO_MATRIX, "no batch loaded (rchol_batch_set)");
+    if (!valid_k(k)) return fail(ctx, RCHOL_ERR_INVALID, "k must be 1, 2, 4, 8, 16 or 32");
+    if (f->F.n != ctx->At.n || ldb < ctx->At.n) return fail(ctx, RCHOL_ERR_INVALID, "factor/ldb mismatch");
+    cudaSetDevice(ctx->device);
+    const rchol_opts& o = ctx->o;
+    const int nsys = (int)ctx->batch_off.size() - 1;
+    if (!(ctx->bsolver && ctx->bsolver_f == f && ctx->bsolver_k == k)) {
+        drop_solver(ctx);
+        rchol::SolveConfig cfg;
+        cfg.k = k;
+        cfg.fp32_factor = o.precision == RCHOL_PREC_FP32_FACTOR;
+        cfg.tol = o.tol;
+        cfg.max_iter = o.max_iter;
+        cfg.stop_rule = o.stop_rule;
+        cfg.unroll = o.unroll;
+        cfg.use_graph = o.use_graph != 0;
+        cfg.timeout_s = o.timeout_s;
+        cfg.poll_ns = o.poll_ns;
+        if (cfg.fp32_factor && !f->F.sf_val32) return fail(ctx, RCHOL_ERR_INVALID, "factor has no FP32 copy");
+        cudaError_t e = cudaSuccess;
+        ctx->bsolver = rchol::batch_create(ctx->At, f->F, cfg, ctx->device, ctx->stream, ctx->batch_off.data(), nsys, &e);
+        if (!ctx->bsolver) return cuda_fail(ctx, e, "create batch solver");
+        ctx->bsolver_f = f;
+        ctx->bsolver_k = k;
+    }
+    rchol_status s = ensure_stage(ctx, (size_t)ctx->At.n * (size_t)k);
+    if (s != RCHOL_OK) return s;
+    s = stage_in(ctx, B, ldb, k, on_device, ctx->dB);
+    if (s != RCHOL_OK) return s;
+    rchol::BatchResult r;
+    cudaError_t e = rchol::batch_solve(ctx->bsolver, ctx->dB, ctx->dX, &r);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batch pcg");
+    s = stage_out(ctx, ctx->dX, X, ldb, k, on_device);
+    if (s != RCHOL_OK) return s;
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    int maxit = 0;
+    double maxrel = 0.0;
+    for (int q = 0; q < nsys; ++q) {
+        maxit = std::max(maxit, r.iterations[(size_t)q]);
+        maxrel = std::max(maxrel, r.relres[(size_t)q]);
+        if (per_system) {
+            std::memset(&per_system[q], 0, sizeof(rchol_solve_info));
+            per_system[q].iterations = r.iterations[(size_t)q];
+            per_system[q].relres_true = r.relres[(size_t)q];
+            per_system[q].converged = o.stop_rule != RCHOL_STOP_RELRES || r.relres[(size_t)q] <= o.tol;
+            per_system[q].device_status = r.status;
+        }
+    }
+    if (total) {
+        std::memset(total, 0, sizeof(*total));
+        total->iterations = maxit;
+        total->relres_true = maxrel;
+        total->converged = r.converged;
+        total->device_status = r.status;
+        total->ms_total = r.ms_total;
+        total->ms_iterations = r.ms_iterations;
+        total->kernel_launches = r.kernel_launches;
+        total->graph_launches = r.graph_launches;
+    }
+    if (r.status == rchol::kDevTimeout) return fail(ctx, RCHOL_ERR_TIMEOUT, "batch pcg: a device wait timed out");
+    if (!r.converged) return fail(ctx, RCHOL_ERR_NOT_CONVERGED, "batch pcg did not reach the tolerance");
+    return RCHOL_OK;
+}
 
 extern "C" rchol_status rchol_factorization_driver(const char* path, int num_blocks, int check_solve, double tol,
                                                    int physics) {

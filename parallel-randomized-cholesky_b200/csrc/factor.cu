@@ -184,11 +184,203 @@ __device__ bool append_fill(const FactorArgs& a, int32_t col, int32_t row, doubl
     return true;
 }
 
+// Release one chunk of merged neighbours after the elimination of a column:
+// raise their forward level, decrement their dependency counters (acq_rel),
+// keep the first neighbour that becomes ready in `next` and push the others
+// with one queue reservation for the warp.
+__device__ __forceinline__ void release_chunk(const FactorArgs& a, int lk, int lane, bool valid, int32_t r, int mult,
+                                              int32_t& next) {
+    bool ready = false;
+    if (valid) {
+        atomicMax(a.level + r, lk);
+        ready = atom_add_acq_rel(a.dep + r, -mult) == mult;
+    }
+    unsigned bal = __ballot_sync(kFull, ready);
+    if (bal && next < 0) {
+        const int leader = __ffs(bal) - 1;
+        next = __shfl_sync(kFull, r, leader);
+        if (lane == leader) ready = false;
+        bal &= bal - 1u;
+    }
+    if (bal) {
+        int slot = 0;
+        if (lane == 0) slot = atomicAdd(a.counters + kQTail, __popc(bal));
+        slot = __shfl_sync(kFull, slot, 0) + __popc(bal & ((1u << lane) - 1u));
+        if (ready) {
+            if (slot < a.n) st_release(a.queue + slot, r);
+            else fail(a, kDevBadInput);
+        }
+    }
+}
+
+// Reserve m entries of the L pool for this warp (grabbing kPoolGrab at a time).
+__device__ __forceinline__ bool pool_take(const FactorArgs& a, int m, int lane, int64_t& pool_cur, int64_t& pool_end,
+                                          int64_t& base) {
+    if (pool_end - pool_cur < m) {
+        const int64_t grab = m > kPoolGrab ? (int64_t)m : (int64_t)kPoolGrab;
+        unsigned long long got = 0;
+        if (lane == 0) got = atomicAdd(a.pool_cursor, (unsigned long long)grab);
+        got = __shfl_sync(kFull, got, 0);
+        if ((int64_t)got + grab > a.pool_cap) return false;
+        pool_cur = (int64_t)got;
+        pool_end = (int64_t)got + grab;
+    }
+    base = pool_cur;
+    pool_cur += m;
+    return true;
+}
+
+__device__ __forceinline__ bool row_value_gt(int32_t r1, unsigned long long v1, int32_t r2, unsigned long long v2) {
+    return (r1 > r2) || (r1 == r2 && v1 > v2);
+}
+
+// Elimination of a vertex whose gathered list fits one warp (at most 32
+// entries, all fills in the first bucket chunk): one entry per lane; sorts,
+// merge, compaction, scan and CDF search as warp shuffles.  Same arithmetic
+// in the same order as the slab path (and the oracle), so the bits agree.
+__device__ bool eliminate_small(const FactorArgs& a, int32_t k, int nf, int o0, int no, int lane,
+                                int64_t& pool_cur, int64_t& pool_end, long long& fills, int32_t& next) {
+    const int total = nf + no;
+    int32_t row = INT_MAX;
+    unsigned long long vb = kInfBits;
+    if (lane < nf) {
+        const size_t o = (size_t)k * (size_t)a.c0 + (size_t)lane;
+        row = __ldcg(a.brow + o);
+        vb = (unsigned long long)__double_as_longlong(__ldcg(a.bval + o));
+    } else if (lane < total) {
+        row = a.lrow[o0 + lane - nf];
+        vb = (unsigned long long)__double_as_longlong(a.lval[o0 + lane - nf]);
+    }
+    // bitonic sort of the 32 lanes by (row, value bits); padding sorts last
+#pragma unroll
+    for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+            const int32_t r2 = __shfl_xor_sync(kFull, row, j);
+            const unsigned long long v2 = __shfl_xor_sync(kFull, vb, j);
+            const bool keep_min = ((lane & j) == 0) == ((lane & kk) == 0);
+            const bool take = keep_min ? row_value_gt(row, vb, r2, v2) : row_value_gt(r2, v2, row, vb);
+            if (take) {
+                row = r2;
+                vb = v2;
+            }
+        }
+    }
+    // merge equal rows: the head of each run sums its run left to right
+    const double v = __longlong_as_double((long long)vb);
+    const int32_t rprev = __shfl_up_sync(kFull, row, 1);
+    const bool head = lane < total && (lane == 0 || rprev != row);
+    double acc = v;
+    int cnt = 1;
+    bool going = head;
+    for (int d = 1; d < 32; ++d) {
+        if (!__any_sync(kFull, going)) break;
+        const double vd = __shfl_down_sync(kFull, v, d);
+        const int32_t rd = __shfl_down_sync(kFull, row, d);
+        if (going) {
+            if (lane + d < total && rd == row) {
+                acc = __dadd_rn(acc, vd);
+                ++cnt;
+            } else {
+                going = false;
+            }
+        }
+    }
+    const unsigned hb = __ballot_sync(kFull, head);
+    const int m = __popc(hb);
+    const int src = lane < m ? (int)__fns(hb, 0, lane + 1) : 0;
+    int32_t mrow = __shfl_sync(kFull, row, src);
+    double mval = __shfl_sync(kFull, acc, src);
+    int mcnt = __shfl_sync(kFull, cnt, src);
+    int pos = lane;  // position in row order
+    if (lane >= m) {
+        mrow = INT_MAX;
+        mval = __longlong_as_double((long long)kInfBits);
+        mcnt = 0;
+    }
+    // sort by (value, row) carrying (multiplicity, row-order position)
+#pragma unroll
+    for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+            const double v2 = __shfl_xor_sync(kFull, mval, j);
+            const int32_t r2 = __shfl_xor_sync(kFull, mrow, j);
+            const int c2 = __shfl_xor_sync(kFull, mcnt, j);
+            const int p2 = __shfl_xor_sync(kFull, pos, j);
+            const bool keep_min = ((lane & j) == 0) == ((lane & kk) == 0);
+            const bool self_gt = (mval > v2) || (mval == v2 && mrow > r2);
+            const bool other_gt = (v2 > mval) || (v2 == mval && r2 > mrow);
+            if (keep_min ? self_gt : other_gt) {
+                mval = v2;
+                mrow = r2;
+                mcnt = c2;
+                pos = p2;
+            }
+        }
+    }
+    // inclusive prefix sum (one 32-wide Kogge-Stone chunk)
+    double cum = lane < m ? mval : 0.0;
+#pragma unroll
+    for (int off = 1; off < kWarp; off <<= 1) {
+        const double t = __shfl_up_sync(kFull, cum, off);
+        if (lane >= off) cum = __dadd_rn(cum, t);
+    }
+    const double S = __shfl_sync(kFull, cum, m - 1);
+    int64_t pbase = 0;
+    if (!pool_take(a, m, lane, pool_cur, pool_end, pbase)) {
+        if (lane == 0) fail(a, kDevCapacity);
+        return false;
+    }
+    fills += m - 1;
+    if (lane == 0) {
+        a.diag[k] = S;
+        a.pstart[k] = pbase;
+        a.pcnt[k] = m;
+    }
+    if (lane < m) {
+        a.prow[pbase + pos] = mrow;
+        a.pval[pbase + pos] = __ddiv_rn(mval, S);
+    }
+    // clique sampling: first j > lane with (C_j - C_lane) >= u * (S - C_lane)
+    const double rem = __dsub_rn(S, cum);
+    const double target = __dmul_rn(sample_uniform(a.seed, k, lane), rem);
+    int lo = lane + 1, hi = m;
+#pragma unroll
+    for (int step = 0; step < 6; ++step) {
+        const int mid = lo < hi ? lo + ((hi - lo) >> 1) : 0;
+        const double cm = __shfl_sync(kFull, cum, mid);
+        if (lo < hi) {
+            if (__dsub_rn(cm, cum) < target) lo = mid + 1;
+            else hi = mid;
+        }
+    }
+    const int jj = lo < m ? lo : m - 1;
+    const int32_t rj = __shfl_sync(kFull, mrow, jj);
+    bool ok = true;
+    if (lane < m - 1) {
+        const int32_t grow = mrow > rj ? mrow : rj;
+        const int32_t gcol = mrow > rj ? rj : mrow;
+        const double gval = __ddiv_rn(__dmul_rn(mval, rem), S);
+        if (!append_fill(a, gcol, grow, gval)) ok = false;
+        atomicAdd(a.dep + grow, 1);
+    }
+    if (__any_sync(kFull, !ok)) {
+        if (lane == 0) fail(a, kDevCapacity);
+        return false;
+    }
+    const int lk = ld_relaxed(a.level + k) + 1;
+    __threadfence();
+    __syncwarp();
+    release_chunk(a, lk, lane, lane < m, mrow, mcnt, next);
+    __syncwarp();
+    return true;
+}
+
 // Eliminate vertex k with one warp.  Returns false if the kernel must stop.
 // `next` receives one neighbour this elimination released (or stays -1);
 // the other released neighbours go to the global queue.
 __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_global, int lane,
-                          int64_t& pool_cur, int64_t& pool_end, long long& fills, int32_t& next) {
+                          int64_t& pool_cur, int64_t& pool_end, long long& fills, int32_t& next, int& max_gather) {
     const int nf = ld_relaxed(a.fcnt + k);
     const int o0 = a.lcolptr[k];
     const int no = a.lcolptr[k + 1] - o0;
@@ -201,6 +393,9 @@ __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_glob
         }
         return true;
     }
+    if (total > max_gather) max_gather = total;
+    if (total <= kWarp && nf <= a.c0)
+        return eliminate_small(a, k, nf, o0, no, lane, pool_cur, pool_end, fills, next);
     Slab s = sm;
     if (total > a.smem_slab) {
         if ((int64_t)total > a.gscratch_entries) {
@@ -211,7 +406,6 @@ __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_glob
                       (int)a.gscratch_entries);
         if (lane == 0) atomicAdd(a.counters + kBigCount, 1);
     }
-    if (lane == 0) atomicMax(a.counters + kMaxGather, total);
     const int P = pow2_at_least(total);
 
     // ---- gather: fills (first chunk, then overflow chunks), original column
@@ -297,20 +491,11 @@ __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_glob
     const double S = s.a_val[m - 1];
 
     // ---- L column k into the pool (row order), D_k
-    if (pool_end - pool_cur < m) {
-        int64_t grab = m > kPoolGrab ? (int64_t)m : (int64_t)kPoolGrab;
-        unsigned long long got = 0;
-        if (lane == 0) got = atomicAdd(a.pool_cursor, (unsigned long long)grab);
-        got = __shfl_sync(kFull, got, 0);
-        if ((int64_t)got + grab > a.pool_cap) {
-            if (lane == 0) fail(a, kDevCapacity);
-            return false;
-        }
-        pool_cur = (int64_t)got;
-        pool_end = (int64_t)got + grab;
+    int64_t pbase = 0;
+    if (!pool_take(a, m, lane, pool_cur, pool_end, pbase)) {
+        if (lane == 0) fail(a, kDevCapacity);
+        return false;
     }
-    const int64_t pbase = pool_cur;
-    pool_cur += m;
     fills += m - 1;
     if (lane == 0) {
         a.diag[k] = S;
@@ -355,33 +540,10 @@ __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_glob
     // released
     __threadfence();
     __syncwarp();
-    const unsigned lt = (1u << lane) - 1u;
     for (int base = 0; base < m; base += kWarp) {
         const int i = base + lane;
-        bool ready = false;
-        int32_t r = -1;
-        if (i < m) {
-            const int mult = (int)(s.b_aux[i] >> 32);
-            r = s.b_row[i];
-            atomicMax(a.level + r, lk);
-            ready = atom_add_acq_rel(a.dep + r, -mult) == mult;
-        }
-        unsigned bal = __ballot_sync(kFull, ready);
-        if (bal && next < 0) {  // keep the first released neighbour for this warp
-            const int leader = __ffs(bal) - 1;
-            next = __shfl_sync(kFull, r, leader);
-            if (lane == leader) ready = false;
-            bal &= bal - 1u;
-        }
-        if (bal) {  // the rest go to the global queue, one reservation per warp
-            int slot = 0;
-            if (lane == 0) slot = atomicAdd(a.counters + kQTail, __popc(bal));
-            slot = __shfl_sync(kFull, slot, 0) + __popc(bal & lt);
-            if (ready) {
-                if (slot < a.n) st_release(a.queue + slot, r);
-                else fail(a, kDevBadInput);
-            }
-        }
+        const bool valid = i < m;
+        release_chunk(a, lk, lane, valid, valid ? s.b_row[i] : -1, valid ? (int)(s.b_aux[i] >> 32) : 0, next);
     }
     __syncwarp();
     return true;
@@ -397,10 +559,16 @@ __global__ void __launch_bounds__(256) factor_kernel(FactorArgs a) {
     int64_t pool_cur = 0, pool_end = 0;
     long long fills = 0;
     int32_t next = -1;
+    int max_gather = 0;
+    int done_local = 0;  // eliminations not yet added to the global count
     while (true) {
         int k = next;
         next = -1;
         if (k < 0) {
+            // publish finished work before waiting: other warps end their
+            // waits once the global count reaches n
+            if (lane == 0 && done_local) atomicAdd(a.counters + kDone, done_local);
+            done_local = 0;
             // pop: reserve the next queue slot and wait for its vertex.  A
             // slot may never be filled (vertices released to the warp that
             // freed them skip the queue), so the wait also ends once every
@@ -425,10 +593,12 @@ __global__ void __launch_bounds__(256) factor_kernel(FactorArgs a) {
             if (k < 0) break;
         }
         __threadfence();
-        if (!eliminate(a, k, sm, warp_global, lane, pool_cur, pool_end, fills, next)) break;
-        if (lane == 0) atomicAdd(a.counters + kDone, 1);
+        if (!eliminate(a, k, sm, warp_global, lane, pool_cur, pool_end, fills, next, max_gather)) break;
+        ++done_local;
         if (aborted(a)) break;
     }
+    if (lane == 0 && done_local) atomicAdd(a.counters + kDone, done_local);
+    if (lane == 0 && max_gather) atomicMax(a.counters + kMaxGather, max_gather);
     if (lane == 0 && fills) atomicAdd(a.pool_cursor + 1, (unsigned long long)fills);
 }
 

@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <vector>
+
 namespace rchol {
 
 // Bump allocator for the temporaries of one assembly (reset per call):
@@ -240,6 +242,22 @@ cudaError_t pcg_solve(PcgSolver* s, const double* dB, double* dX, SolveResult* r
 void pcg_destroy(PcgSolver* s);
 // Mean device time of spmv_update / fwd / bwd over `reps` iterations.
 cudaError_t pcg_profile(PcgSolver* s, const double* dB, double* dX, int reps, float* ms_out);
+
+// Batched independent systems stacked block-diagonally (rows grouped by
+// system, offsets h_off[nsys+1]); one PCG per (system, right-hand side).
+struct BatchResult {
+    int converged = 0;
+    int status = 0;
+    float ms_total = 0, ms_iterations = 0;
+    int kernel_launches = 0, graph_launches = 0;
+    std::vector<int> iterations;      // per system (max over its columns)
+    std::vector<double> relres;       // per system, true relative residual
+};
+class BatchSolver;
+BatchSolver* batch_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cfg, int device,
+                          cudaStream_t stream, const int64_t* h_off, int nsys, cudaError_t* err);
+cudaError_t batch_solve(BatchSolver* s, const double* dB, double* dX, BatchResult* res);
+void batch_destroy(BatchSolver* s);
 
 // Kernel-level entry points used by tests/bench (one operator application).
 cudaError_t spmv_f64(const DevCsc& A, const double* x, double* y, int k, cudaStream_t s);

@@ -15,6 +15,7 @@
 // sets, no analysis phase).  Every wait is bounded by a wall-clock limit and
 // reports kDevTimeout instead of hanging.  Reductions write per-block
 // partials and the last block sums them in block order (deterministic).
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <algorithm>
@@ -102,6 +103,9 @@ struct SolveArgs {
     int reduce;              // compute reductions / scalars
     int poll_ns;             // back-off between polls of a pending value
     unsigned long long timeout_ns;
+    // batched systems: row -> system, per-(system, column) step lengths
+    const int32_t* __restrict__ seg;
+    const double* __restrict__ seg_alpha;
 };
 
 // Block-wide sum of one double per (thread, column) slot: `v` holds the
@@ -183,12 +187,18 @@ __device__ __forceinline__ double wait_value(const double* p, unsigned long long
                                              int* status, bool& ok, int poll_ns) {
     double v = ld_relaxed_f64(p);
     if (!is_pending(v)) return v;
+    // exponential back-off capped at poll_ns: waits that end soon keep
+    // polling fast, long waits stop flooding L2 with polls
     unsigned spins = 0;
+    unsigned sleep_ns = 16;
     while (true) {
-        if (poll_ns > 0) __nanosleep(poll_ns);
+        if (poll_ns > 0 && spins >= 2) {
+            __nanosleep(sleep_ns);
+            sleep_ns = min(2u * sleep_ns, (unsigned)poll_ns);
+        }
         v = ld_relaxed_f64(p);
         if (!is_pending(v)) return v;
-        if ((++spins & 255u) == 0 && timed_out(t0, limit)) {
+        if ((++spins & 63u) == 0 && timed_out(t0, limit)) {
             raise_error(status, kDevTimeout);
             ok = false;
             return 0.0;
@@ -382,7 +392,7 @@ __global__ void __launch_bounds__(kBlock) spmv_update_kernel(SolveArgs a) {
 template <int K, typename TV>
 __global__ void __launch_bounds__(kBlock) fwd_kernel(SolveArgs a) {
     // K >= 2 right-hand sides: K lanes per row, lane c owns column c
-    if (a.reduce && ld_relaxed(&a.sc->done)) return;
+    if ((a.reduce || a.seg) && ld_relaxed(&a.sc->done)) return;
     constexpr int G = K;
     const int lane = threadIdx.x & 31;
     const int c = lane % G;
@@ -399,8 +409,9 @@ __global__ void __launch_bounds__(kBlock) fwd_kernel(SolveArgs a) {
         const size_t o = (size_t)i * K + c;
         double ri = a.r[o];
         if (a.update) {
-            a.x[o] = a.x[o] + alpha * a.p[o];
-            ri = ri - alpha * a.q[o];
+            const double al = a.seg ? a.seg_alpha[(size_t)a.seg[i] * K + c] : alpha;
+            a.x[o] = a.x[o] + al * a.p[o];
+            ri = ri - al * a.q[o];
             a.r[o] = ri;
             acc += ri * ri;
         }
@@ -431,7 +442,7 @@ __global__ void __launch_bounds__(kBlock) fwd_kernel(SolveArgs a) {
 template <int K, typename TV>
 __global__ void __launch_bounds__(kBlock) bwd_kernel(SolveArgs a) {
     // K >= 2 right-hand sides: K lanes per row, lane c owns column c
-    if (a.reduce && ld_relaxed(&a.sc->done)) return;
+    if ((a.reduce || a.seg) && ld_relaxed(&a.sc->done)) return;
     constexpr int G = K;
     const int lane = threadIdx.x & 31;
     const int c = lane % G;
@@ -521,7 +532,7 @@ __device__ __forceinline__ double group_sum(double v, int G) {
 
 template <typename TV>
 __global__ void __launch_bounds__(kBlock) fwd_task_kernel(SolveArgs a) {
-    if (a.reduce && ld_relaxed(&a.sc->done)) return;
+    if ((a.reduce || a.seg) && ld_relaxed(&a.sc->done)) return;
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -550,8 +561,9 @@ __global__ void __launch_bounds__(kBlock) fwd_task_kernel(SolveArgs a) {
         if (active && gl == 0) {
             double ri = a.r[i];
             if (a.update) {
-                a.x[i] = a.x[i] + alpha * a.p[i];
-                ri = ri - alpha * a.q[i];
+                const double al = a.seg ? a.seg_alpha[a.seg[i]] : alpha;
+                a.x[i] = a.x[i] + al * a.p[i];
+                ri = ri - al * a.q[i];
                 a.r[i] = ri;
                 acc[0] += ri * ri;
             }
@@ -577,7 +589,7 @@ __global__ void __launch_bounds__(kBlock) fwd_task_kernel(SolveArgs a) {
 
 template <typename TV>
 __global__ void __launch_bounds__(kBlock) bwd_task_kernel(SolveArgs a) {
-    if (a.reduce && ld_relaxed(&a.sc->done)) return;
+    if ((a.reduce || a.seg) && ld_relaxed(&a.sc->done)) return;
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -771,6 +783,8 @@ class PcgSolver {
         a.reduce = 1;
         a.poll_ns = cfg.poll_ns;
         a.timeout_ns = (unsigned long long)(cfg.timeout_s * 1e9);
+        a.seg = nullptr;
+        a.seg_alpha = nullptr;
         return a;
     }
 
@@ -1045,6 +1059,481 @@ cudaError_t pcg_profile(PcgSolver* s, const double* dB, double* dX, int reps, fl
     for (int q = 0; q < 3; ++q) ms_out[q] = (float)(acc[q] / std::max(reps, 1));
     s->cfg = keep;
     return e;
+}
+
+
+// ===========================================================================
+// Batched independent systems (block-diagonal matrix, one PCG per system and
+// right-hand side).  Rows are grouped by system; the dot products reduce
+// over fixed row chunks (a chunk spans at most two systems) and then over
+// the chunks of each system in order, so the sums are deterministic.
+// One iteration: batch_spmv (q, p, p.q -> alpha per pair), fwd (x, r, y),
+// bwd (z), batch_dots (r.r, r.z -> convergence, beta per pair).
+// ===========================================================================
+
+struct BatchScalarsDev {
+    double *alpha, *beta, *rz, *rz0, *rr, *pq, *bnorm2, *tr2, *rzn;
+    int *active, *iters;
+};
+
+struct BatchArgs {
+    int32_t n;
+    int32_t nsys;
+    int32_t chunk;           // rows per reduction chunk
+    int32_t nchunks;
+    const int32_t* __restrict__ seg;          // row -> system
+    const int64_t* __restrict__ sys_off;      // [nsys+1]
+    const int32_t* __restrict__ a_ptr;
+    const int32_t* __restrict__ a_idx;
+    const double* __restrict__ a_val;
+    const double* __restrict__ b;
+    double *x, *r, *p, *q, *y, *z;
+    double* part;            // [nchunks][2 slots][K]
+    BatchScalarsDev s;
+    PcgScalars* sc;          // global flags: done, iter, phase, status, tickets
+    double tol;
+    int max_iter;
+    int stop_rule;
+};
+
+// Per-chunk, per-column sums of (va for the chunk's first system, vb for
+// the second); thread column = lane % K.  Deterministic block reduction.
+template <int K>
+__device__ void chunk_store(double va, double vb, double* out /* [2][K] */) {
+    __shared__ double red[2][kBlock / 32][K];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o >= K; o >>= 1) {
+        va += __shfl_xor_sync(kFull, va, o);
+        vb += __shfl_xor_sync(kFull, vb, o);
+    }
+    if (lane < K) {
+        red[0][w][lane] = va;
+        red[1][w][lane] = vb;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * K) {
+        const int slot = threadIdx.x / K, c = threadIdx.x % K;
+        double t = 0.0;
+        for (int i = 0; i < kBlock / 32; ++i) t += red[slot][i][c];
+        out[slot * K + c] = t;
+    }
+    __syncthreads();
+}
+
+// Sum of the chunk partials of every (system, column) pair into out[pair]:
+// one warp per pair, lanes over the system's chunks, fixed tree.
+template <int K>
+__device__ void reduce_pairs(const BatchArgs& a, const double* part, double* out) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int pairs = a.nsys * K;
+    for (int pr = w; pr < pairs; pr += kBlock / 32) {
+        const int sys = pr / K, c = pr % K;
+        const int64_t r0 = a.sys_off[sys], r1 = a.sys_off[sys + 1];
+        double t = 0.0;
+        if (r1 > r0) {
+            const int64_t c0 = r0 / a.chunk, c1 = (r1 - 1) / a.chunk;
+            for (int64_t ch = c0 + lane; ch <= c1; ch += 32) {
+                const int slot = a.seg[ch * a.chunk] == sys ? 0 : 1;
+                t += part[(size_t)ch * 2 * K + slot * K + c];
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(kFull, t, o);
+        if (lane == 0) out[pr] = t;
+    }
+    __syncthreads();
+}
+
+// Row loop of one chunk: fn(row, column) returns the row's contribution.
+template <int K, typename F>
+__device__ void chunk_rows(const BatchArgs& a, int64_t ch, F fn, double& va, double& vb) {
+    const int64_t r0 = ch * a.chunk;
+    const int64_t r1 = min((int64_t)a.n, r0 + a.chunk);
+    const int first = a.seg[r0];
+    const int c = threadIdx.x % K;
+    for (int64_t i = r0 + threadIdx.x / K; i < r1; i += kBlock / K) {
+        const double v = fn(i, c);
+        if (a.seg[i] == first) va += v;
+        else vb += v;
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(kBlock) batch_init_kernel(BatchArgs a) {
+    for (int64_t ch = blockIdx.x; ch < a.nchunks; ch += gridDim.x) {
+        double va = 0.0, vb = 0.0;
+        chunk_rows<K>(a, ch, [&](int64_t i, int c) {
+            const size_t o = (size_t)i * K + c;
+            const double bv = a.b[o];
+            a.x[o] = 0.0;
+            a.r[o] = bv;
+            a.p[o] = 0.0;
+            a.q[o] = 0.0;
+            a.y[o] = pending_value();
+            return bv * bv;
+        }, va, vb);
+        chunk_store<K>(va, vb, a.part + (size_t)ch * 2 * K);
+    }
+    if (last_block(&a.sc->ticket[0])) {
+        reduce_pairs<K>(a, a.part, a.s.bnorm2);
+        for (int pr = threadIdx.x; pr < a.nsys * K; pr += kBlock) {
+            a.s.alpha[pr] = 0.0;
+            a.s.beta[pr] = 0.0;
+            a.s.rz[pr] = 0.0;
+            a.s.active[pr] = a.s.bnorm2[pr] > 0.0 ? 1 : 0;
+            a.s.iters[pr] = 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int any = 0;
+            for (int pr = 0; pr < a.nsys * K; ++pr) any |= a.s.active[pr];
+            a.sc->done = any ? 0 : 1;
+            a.sc->iter = 0;
+            a.sc->phase = 0;
+            a.sc->status = 0;
+            a.sc->ticket[0] = 0;
+        }
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(kBlock) batch_spmv_kernel(BatchArgs a) {
+    if (ld_relaxed(&a.sc->done)) return;
+    for (int64_t ch = blockIdx.x; ch < a.nchunks; ch += gridDim.x) {
+        double va = 0.0, vb = 0.0;
+        chunk_rows<K>(a, ch, [&](int64_t i, int c) {
+            const double beta = a.s.beta[(size_t)a.seg[i] * K + c];
+            const double sum = row_dot_plain<K>(a.a_idx, a.a_val, a.a_ptr[i], a.a_ptr[i + 1], a.z, c);
+            const size_t o = (size_t)i * K + c;
+            const double qi = sum + beta * a.q[o];
+            const double pi = a.z[o] + beta * a.p[o];
+            a.q[o] = qi;
+            a.p[o] = pi;
+            a.y[o] = pending_value();
+            return pi * qi;
+        }, va, vb);
+        chunk_store<K>(va, vb, a.part + (size_t)ch * 2 * K);
+    }
+    if (last_block(&a.sc->ticket[1])) {
+        reduce_pairs<K>(a, a.part, a.s.pq);
+        for (int pr = threadIdx.x; pr < a.nsys * K; pr += kBlock) {
+            const double pq = a.s.pq[pr];
+            a.s.alpha[pr] = (a.s.active[pr] && pq != 0.0) ? a.s.rz[pr] / pq : 0.0;
+        }
+        if (threadIdx.x == 0) a.sc->ticket[1] = 0;
+    }
+}
+
+// r.r and r.z per pair; phase 0 initialises rz, otherwise beta, the stop
+// test and the iteration count.
+template <int K>
+__global__ void __launch_bounds__(kBlock) batch_dots_kernel(BatchArgs a) {
+    if (ld_relaxed(&a.sc->done)) return;
+    double* part_rr = a.part;
+    double* part_rz = a.part + (size_t)a.nchunks * 2 * K;
+    for (int64_t ch = blockIdx.x; ch < a.nchunks; ch += gridDim.x) {
+        double va = 0.0, vb = 0.0, wa = 0.0, wb = 0.0;
+        const int64_t r0 = ch * a.chunk;
+        const int64_t r1 = min((int64_t)a.n, r0 + a.chunk);
+        const int first = a.seg[r0];
+        const int c = threadIdx.x % K;
+        for (int64_t i = r0 + threadIdx.x / K; i < r1; i += kBlock / K) {
+            const size_t o = (size_t)i * K + c;
+            const double ri = a.r[o], zi = a.z[o];
+            if (a.seg[i] == first) {
+                va += ri * ri;
+                wa += ri * zi;
+            } else {
+                vb += ri * ri;
+                wb += ri * zi;
+            }
+        }
+        chunk_store<K>(va, vb, part_rr + (size_t)ch * 2 * K);
+        chunk_store<K>(wa, wb, part_rz + (size_t)ch * 2 * K);
+    }
+    if (last_block(&a.sc->ticket[3])) {
+        reduce_pairs<K>(a, part_rr, a.s.rr);
+        reduce_pairs<K>(a, part_rz, a.s.rzn);
+        const bool init = a.sc->phase == 0;
+        const int it = init ? a.sc->iter : a.sc->iter + 1;
+        for (int pr = threadIdx.x; pr < a.nsys * K; pr += kBlock) {
+            if (!a.s.active[pr]) {
+                a.s.beta[pr] = 0.0;
+                continue;
+            }
+            const double rn = a.s.rzn[pr];
+            if (init) {
+                a.s.rz[pr] = rn;
+                a.s.rz0[pr] = rn;
+                a.s.beta[pr] = 0.0;
+                continue;
+            }
+            a.s.iters[pr] = it;
+            bool conv = false;
+            if (a.stop_rule == 0) conv = sqrt(a.s.rr[pr]) <= a.tol * sqrt(a.s.bnorm2[pr]);
+            else if (a.stop_rule == 2) conv = a.s.rr[pr] <= a.tol;
+            else conv = !(sqrt(rn) / sqrt(a.s.rz0[pr]) > a.tol);
+            const double ro = a.s.rz[pr];
+            a.s.beta[pr] = ro != 0.0 ? rn / ro : 0.0;
+            a.s.rz[pr] = rn;
+            if (conv) a.s.active[pr] = 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int any = 0;
+            for (int pr = 0; pr < a.nsys * K; ++pr) any |= a.s.active[pr];
+            a.sc->iter = it;
+            a.sc->phase = 1;
+            if (!any || it >= a.max_iter) a.sc->done = 1;
+            a.sc->ticket[3] = 0;
+        }
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(kBlock) batch_true_kernel(BatchArgs a) {
+    for (int64_t ch = blockIdx.x; ch < a.nchunks; ch += gridDim.x) {
+        double va = 0.0, vb = 0.0;
+        chunk_rows<K>(a, ch, [&](int64_t i, int c) {
+            const double sum = row_dot_plain<K>(a.a_idx, a.a_val, a.a_ptr[i], a.a_ptr[i + 1], a.x, c);
+            const double t = a.b[(size_t)i * K + c] - sum;
+            return t * t;
+        }, va, vb);
+        chunk_store<K>(va, vb, a.part + (size_t)ch * 2 * K);
+    }
+    if (last_block(&a.sc->ticket[0])) {
+        reduce_pairs<K>(a, a.part, a.s.tr2);
+        if (threadIdx.x == 0) a.sc->ticket[0] = 0;
+    }
+}
+
+class BatchSolver {
+   public:
+    PcgSolver* base = nullptr;       // vectors, factor kernels, scalars struct
+    BatchArgs ba;
+    int32_t* seg = nullptr;
+    int64_t* off = nullptr;
+    double* pool = nullptr;          // per-pair scalars
+    int* ipool = nullptr;
+    double* part = nullptr;
+    int grid = 0;
+    void *k_init = nullptr, *k_spmv = nullptr, *k_dots = nullptr, *k_true = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    const double* gb = nullptr;
+    double* gx = nullptr;
+    std::vector<double> h_tr2, h_b2;
+    std::vector<int> h_iters;
+
+    BatchArgs args(const double* b, double* x) {
+        BatchArgs a = ba;
+        a.b = b;
+        a.x = x;
+        return a;
+    }
+    SolveArgs solve_args(const double* b, double* x) {
+        SolveArgs a = base->args(b, x);
+        a.reduce = 0;
+        a.update = 1;
+        a.seg = seg;
+        a.seg_alpha = ba.s.alpha;
+        return a;
+    }
+    cudaError_t launch(void* fn, int g, void* arg) {
+        void* params[] = {arg};
+        return cudaLaunchKernel(fn, dim3(g), dim3(kBlock), params, 0, base->stream);
+    }
+    cudaError_t iteration(const double* b, double* x) {
+        BatchArgs a = args(b, x);
+        SolveArgs sa = solve_args(b, x);
+        cudaError_t e;
+        if ((e = launch(k_spmv, grid, &a)) != cudaSuccess) return e;
+        if ((e = launch(base->k_fwd, base->grid_fwd, &sa)) != cudaSuccess) return e;
+        if ((e = launch(base->k_bwd, base->grid_bwd, &sa)) != cudaSuccess) return e;
+        return launch(k_dots, grid, &a);
+    }
+};
+
+template <int K>
+static void bind_batch(BatchSolver* s) {
+    s->k_init = (void*)batch_init_kernel<K>;
+    s->k_spmv = (void*)batch_spmv_kernel<K>;
+    s->k_dots = (void*)batch_dots_kernel<K>;
+    s->k_true = (void*)batch_true_kernel<K>;
+}
+
+BatchSolver* batch_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cfg, int device,
+                          cudaStream_t stream, const int64_t* h_off, int nsys, cudaError_t* err) {
+    *err = cudaSuccess;
+    // the smallest system bounds the chunk (a chunk must span <= 2 systems)
+    int64_t minsys = INT64_MAX;
+    for (int i = 0; i < nsys; ++i) minsys = std::min(minsys, h_off[i + 1] - h_off[i]);
+    if (nsys < 1 || minsys < 32 || h_off[nsys] != A.n) {
+        *err = cudaErrorInvalidValue;
+        return nullptr;
+    }
+    PcgSolver* base = pcg_create(A, F, cfg, device, stream, err);
+    if (!base) return nullptr;
+    BatchSolver* s = new BatchSolver();
+    s->base = base;
+    switch (cfg.k) {
+        case 1: bind_batch<1>(s); break;
+        case 2: bind_batch<2>(s); break;
+        case 4: bind_batch<4>(s); break;
+        case 8: bind_batch<8>(s); break;
+        case 16: bind_batch<16>(s); break;
+        case 32: bind_batch<32>(s); break;
+        default: *err = cudaErrorInvalidValue; batch_destroy(s); return nullptr;
+    }
+    int64_t chunk = 32;
+    while (chunk * 2 <= std::min<int64_t>(minsys, 4096)) chunk *= 2;
+    const int K = cfg.k;
+    const int64_t pairs = (int64_t)nsys * K;
+    BatchArgs& a = s->ba;
+    a.n = A.n;
+    a.nsys = nsys;
+    a.chunk = (int32_t)chunk;
+    a.nchunks = (int32_t)ceil_div(A.n, chunk);
+    a.a_ptr = A.colptr;
+    a.a_idx = A.rowind;
+    a.a_val = A.val;
+    a.r = base->r;
+    a.p = base->p;
+    a.q = base->q;
+    a.y = base->y;
+    a.z = base->z;
+    a.sc = base->sc;
+    a.tol = cfg.tol;
+    a.max_iter = cfg.max_iter;
+    a.stop_rule = cfg.stop_rule;
+    std::vector<int32_t> hseg((size_t)A.n);
+    for (int i = 0; i < nsys; ++i)
+        for (int64_t r = h_off[i]; r < h_off[i + 1]; ++r) hseg[(size_t)r] = i;
+    cudaError_t e = cudaMalloc(&s->seg, sizeof(int32_t) * hseg.size());
+    if (e == cudaSuccess) e = cudaMemcpy(s->seg, hseg.data(), sizeof(int32_t) * hseg.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&s->off, sizeof(int64_t) * (size_t)(nsys + 1));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(s->off, h_off, sizeof(int64_t) * (size_t)(nsys + 1), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&s->pool, sizeof(double) * (size_t)pairs * 9);
+    if (e == cudaSuccess) e = cudaMalloc(&s->ipool, sizeof(int) * (size_t)pairs * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&s->part, sizeof(double) * (size_t)a.nchunks * 2 * K * 2);
+    if (e != cudaSuccess) {
+        *err = e;
+        batch_destroy(s);
+        return nullptr;
+    }
+    a.seg = s->seg;
+    a.sys_off = s->off;
+    a.part = s->part;
+    double* P = s->pool;
+    a.s.alpha = P;
+    a.s.beta = P + pairs;
+    a.s.rz = P + 2 * pairs;
+    a.s.rz0 = P + 3 * pairs;
+    a.s.rr = P + 4 * pairs;
+    a.s.pq = P + 5 * pairs;
+    a.s.bnorm2 = P + 6 * pairs;
+    a.s.tr2 = P + 7 * pairs;
+    a.s.rzn = P + 8 * pairs;
+    a.s.active = s->ipool;
+    a.s.iters = s->ipool + pairs;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    s->grid = (int)std::min<int64_t>(a.nchunks, (int64_t)sms * 8);
+    return s;
+}
+
+void batch_destroy(BatchSolver* s) {
+    if (!s) return;
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    cudaFree(s->seg);
+    cudaFree(s->off);
+    cudaFree(s->pool);
+    cudaFree(s->ipool);
+    cudaFree(s->part);
+    pcg_destroy(s->base);
+    delete s;
+}
+
+cudaError_t batch_solve(BatchSolver* s, const double* dB, double* dX, BatchResult* res) {
+    PcgSolver* b = s->base;
+    const int K = b->K;
+    const int nsys = s->ba.nsys;
+    const int64_t pairs = (int64_t)nsys * K;
+    cudaError_t e;
+    if (b->cfg.use_graph && !(s->graph && s->gb == dB && s->gx == dX)) {
+        if (s->graph) cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+        cudaGraph_t g = nullptr;
+        if ((e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+        cudaError_t ce = cudaSuccess;
+        for (int u = 0; u < b->cfg.unroll && ce == cudaSuccess; ++u) ce = s->iteration(dB, dX);
+        e = cudaStreamEndCapture(b->stream, &g);
+        if (ce != cudaSuccess) return ce;
+        if (e != cudaSuccess) return e;
+        e = cudaGraphInstantiate(&s->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return e;
+        s->gb = dB;
+        s->gx = dX;
+    }
+    cudaEventRecord(b->ev0, b->stream);
+    BatchArgs a = s->args(dB, dX);
+    if ((e = s->launch(s->k_init, s->grid, &a)) != cudaSuccess) return e;
+    {  // start: z = M r, rz per pair
+        SolveArgs sa = s->solve_args(dB, dX);
+        sa.update = 0;
+        if ((e = s->launch(b->k_fwd, b->grid_fwd, &sa)) != cudaSuccess) return e;
+        if ((e = s->launch(b->k_bwd, b->grid_bwd, &sa)) != cudaSuccess) return e;
+        if ((e = s->launch(s->k_dots, s->grid, &a)) != cudaSuccess) return e;
+    }
+    cudaEventRecord(b->ev1, b->stream);
+    res->kernel_launches = 4;
+    res->graph_launches = 0;
+    while (true) {
+        if (b->cfg.use_graph) {
+            if ((e = cudaGraphLaunch(s->graph, b->stream)) != cudaSuccess) return e;
+            res->graph_launches++;
+        } else {
+            for (int u = 0; u < b->cfg.unroll; ++u)
+                if ((e = s->iteration(dB, dX)) != cudaSuccess) return e;
+        }
+        res->kernel_launches += 4 * b->cfg.unroll;
+        if ((e = cudaMemcpyAsync(b->sc_host, b->sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, b->stream)) !=
+            cudaSuccess)
+            return e;
+        if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return e;
+        if (b->sc_host->done) break;
+    }
+    if ((e = s->launch(s->k_true, s->grid, &a)) != cudaSuccess) return e;
+    res->kernel_launches++;
+    cudaEventRecord(b->ev2, b->stream);
+    s->h_tr2.resize((size_t)pairs);
+    s->h_b2.resize((size_t)pairs);
+    s->h_iters.resize((size_t)pairs);
+    cudaMemcpyAsync(s->h_tr2.data(), s->ba.s.tr2, sizeof(double) * pairs, cudaMemcpyDeviceToHost, b->stream);
+    cudaMemcpyAsync(s->h_b2.data(), s->ba.s.bnorm2, sizeof(double) * pairs, cudaMemcpyDeviceToHost, b->stream);
+    cudaMemcpyAsync(s->h_iters.data(), s->ba.s.iters, sizeof(int) * pairs, cudaMemcpyDeviceToHost, b->stream);
+    cudaMemcpyAsync(b->sc_host, b->sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, b->stream);
+    if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return e;
+    cudaEventElapsedTime(&res->ms_total, b->ev0, b->ev2);
+    cudaEventElapsedTime(&res->ms_iterations, b->ev1, b->ev2);
+    res->status = b->sc_host->status;
+    res->iterations.assign((size_t)nsys, 0);
+    res->relres.assign((size_t)nsys, 0.0);
+    res->converged = 1;
+    for (int sys = 0; sys < nsys; ++sys) {
+        for (int c = 0; c < K; ++c) {
+            const size_t pr = (size_t)sys * K + c;
+            const double bn = std::sqrt(s->h_b2[pr]);
+            const double rel = bn > 0 ? std::sqrt(s->h_tr2[pr]) / bn : 0.0;
+            res->iterations[(size_t)sys] = std::max(res->iterations[(size_t)sys], s->h_iters[pr]);
+            res->relres[(size_t)sys] = std::max(res->relres[(size_t)sys], rel);
+            if (b->cfg.stop_rule == 0 && rel > b->cfg.tol) res->converged = 0;
+        }
+    }
+    if (res->status != 0) res->converged = 0;
+    return cudaSuccess;
 }
 
 // ---- single operator applications ----------------------------------------

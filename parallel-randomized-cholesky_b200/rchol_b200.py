@@ -31,7 +31,8 @@ EXPORTS = [
     "rchol_read_mtx", "rchol_matrix_info", "rchol_matrix_copy_to_host", "rchol_factor", "rchol_factor_get_info",
     "rchol_factor_copy_to_host", "rchol_factor_write", "rchol_factor_read", "rchol_factor_from_csr_upper",
     "rchol_factor_free", "rchol_pcg_solve", "rchol_precond_apply", "rchol_profile_solve", "rchol_spmv", "rchol_factorization_driver",
-    "rchol_prepare_and_solve", "rchol_generate", "rchol_free_host", "rchol_write_mtx",
+    "rchol_prepare_and_solve", "rchol_generate", "rchol_free_host", "rchol_write_mtx", "rchol_batch_set",
+    "rchol_batch_solve",
 ]
 
 
@@ -59,6 +60,10 @@ class FactorInfo(C.Structure):
                 ("solve_depth", C.c_int), ("kernel_launches", C.c_int),
                 ("lc_ptr", C.c_void_p), ("lc_idx", C.c_void_p), ("lc_val", C.c_void_p),
                 ("lr_ptr", C.c_void_p), ("lr_idx", C.c_void_p), ("lr_val", C.c_void_p), ("diag", C.c_void_p)]
+
+
+class System(C.Structure):
+    _fields_ = [("n", C.c_int), ("colptr", C.c_void_p), ("rowind", C.c_void_p), ("val", C.c_void_p)]
 
 
 class SolveInfo(C.Structure):
@@ -125,6 +130,9 @@ def lib():
         L.rchol_free_host.argtypes = [vp]
         L.rchol_free_host.restype = None
         L.rchol_write_mtx.argtypes = [C.c_char_p, C.c_int, C.c_longlong, vp, vp, vp]
+        L.rchol_batch_set.argtypes = [vp, C.c_int, C.POINTER(System), C.POINTER(C.c_longlong)]
+        L.rchol_batch_solve.argtypes = [vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, C.POINTER(SolveInfo),
+                                        C.POINTER(SolveInfo)]
         _lib = L
     return _lib
 
@@ -369,6 +377,41 @@ class Context:
         _check(lib().rchol_precond_apply(self.h, factor.h, k, Rf.ctypes.data_as(C.c_void_p),
                                          Z.ctypes.data_as(C.c_void_p), n, 0, int(fp32)), self.h)
         return Z[:, 0].copy() if vec else np.ascontiguousarray(Z)
+
+    def batch_set(self, systems):
+        """systems: list of (n, colptr, rowind, val) preprocessed CSC arrays.
+        Returns the row offsets of the block-diagonal stacking."""
+        keep = []
+        arr = (System * len(systems))()
+        for q, (n, cp, ri, v) in enumerate(systems):
+            cp = np.ascontiguousarray(cp, np.int32)
+            ri = np.ascontiguousarray(ri, np.int32)
+            v = np.ascontiguousarray(v, np.float64)
+            keep += [cp, ri, v]
+            arr[q] = System(n, _ptr(cp), _ptr(ri), _ptr(v))
+        off = (C.c_longlong * (len(systems) + 1))()
+        _check(lib().rchol_batch_set(self.h, len(systems), arr, off), self.h)
+        self.batch_offsets = np.array(off[:], np.int64)
+        return self.batch_offsets
+
+    def batch_solve(self, factor, B):
+        """B: (n_total,) or (n_total, k); returns X, per-system info, total info."""
+        B = np.asarray(B, np.float64)
+        vec = B.ndim == 1
+        Bm = B.reshape(-1, 1) if vec else B
+        n, k = Bm.shape
+        Bf = np.asfortranarray(Bm)
+        X = np.zeros((n, k), np.float64, order="F")
+        nsys = len(self.batch_offsets) - 1
+        per = (SolveInfo * nsys)()
+        tot = SolveInfo()
+        st = lib().rchol_batch_solve(self.h, factor.h, k, Bf.ctypes.data_as(C.c_void_p),
+                                     X.ctypes.data_as(C.c_void_p), n, 0, per, C.byref(tot))
+        if st not in (OK, 6):
+            _check(st, self.h)
+        info = _struct_dict(tot)
+        info["status"] = st
+        return (X[:, 0].copy() if vec else np.ascontiguousarray(X)), [_struct_dict(p) for p in per], info
 
     def profile_solve(self, factor, k=1, reps=5):
         """Mean ms of (spmv_update, fwd, bwd) per iteration."""
