@@ -171,6 +171,24 @@ rchol_status rchol_pcg_solve(rchol_ctx* ctx, const rchol_factor_t* f, int k, con
 /* One preconditioner application Z = L^-T D^+ L^-1 R (same layout rules). */
 rchol_status rchol_precond_apply(rchol_ctx* ctx, const rchol_factor_t* f, int k, const double* R, double* Z,
                                  int ldb, int on_device, int fp32);
+/* Allocation-free variant of rchol_precond_apply, Z = L^-T D^+ L^-1 R, for
+ * callers that must not allocate device memory: code running inside another
+ * framework's memory budget (a caching allocator that already holds most of
+ * HBM, where a cudaMalloc can fail) and latency-sensitive loops, where
+ * cudaMalloc/cudaFree stall because they synchronise with the device.  R and
+ * Z are caller-owned DEVICE arrays, row-major n x k (R[i*k + c]), that must
+ * not overlap; k in {1,2,4,8,16,32}; stream may be NULL (legacy default
+ * stream).  The call returns after the stream has finished the apply.
+ * Scratch is one fixed array in the library's device code, limited to
+ * n * k <= 4194304 (2^22 doubles, 32 MiB, plus 4 KiB for scalars); larger
+ * sizes return RCHOL_ERR_INVALID.  The first call on each device looks up
+ * that array's address (this may load the library's device code), so make
+ * it before any stream capture.  All calls on a device share the array:
+ * calls that overlap on the GPU (other threads or streams) race on it and
+ * must be serialised by the caller.  No counterpart in the reference, which
+ * allocates its solver work vectors for each solve. */
+rchol_status rchol_precond_apply_noalloc(const rchol_factor_t* f, int k, const double* R, double* Z, int fp32,
+                                         void* stream);
 /* Mean device time (ms) of the three PCG iteration kernels over `reps`
  * iterations on this factor with k right-hand sides: ms_out[0] SpMV +
  * vector update, ms_out[1] forward solve, ms_out[2] backward solve. */

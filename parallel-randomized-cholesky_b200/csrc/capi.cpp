@@ -926,6 +926,27 @@ extern "C" rchol_status rchol_precond_apply(rchol_ctx* ctx, const rchol_factor_t
     return RCHOL_OK;
 }
 
+extern "C" rchol_status rchol_precond_apply_noalloc(const rchol_factor_t* f, int k, const double* R, double* Z,
+                                                    int fp32, void* stream) {
+    if (!f) return RCHOL_ERR_INVALID;
+    rchol_ctx* ctx = f->ctx;
+    if (!R || !Z) return fail(ctx, RCHOL_ERR_INVALID, "null argument");
+    if (!valid_k(k)) return fail(ctx, RCHOL_ERR_INVALID, "k must be 1, 2, 4, 8, 16 or 32");
+    if (fp32 && !f->F.lr_val32) return fail(ctx, RCHOL_ERR_INVALID, "factor has no FP32 copy");
+    if ((long long)f->F.n * k > rchol::kNoAllocMaxElems)
+        return fail(ctx, RCHOL_ERR_INVALID,
+                    "precond_apply_noalloc: n * k = " + std::to_string((long long)f->F.n * k) +
+                        " exceeds the allocation-free limit of " + std::to_string(rchol::kNoAllocMaxElems) +
+                        " elements");
+    if (ctx) cudaSetDevice(ctx->device);
+    int status = 0;
+    CK(rchol::precond_apply_noalloc(f->F, R, Z, k, fp32 != 0, &status, ctx ? ctx->o.timeout_s : 30.0,
+                                    (cudaStream_t)stream),
+       "precond apply (no alloc)");
+    if (status != 0) return fail(ctx, RCHOL_ERR_TIMEOUT, "precond apply: a device wait timed out");
+    return RCHOL_OK;
+}
+
 extern "C" rchol_status rchol_profile_solve(rchol_ctx* ctx, const rchol_factor_t* f, int k, int reps,
                                             float* ms_out) {
     if (!ctx || !f || !ms_out || reps < 1) return fail(ctx, RCHOL_ERR_INVALID, "bad argument");

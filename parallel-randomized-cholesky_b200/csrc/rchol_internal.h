@@ -266,5 +266,14 @@ cudaError_t cm_to_rm(const double* cm, int ld, double* rm, int32_t n, int k, cud
 cudaError_t rm_to_cm(const double* rm, double* cm, int ld, int32_t n, int k, cudaStream_t s);
 cudaError_t precond_apply(const DevFactor& F, const double* r, double* z, double* ywork, int k,
                           bool fp32, int* status, double timeout_s, cudaStream_t s);
+// Largest n * k accepted by precond_apply_noalloc (its y vector lives in a
+// fixed module array of this many doubles, 32 MiB, plus a 4 KiB header).
+constexpr long long kNoAllocMaxElems = 1LL << 22;
+// precond_apply on caller-provided device vectors (row-major n x k) with no
+// device allocation: scratch comes from the module array, located once per
+// device on first use.  Returns cudaErrorInvalidValue when n * k exceeds
+// kNoAllocMaxElems.
+cudaError_t precond_apply_noalloc(const DevFactor& F, const double* r, double* z, int k, bool fp32, int* status,
+                                  double timeout_s, cudaStream_t s);
 
 }  // namespace rchol

@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -1649,6 +1650,115 @@ cudaError_t precond_apply(const DevFactor& F, const double* r, double* z, double
             return cudaErrorInvalidValue;
     }
 #undef RCHOL_PA
+}
+
+// ---- allocation-free preconditioner apply --------------------------------
+// The same forward and backward sweeps as precond_apply, with every piece of
+// device scratch (the PCG scalar block that carries the wait status, and the
+// n x k forward-solve vector y) taken from one statically sized module
+// array instead of cudaMalloc.  All calls on a device share that array and
+// leave their contents in it; two calls whose kernels overlap on the GPU
+// race on it.
+
+constexpr int kNoAllocHeadDoubles = 512;  // 4 KiB: the PcgScalars block
+static_assert(sizeof(PcgScalars) <= kNoAllocHeadDoubles * sizeof(double), "scalar block does not fit");
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocHeadDoubles + kNoAllocMaxElems];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_base[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on `device` (which must be current),
+// looked up once per device; the lookup may load this module onto the device.
+cudaError_t noalloc_scratch(int device, double** out) {
+    if (device < 0 || device >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> guard(g_noalloc_mu);
+    if (!g_noalloc_base[device]) {
+        double* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_base[device] = p;
+    }
+    *out = g_noalloc_base[device];
+    return cudaSuccess;
+}
+
+template <int K, typename TV>
+cudaError_t precond_apply_noalloc_t(const DevFactor& F, const double* r, double* z, double* scratch, int* status,
+                                    double timeout_s, cudaStream_t s, int device) {
+    PcgScalars* sc = reinterpret_cast<PcgScalars*>(scratch);
+    double* y = scratch + kNoAllocHeadDoubles;
+    // the status word and counters must start at zero; y starts "pending"
+    cudaError_t e = cudaMemsetAsync(sc, 0, sizeof(PcgScalars), s);
+    if (e != cudaSuccess) return e;
+    SolveArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = F.n;
+    a.lr_ptr = F.sf_ptr;
+    a.lr_idx = F.sf_idx;
+    a.lr_val = std::is_same<TV, float>::value ? (const void*)F.sf_val32 : (const void*)F.sf_val;
+    a.lc_ptr = F.sb_ptr;
+    a.lc_idx = F.sb_idx;
+    a.lc_val = std::is_same<TV, float>::value ? (const void*)F.sb_val32 : (const void*)F.sb_val;
+    a.diag = std::is_same<TV, float>::value ? (const void*)F.diag32 : (const void*)F.diag;
+    a.order_f = F.order_f;
+    a.order_b = F.order_b;
+    a.tasks_f = F.tasks_f;
+    a.tasks_b = F.tasks_b;
+    a.ntasks_f = F.ntasks_f;
+    a.ntasks_b = F.ntasks_b;
+    a.r = const_cast<double*>(r);
+    a.y = y;
+    a.z = z;
+    a.sc = sc;
+    a.update = 0;
+    a.reduce = 0;
+    a.timeout_ns = (unsigned long long)(timeout_s * 1e9);
+    fill_pending_kernel<<<148 * 8, kBlock, 0, s>>>(y, (int64_t)F.n * K);
+    if (K == 1) {
+        fwd_task_kernel<TV><<<resident_blocks((void*)fwd_task_kernel<TV>, device), kBlock, 0, s>>>(a);
+        bwd_task_kernel<TV><<<resident_blocks((void*)bwd_task_kernel<TV>, device), kBlock, 0, s>>>(a);
+    } else {
+        fwd_kernel<K, TV><<<resident_blocks((void*)fwd_kernel<K, TV>, device), kBlock, 0, s>>>(a);
+        bwd_kernel<K, TV><<<resident_blocks((void*)bwd_kernel<K, TV>, device), kBlock, 0, s>>>(a);
+    }
+    e = cudaGetLastError();
+    int st = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&st, &sc->status, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    *status = st;
+    return e;
+}
+
+}  // namespace
+
+cudaError_t precond_apply_noalloc(const DevFactor& F, const double* r, double* z, int k, bool fp32, int* status,
+                                  double timeout_s, cudaStream_t s) {
+    if ((long long)F.n * k > kNoAllocMaxElems) return cudaErrorInvalidValue;
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    double* scratch = nullptr;
+    e = noalloc_scratch(device, &scratch);
+    if (e != cudaSuccess) return e;
+#define RCHOL_PAN(KK)                                                                                        \
+    case KK:                                                                                                 \
+        return fp32 ? precond_apply_noalloc_t<KK, float>(F, r, z, scratch, status, timeout_s, s, device)     \
+                    : precond_apply_noalloc_t<KK, double>(F, r, z, scratch, status, timeout_s, s, device);
+    switch (k) {
+        RCHOL_PAN(1)
+        RCHOL_PAN(2)
+        RCHOL_PAN(4)
+        RCHOL_PAN(8)
+        RCHOL_PAN(16)
+        RCHOL_PAN(32)
+        default:
+            return cudaErrorInvalidValue;
+    }
+#undef RCHOL_PAN
 }
 
 }  // namespace rchol

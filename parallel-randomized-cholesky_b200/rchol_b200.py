@@ -30,7 +30,7 @@ EXPORTS = [
     "rchol_last_error", "rchol_load_mtx", "rchol_set_triplets", "rchol_set_csc", "rchol_csc_from_triplets",
     "rchol_read_mtx", "rchol_matrix_info", "rchol_matrix_copy_to_host", "rchol_factor", "rchol_factor_get_info",
     "rchol_factor_copy_to_host", "rchol_factor_write", "rchol_factor_read", "rchol_factor_from_csr_upper",
-    "rchol_factor_free", "rchol_pcg_solve", "rchol_precond_apply", "rchol_profile_solve", "rchol_spmv", "rchol_factorization_driver",
+    "rchol_factor_free", "rchol_pcg_solve", "rchol_precond_apply", "rchol_precond_apply_noalloc", "rchol_profile_solve", "rchol_spmv", "rchol_factorization_driver",
     "rchol_prepare_and_solve", "rchol_generate", "rchol_free_host", "rchol_write_mtx", "rchol_batch_set",
     "rchol_batch_solve",
 ]
@@ -118,6 +118,7 @@ def lib():
         L.rchol_factor_free.restype = None
         L.rchol_pcg_solve.argtypes = [vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, C.POINTER(SolveInfo)]
         L.rchol_precond_apply.argtypes = [vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int]
+        L.rchol_precond_apply_noalloc.argtypes = [vp, C.c_int, vp, vp, C.c_int, vp]
         L.rchol_spmv.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.c_int]
         L.rchol_profile_solve.argtypes = [vp, vp, C.c_int, C.c_int, C.POINTER(C.c_float)]
         L.rchol_factorization_driver.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_int]
@@ -377,6 +378,14 @@ class Context:
         _check(lib().rchol_precond_apply(self.h, factor.h, k, Rf.ctypes.data_as(C.c_void_p),
                                          Z.ctypes.data_as(C.c_void_p), n, 0, int(fp32)), self.h)
         return Z[:, 0].copy() if vec else np.ascontiguousarray(Z)
+
+    def precond_apply_noalloc(self, factor, r_ptr, z_ptr, k=1, fp32=False, stream=0):
+        """Z = M^+ R on caller-owned device arrays (row-major n x k, given as
+        integer device addresses) without any device allocation; scratch is
+        a fixed library array (n * k <= 2**22), shared by every call on the
+        device, so overlapping calls must be serialised by the caller."""
+        _check(lib().rchol_precond_apply_noalloc(factor.h, int(k), C.c_void_p(r_ptr), C.c_void_p(z_ptr), int(fp32),
+                                                 C.c_void_p(stream or None)), self.h)
 
     def batch_set(self, systems):
         """systems: list of (n, colptr, rowind, val) preprocessed CSC arrays.
