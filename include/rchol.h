@@ -65,7 +65,7 @@ typedef struct rchol_opts {
     int verbose;              /* print phase timings (the reference's stdout) */
     int poll_ns;              /* back-off (ns) between polls in the triangular solves */
     int sched_epl;            /* triangular-solve schedule: matrix entries per lane (1..64) */
-    int exact_bwd_levels;     /* order the backward solve by its true DAG levels */
+    int exact_bwd_levels;     /* order the backward solve by its true DAG levels (default 1) */
 } rchol_opts;
 
 typedef struct rchol_factor_info {

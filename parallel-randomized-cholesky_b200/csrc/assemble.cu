@@ -274,6 +274,78 @@ __global__ void sched_task_emit_kernel(const int32_t* __restrict__ hist, const i
     }
 }
 
+// slots per lane of each task: the longest of its rows over G lanes
+__global__ void pack_m_kernel(const int2* __restrict__ tasks, int32_t ntasks, const int64_t* __restrict__ optr,
+                              int32_t* m) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntasks; t += stride) {
+        const int2 d = tasks[t];
+        const int cls = d.y >> 8, cnt = d.y & 0xff;
+        int64_t longest = 0;
+        for (int r = 0; r < cnt; ++r) longest = max(longest, optr[d.x + r + 1] - optr[d.x + r]);
+        m[t] = (int32_t)((longest + (1 << cls) - 1) >> cls);
+    }
+}
+
+__global__ void pack_desc_kernel(const int2* __restrict__ tasks, int32_t ntasks, const int32_t* __restrict__ m,
+                                 const int64_t* __restrict__ base, int4* pack) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntasks; t += stride) {
+        const int2 d = tasks[t];
+        pack[t] = make_int4(d.x, (int32_t)base[t], d.y, m[t]);
+    }
+}
+
+// One warp per task: slot (k, lane) <- entry k*G + lane%G of row lane/G,
+// except that entry 0 and the row's gate trade places.  The gate is the
+// dependency scheduled last (largest sign * level; the first such entry on
+// ties): the solve polls it alone before reading the rest of the row.
+__global__ void pack_fill_kernel(const int4* __restrict__ pack, int32_t ntasks, const int64_t* __restrict__ optr,
+                                 const int32_t* __restrict__ sidx, const double* __restrict__ sval,
+                                 const float* __restrict__ sval32, const int32_t* __restrict__ level, int sign,
+                                 int32_t* pidx, double* pval, float* pval32) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < ntasks; t += warps) {
+        const int4 d = pack[t];
+        const int cls = (d.z >> 8) & 7, cnt = d.z & 0xff;
+        const int G = 1 << cls;
+        const int r = lane >> cls, gl = lane & (G - 1);
+        int64_t s = 0, len = 0;
+        if (r < cnt) {
+            s = optr[d.x + r];
+            len = optr[d.x + r + 1] - s;
+        }
+        // gate of the row: best (key, entry) over the lane's entries, then over the G lanes
+        long long best_key = LLONG_MIN, best_e = 0;
+        for (int64_t e = gl; e < len; e += G) {
+            const long long key = (long long)sign * level[sidx[s + e]];
+            if (key > best_key) {
+                best_key = key;
+                best_e = e;
+            }
+        }
+        for (int o = 1; o < G; o <<= 1) {
+            const long long ok = __shfl_xor_sync(0xffffffffu, best_key, o);
+            const long long oe = __shfl_xor_sync(0xffffffffu, best_e, o);
+            if (ok > best_key || (ok == best_key && oe < best_e)) {
+                best_key = ok;
+                best_e = oe;
+            }
+        }
+        for (int k = 0; k < d.w; ++k) {
+            int64_t e = ((int64_t)k << cls) + gl;
+            const size_t o = ((size_t)d.y + k) * 32 + lane;
+            const bool have = e < len;
+            if (have && e == 0) e = best_e;
+            else if (have && e == best_e) e = 0;
+            pidx[o] = have ? sidx[s + e] : -1;
+            pval[o] = have ? sval[s + e] : 0.0;
+            if (pval32) pval32[o] = have ? sval32[s + e] : 0.0f;
+        }
+    }
+}
+
 // rows in schedule order: position p copies row order[p] of (ptr, idx, val)
 __global__ void permute_len_kernel(int32_t n, const int32_t* __restrict__ order, const int64_t* __restrict__ ptr,
                                    int32_t* len) {
@@ -533,9 +605,50 @@ static cudaError_t build_layout(int32_t n, const int32_t* order, const int64_t* 
     return cudaGetLastError();
 }
 
+// Task slabs of one direction from its task list and schedule-ordered layout.
+static cudaError_t build_pack(int32_t ntasks, const int2* tasks, const int64_t* optr, const int32_t* sidx,
+                              const double* sval, const float* sval32, const int32_t* level, int sign, int4** pack, int64_t& cap_d, int32_t** pidx,
+                              int64_t& cap_i, double** pval, int64_t& cap_v, float** pval32, int64_t& cap_w,
+                              int64_t* slots, Scratch& sc, cudaStream_t s) {
+    int32_t* m = nullptr;
+    int64_t* base = nullptr;
+    void* tmp = nullptr;
+    const int64_t nt = std::max<int32_t>(ntasks, 1);
+    RCHOL_TRY(sc.get(&m, nt));
+    RCHOL_TRY(sc.get(&base, nt + 1));
+    RCHOL_TRY(sc.get((char**)&tmp, (int64_t)scan_tmp_bytes(nt)));
+    RCHOL_TRY(ensure(pack, cap_d, nt));
+    if (ntasks == 0) {
+        *slots = 0;
+        return cudaSuccess;
+    }
+    pack_m_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(tasks, ntasks, optr, m);
+    RCHOL_TRY(exclusive_scan_i32_to_i64(m, base, ntasks, tmp, s));
+    int64_t units = 0;
+    RCHOL_TRY(cudaMemcpyAsync(&units, base + ntasks, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RCHOL_TRY(cudaStreamSynchronize(s));
+    if (units >= (int64_t)INT32_MAX) return cudaErrorInvalidValue;  // slab offsets are int32 units
+    const int64_t nslots = std::max<int64_t>(units * 32, 32);
+    *slots = units * 32;
+    RCHOL_TRY(ensure(pidx, cap_i, nslots));
+    RCHOL_TRY(ensure(pval, cap_v, nslots));
+    if (sval32) {
+        RCHOL_TRY(ensure(pval32, cap_w, nslots));
+    } else {
+        cudaFree(*pval32);
+        *pval32 = nullptr;
+        cap_w = 0;
+    }
+    pack_desc_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(tasks, ntasks, m, base, *pack);
+    pack_fill_kernel<<<grid_for((int64_t)ntasks * 32, 256), 256, 0, s>>>(
+        *pack, ntasks, optr, sidx, sval, sval32, level, sign, *pidx, *pval, sval32 ? *pval32 : nullptr);
+    return cudaGetLastError();
+}
+
 // The solve layouts (schedule-ordered copies of Lr and Lc) for the orders
 // already built; FP32 values are copied when the factor has them.
-static cudaError_t build_layouts(DevFactor& f, Scratch& sc, cudaStream_t s) {
+static cudaError_t build_layouts(DevFactor& f, const int32_t* level_f, const int32_t* level_b, int sign_b,
+                                 Scratch& sc, cudaStream_t s) {
     const bool grow_n = f.cap_ln < (int64_t)f.n + 1;
     const int64_t capn = std::max<int64_t>(f.cap_ln, (int64_t)f.n + 1);
     RCHOL_TRY(realloc_if(&f.sf_ptr, grow_n, capn));
@@ -561,6 +674,12 @@ static cudaError_t build_layouts(DevFactor& f, Scratch& sc, cudaStream_t s) {
                            f.sf_val32, sc, s));
     RCHOL_TRY(build_layout(f.n, f.order_b, f.lc_ptr, f.lc_idx, f.lc_val, f.lc_val32, f.sb_ptr, f.sb_idx, f.sb_val,
                            f.sb_val32, sc, s));
+    RCHOL_TRY(build_pack(f.ntasks_f, f.tasks_f, f.sf_ptr, f.sf_idx, f.sf_val, f.sf_val32, level_f, 1, &f.pack_f,
+                         f.cap_pdf,
+                         &f.pf_idx, f.cap_pif, &f.pf_val, f.cap_pvf, &f.pf_val32, f.cap_pwf, &f.slots_f, sc, s));
+    RCHOL_TRY(build_pack(f.ntasks_b, f.tasks_b, f.sb_ptr, f.sb_idx, f.sb_val, f.sb_val32, level_b, sign_b, &f.pack_b,
+                         f.cap_pdb,
+                         &f.pb_idx, f.cap_pib, &f.pb_val, f.cap_pvb, &f.pb_val32, f.cap_pwb, &f.slots_b, sc, s));
     return cudaSuccess;
 }
 
@@ -582,7 +701,8 @@ cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bo
                                  &f.ntasks_b, s));
     f.depth_b = f.depth;
     if (!exact_bwd || f.n == 0) {
-        RCHOL_TRY(build_layouts(f, sc, s));
+        // reversed forward levels: the backward gate is the dependency of least forward level
+        RCHOL_TRY(build_layouts(f, level, level, -1, sc, s));
         return cudaStreamSynchronize(s);
     }
     // true backward levels, visited in the reversed-forward order just built
@@ -606,7 +726,7 @@ cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bo
     f.depth_b = hs[1] + 1;
     RCHOL_TRY(build_one_schedule(levb, f.lc_ptr, f.n, f.depth_b, 0, epl, sc, f.order_b, &f.tasks_b, f.cap_tb,
                                  &f.ntasks_b, s));
-    RCHOL_TRY(build_layouts(f, sc, s));
+    RCHOL_TRY(build_layouts(f, level, levb, 1, sc, s));
     return cudaStreamSynchronize(s);
 }
 

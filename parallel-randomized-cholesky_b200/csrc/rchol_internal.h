@@ -152,6 +152,23 @@ struct DevFactor {
     int32_t* sb_idx = nullptr;
     double* sb_val = nullptr;
     float* sb_val32 = nullptr;
+    // Task slabs of the K = 1 solves.  Task t (descriptor int4 {first
+    // position, slab offset in 32-slot units, row count | log2(G) << 8,
+    // slots per lane m}) owns slots (d.y + k) * 32 + lane, k < m: lane
+    // lane/G-th row of the task, entry k * G + lane % G of that row (index
+    // -1 and value 0 past the row's end).  All of a lane's entries are thus
+    // addressable from the descriptor alone and load in one round trip.
+    int4* pack_f = nullptr;
+    int4* pack_b = nullptr;
+    int32_t* pf_idx = nullptr;
+    double* pf_val = nullptr;
+    float* pf_val32 = nullptr;
+    int32_t* pb_idx = nullptr;
+    double* pb_val = nullptr;
+    float* pb_val32 = nullptr;
+    int64_t slots_f = 0, slots_b = 0;
+    int64_t cap_pdf = 0, cap_pdb = 0, cap_pif = 0, cap_pib = 0, cap_pvf = 0, cap_pvb = 0, cap_pwf = 0,
+            cap_pwb = 0;
     int32_t depth = 0;        // number of levels of the forward solve DAG
     int32_t depth_b = 0;      // levels of the backward schedule
     // allocated capacities (buffers of a released factor are reused)

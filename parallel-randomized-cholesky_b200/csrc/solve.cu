@@ -81,8 +81,13 @@ struct SolveArgs {
     const void* __restrict__ diag;
     const int32_t* __restrict__ order_f;  // forward-solve row order
     const int32_t* __restrict__ order_b;  // backward-solve row order
-    const int2* __restrict__ tasks_f;
-    const int2* __restrict__ tasks_b;
+    // K = 1 task slabs (see DevFactor::pack_f)
+    const int4* __restrict__ pack_f;
+    const int4* __restrict__ pack_b;
+    const int32_t* __restrict__ pf_idx;
+    const void* __restrict__ pf_val;
+    const int32_t* __restrict__ pb_idx;
+    const void* __restrict__ pb_val;
     int32_t ntasks_f, ntasks_b;
     // vectors (n x K row-major)
     const double* __restrict__ b;
@@ -491,35 +496,173 @@ __global__ void __launch_bounds__(kBlock) bwd_kernel(SolveArgs a) {
 
 // Strided partial dot product of one lane of a G-lane row group: entries
 // s+gl, s+gl+G, ... fetched four at a time.
+// ---- K = 1 solves over task slabs ------------------------------------------
+// A warp takes the tasks warp, warp + nwarps, ... in schedule order.  While
+// it waits on the dependencies of one task, the slab entries, row indices
+// and row data of its next task are already in flight, so a task's critical
+// path after its last dependency lands is one poll round trip, a short
+// dot product and one store.
+
+constexpr int kPackM = 4;  // slab slots per lane held in registers
+#ifndef RCHOL_TRICKLE
+#define RCHOL_TRICKLE 2
+#endif
+constexpr unsigned kTrickle = RCHOL_TRICKLE;
+// 4 CTAs of 256 threads per SM (64 registers): more warps for the wide
+// levels outweigh the few spilled registers
+#ifndef RCHOL_PACK_MINB
+#define RCHOL_PACK_MINB 4
+#endif  // gate rounds per re-read of the other pending slots (0: none)
+
 template <typename TV>
-__device__ __forceinline__ double group_dot(const int32_t* __restrict__ idx, const TV* __restrict__ val, int64_t s,
-                                            int64_t e, int gl, int G, const double* vec, unsigned long long t0,
-                                            unsigned long long limit, int* status, bool& ok, int poll_ns) {
-    double sum = 0.0;
-    int64_t p = s + gl;
-    const int64_t G4 = 4ll * G;
-    for (; p + 3 * G < e; p += G4) {
-        const double* q0 = vec + idx[p];
-        const double* q1 = vec + idx[p + G];
-        const double* q2 = vec + idx[p + 2 * G];
-        const double* q3 = vec + idx[p + 3 * G];
-        const double l0 = to_d(val[p]), l1 = to_d(val[p + G]), l2 = to_d(val[p + 2 * G]), l3 = to_d(val[p + 3 * G]);
-        double v0 = ld_relaxed_f64(q0), v1 = ld_relaxed_f64(q1);
-        double v2 = ld_relaxed_f64(q2), v3 = ld_relaxed_f64(q3);
-        if (is_pending(v0)) v0 = wait_value(q0, t0, limit, status, ok, poll_ns);
-        if (is_pending(v1)) v1 = wait_value(q1, t0, limit, status, ok, poll_ns);
-        if (is_pending(v2)) v2 = wait_value(q2, t0, limit, status, ok, poll_ns);
-        if (is_pending(v3)) v3 = wait_value(q3, t0, limit, status, ok, poll_ns);
-        sum += l0 * v0;
-        sum += l1 * v1;
-        sum += l2 * v2;
-        sum += l3 * v3;
+struct PackLane {
+    int4 d;
+    int32_t row;
+    int32_t idx[kPackM];
+    TV val[kPackM];
+};
+
+template <typename TV>
+__device__ __forceinline__ void pack_load(PackLane<TV>& L, const int4 d, int lane, const int32_t* __restrict__ order,
+                                          const int32_t* __restrict__ pidx, const TV* __restrict__ pval) {
+    L.d = d;
+    const int cls = (d.z >> 8) & 7, cnt = d.z & 0xff;
+    L.row = (lane >> cls) < cnt ? order[d.x + (lane >> cls)] : 0;
+    const size_t o = (size_t)d.y * 32 + lane;
+#pragma unroll
+    for (int k = 0; k < kPackM; ++k) {
+        if (k < d.w) {
+            L.idx[k] = pidx[o + 32 * k];
+            L.val[k] = pval[o + 32 * k];
+        } else {
+            L.idx[k] = -1;
+            L.val[k] = TV(0);
+        }
     }
-    for (; p < e; p += G) {
-        const double* q = vec + idx[p];
-        double v = ld_relaxed_f64(q);
-        if (is_pending(v)) v = wait_value(q, t0, limit, status, ok, poll_ns);
-        sum += to_d(val[p]) * v;
+}
+
+// Re-reads the pending components of v (bit k of pend) together until none
+// is pending; false on timeout.
+__device__ __forceinline__ bool poll_pending(double (&v)[kPackM], const int32_t (&idx)[kPackM], const double* vec,
+                                             unsigned pend, unsigned long long t0, unsigned long long limit,
+                                             int* status, int poll_ns) {
+    unsigned spins = 0, sleep_ns = 16;
+    while (pend) {
+        if (poll_ns > 0 && spins >= 2) {
+            __nanosleep(sleep_ns);
+            sleep_ns = min(2u * sleep_ns, (unsigned)poll_ns);
+        }
+#pragma unroll
+        for (int k = 0; k < kPackM; ++k)
+            if ((pend >> k) & 1u) v[k] = ld_relaxed_f64(vec + idx[k]);
+        pend = 0;
+#pragma unroll
+        for (int k = 0; k < kPackM; ++k) pend |= (is_pending(v[k]) ? 1u : 0u) << k;
+        if (pend && (++spins & 63u) == 0 && timed_out(t0, limit)) {
+            raise_error(status, kDevTimeout);
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ unsigned pending_mask(const double (&v)[kPackM]) {
+    unsigned pend = 0;
+#pragma unroll
+    for (int k = 0; k < kPackM; ++k) pend |= (is_pending(v[k]) ? 1u : 0u) << k;
+    return pend;
+}
+
+// The lane's share of its row's dot product.  Slot 0 of the row's first
+// lane holds the row's gate, its dependency scheduled last.  Every slot is
+// read once; rows whose gate is still pending then poll the gate alone
+// (every kTrickle-th round also re-reading their other pending slots), so
+// the values just produced at the solve front are polled by few rows; once
+// the gate has landed the remaining pending slots are polled together.
+// Slots beyond the first kPackM of long rows are fetched at the start and
+// waited on together with the first ones; rows longer than 2 * kPackM slots
+// per lane continue kPackM slots at a time.
+template <typename TV>
+__device__ __forceinline__ void slab_chunk(const PackLane<TV>& L, int k0, int lane, const int32_t* __restrict__ pidx,
+                                           const TV* __restrict__ pval, int32_t (&idx)[kPackM], TV (&val)[kPackM]) {
+    const size_t o = ((size_t)L.d.y + k0) * 32 + lane;
+#pragma unroll
+    for (int k = 0; k < kPackM; ++k) {
+        if (k0 + k < L.d.w) {
+            idx[k] = pidx[o + 32 * k];
+            val[k] = pval[o + 32 * k];
+        } else {
+            idx[k] = -1;
+            val[k] = TV(0);
+        }
+    }
+}
+
+template <typename TV>
+__device__ __forceinline__ double pack_dot(const PackLane<TV>& L, int lane, int G, const int32_t* __restrict__ pidx,
+                                           const TV* __restrict__ pval, const double* vec, unsigned long long t0,
+                                           unsigned long long limit, int* status, bool& ok, int poll_ns) {
+    // slots kPackM..2*kPackM-1 of long rows: fetched now, waited on with the rest
+    int32_t idx2[kPackM];
+    TV val2[kPackM];
+    const bool two = L.d.w > kPackM;
+    if (two) slab_chunk(L, kPackM, lane, pidx, pval, idx2, val2);
+    double v[kPackM], v2[kPackM];
+#pragma unroll
+    for (int k = 0; k < kPackM; ++k) v[k] = L.idx[k] >= 0 ? ld_relaxed_f64(vec + L.idx[k]) : 0.0;
+    if (two) {
+#pragma unroll
+        for (int k = 0; k < kPackM; ++k) v2[k] = idx2[k] >= 0 ? ld_relaxed_f64(vec + idx2[k]) : 0.0;
+    }
+    const bool first = (lane & (G - 1)) == 0;
+    bool gate = first && is_pending(v[0]);
+    unsigned spins = 0;
+    while (__any_sync(kFull, gate)) {
+        if (gate) {
+            v[0] = ld_relaxed_f64(vec + L.idx[0]);
+            gate = is_pending(v[0]);
+        }
+        ++spins;
+        if (kTrickle > 0 && spins % kTrickle == 0) {
+#pragma unroll
+            for (int k = 0; k < kPackM; ++k)
+                if ((k > 0 || !first) && is_pending(v[k])) v[k] = ld_relaxed_f64(vec + L.idx[k]);
+            if (two) {
+#pragma unroll
+                for (int k = 0; k < kPackM; ++k)
+                    if (is_pending(v2[k])) v2[k] = ld_relaxed_f64(vec + idx2[k]);
+            }
+        }
+        if ((spins & 63u) == 0 && __shfl_sync(kFull, timed_out(t0, limit) ? 1 : 0, 0)) {
+            if (gate) raise_error(status, kDevTimeout);
+            ok = false;
+            return 0.0;
+        }
+    }
+    if (!poll_pending(v, L.idx, vec, pending_mask(v), t0, limit, status, poll_ns) ||
+        (two && !poll_pending(v2, idx2, vec, pending_mask(v2), t0, limit, status, poll_ns))) {
+        ok = false;
+        return 0.0;
+    }
+    double sum = 0.0;
+#pragma unroll
+    for (int k = 0; k < kPackM; ++k) sum += to_d(L.val[k]) * v[k];
+    if (two) {
+#pragma unroll
+        for (int k = 0; k < kPackM; ++k) sum += to_d(val2[k]) * v2[k];
+    }
+    for (int k0 = 2 * kPackM; k0 < L.d.w && ok; k0 += kPackM) {
+        int32_t idx[kPackM];
+        TV val[kPackM];
+        slab_chunk(L, k0, lane, pidx, pval, idx, val);
+#pragma unroll
+        for (int k = 0; k < kPackM; ++k) v[k] = idx[k] >= 0 ? ld_relaxed_f64(vec + idx[k]) : 0.0;
+        if (!poll_pending(v, idx, vec, pending_mask(v), t0, limit, status, poll_ns)) {
+            ok = false;
+            break;
+        }
+#pragma unroll
+        for (int k = 0; k < kPackM; ++k) sum += to_d(val[k]) * v[k];
     }
     return sum;
 }
@@ -531,47 +674,47 @@ __device__ __forceinline__ double group_sum(double v, int G) {
     return v;
 }
 
+// y = L^-1 r (with update: x += alpha p, r -= alpha q, ||r||^2 first)
 template <typename TV>
-__global__ void __launch_bounds__(kBlock) fwd_task_kernel(SolveArgs a) {
+__global__ void __launch_bounds__(kBlock, RCHOL_PACK_MINB) fwd_pack_kernel(SolveArgs a) {
     if ((a.reduce || a.seg) && ld_relaxed(&a.sc->done)) return;
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const TV* __restrict__ lv = reinterpret_cast<const TV*>(a.lr_val);
+    const TV* __restrict__ pval = reinterpret_cast<const TV*>(a.pf_val);
     const double alpha = a.update ? a.sc->alpha[0] : 0.0;
     double acc[1] = {0.0};
     const unsigned long long t0 = global_timer_ns();
     bool ok = true;
-    int2 dn = warp < a.ntasks_f ? a.tasks_f[warp] : make_int2(0, 0);
+    PackLane<TV> cur, nxt;
+    if (warp < a.ntasks_f) pack_load(cur, a.pack_f[warp], lane, a.order_f, a.pf_idx, pval);
+    int4 dn = warp + nwarps < a.ntasks_f ? a.pack_f[warp + nwarps] : make_int4(0, 0, 0, 0);
     for (int64_t t = warp; t < a.ntasks_f && ok; t += nwarps) {
-        const int2 d = dn;
-        if (t + nwarps < a.ntasks_f) dn = a.tasks_f[t + nwarps];  // next descriptor in flight
-        const int G = 1 << (d.y >> 8);
-        const int cnt = d.y & 0xff;
-        const int r = lane / G, gl = lane % G;
-        const bool active = r < cnt;
-        int64_t i = 0;
-        double sum = 0.0;
-        if (active) {
-            const int64_t p = d.x + r;
-            i = a.order_f[p];
-            sum = group_dot<TV>(a.lr_idx, lv, a.lr_ptr[p], a.lr_ptr[p + 1], gl, G, a.y, t0, a.timeout_ns,
-                                &a.sc->status, ok, a.poll_ns);
-        }
-        sum = group_sum(sum, G);
-        if (active && gl == 0) {
-            double ri = a.r[i];
+        const int cls = (cur.d.z >> 8) & 7, cnt = cur.d.z & 0xff;
+        const int G = 1 << cls;
+        const bool lead = (lane >> cls) < cnt && (lane & (G - 1)) == 0;
+        const int32_t i = cur.row;
+        // row data and the x / r update do not depend on the dot product
+        double ri = 0.0;
+        if (lead) {
+            ri = a.r[i];
             if (a.update) {
                 const double al = a.seg ? a.seg_alpha[a.seg[i]] : alpha;
-                a.x[i] = a.x[i] + al * a.p[i];
-                ri = ri - al * a.q[i];
+                const double xi = a.x[i], pi = a.p[i], qi = a.q[i];
+                a.x[i] = xi + al * pi;
+                ri = ri - al * qi;
                 a.r[i] = ri;
                 acc[0] += ri * ri;
             }
             if (a.z) a.z[i] = pending_value();
-            st_relaxed_f64(a.y + i, ri - sum);
         }
+        if (t + nwarps < a.ntasks_f) pack_load(nxt, dn, lane, a.order_f, a.pf_idx, pval);
+        if (t + 2 * nwarps < a.ntasks_f) dn = a.pack_f[t + 2 * nwarps];
+        double sum = pack_dot<TV>(cur, lane, G, a.pf_idx, pval, a.y, t0, a.timeout_ns, &a.sc->status, ok, a.poll_ns);
+        sum = group_sum(sum, G);
+        if (lead) st_relaxed_f64(a.y + i, ri - sum);
         ok = __all_sync(kFull, ok);
+        cur = nxt;
     }
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) a.sc->done = 1;
@@ -588,43 +731,44 @@ __global__ void __launch_bounds__(kBlock) fwd_task_kernel(SolveArgs a) {
     }
 }
 
+// z = L^-T D^+ y (with reduce: r.z -> beta, stop test)
 template <typename TV>
-__global__ void __launch_bounds__(kBlock) bwd_task_kernel(SolveArgs a) {
+__global__ void __launch_bounds__(kBlock, RCHOL_PACK_MINB) bwd_pack_kernel(SolveArgs a) {
     if ((a.reduce || a.seg) && ld_relaxed(&a.sc->done)) return;
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const TV* __restrict__ lv = reinterpret_cast<const TV*>(a.lc_val);
+    const TV* __restrict__ pval = reinterpret_cast<const TV*>(a.pb_val);
     const TV* __restrict__ dv = reinterpret_cast<const TV*>(a.diag);
     double acc[1] = {0.0};
     const unsigned long long t0 = global_timer_ns();
     bool ok = true;
-    int2 dn = warp < a.ntasks_b ? a.tasks_b[warp] : make_int2(0, 0);
+    PackLane<TV> cur, nxt;
+    if (warp < a.ntasks_b) pack_load(cur, a.pack_b[warp], lane, a.order_b, a.pb_idx, pval);
+    int4 dn = warp + nwarps < a.ntasks_b ? a.pack_b[warp + nwarps] : make_int4(0, 0, 0, 0);
     for (int64_t t = warp; t < a.ntasks_b && ok; t += nwarps) {
-        const int2 d = dn;
-        if (t + nwarps < a.ntasks_b) dn = a.tasks_b[t + nwarps];  // next descriptor in flight
-        const int G = 1 << (d.y >> 8);
-        const int cnt = d.y & 0xff;
-        const int r = lane / G, gl = lane % G;
-        const bool active = r < cnt;
-        int64_t j = 0;
-        double sum = 0.0;
-        if (active) {
-            const int64_t p = d.x + r;
-            j = a.order_b[p];
-            sum = group_dot<TV>(a.lc_idx, lv, a.lc_ptr[p], a.lc_ptr[p + 1], gl, G, a.z, t0, a.timeout_ns,
-                                &a.sc->status, ok, a.poll_ns);
-        }
-        sum = group_sum(sum, G);
-        if (active && gl == 0) {
+        const int cls = (cur.d.z >> 8) & 7, cnt = cur.d.z & 0xff;
+        const int G = 1 << cls;
+        const bool lead = (lane >> cls) < cnt && (lane & (G - 1)) == 0;
+        const int32_t j = cur.row;
+        double tj = 0.0, rj = 0.0;
+        if (lead) {
             const double dj = to_d(dv[j]);
-            double tj = a.y[j];
+            tj = a.y[j];
             if (dj != 0.0) tj = tj / dj;
+            if (a.reduce) rj = a.r[j];
+        }
+        if (t + nwarps < a.ntasks_b) pack_load(nxt, dn, lane, a.order_b, a.pb_idx, pval);
+        if (t + 2 * nwarps < a.ntasks_b) dn = a.pack_b[t + 2 * nwarps];
+        double sum = pack_dot<TV>(cur, lane, G, a.pb_idx, pval, a.z, t0, a.timeout_ns, &a.sc->status, ok, a.poll_ns);
+        sum = group_sum(sum, G);
+        if (lead) {
             const double zj = tj - sum;
             st_relaxed_f64(a.z + j, zj);
-            if (a.reduce) acc[0] += a.r[j] * zj;
+            if (a.reduce) acc[0] += rj * zj;
         }
         ok = __all_sync(kFull, ok);
+        cur = nxt;
     }
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) a.sc->done = 1;
@@ -749,6 +893,7 @@ class PcgSolver {
 
     SolveArgs args(const double* b, double* x) const {
         SolveArgs a;
+        memset(&a, 0, sizeof(a));
         a.n = A.n;
         a.a_ptr = A.colptr;
         a.a_idx = A.rowind;
@@ -763,8 +908,12 @@ class PcgSolver {
         a.diag = cfg.fp32_factor ? (const void*)F.diag32 : (const void*)F.diag;
         a.order_f = F.order_f;
         a.order_b = F.order_b;
-        a.tasks_f = F.tasks_f;
-        a.tasks_b = F.tasks_b;
+        a.pack_f = F.pack_f;
+        a.pack_b = F.pack_b;
+        a.pf_idx = F.pf_idx;
+        a.pf_val = cfg.fp32_factor ? (const void*)F.pf_val32 : (const void*)F.pf_val;
+        a.pb_idx = F.pb_idx;
+        a.pb_val = cfg.fp32_factor ? (const void*)F.pb_val32 : (const void*)F.pb_val;
         a.ntasks_f = F.ntasks_f;
         a.ntasks_b = F.ntasks_b;
         a.b = b;
@@ -818,8 +967,8 @@ template <int K, typename TV>
 static void bind_kernels(PcgSolver* s) {
     s->k_init = (void*)init_kernel<K>;
     s->k_spmv = (void*)spmv_update_kernel<K>;
-    s->k_fwd = K == 1 ? (void*)fwd_task_kernel<TV> : (void*)fwd_kernel<K, TV>;
-    s->k_bwd = K == 1 ? (void*)bwd_task_kernel<TV> : (void*)bwd_kernel<K, TV>;
+    s->k_fwd = K == 1 ? (void*)fwd_pack_kernel<TV> : (void*)fwd_kernel<K, TV>;
+    s->k_bwd = K == 1 ? (void*)bwd_pack_kernel<TV> : (void*)bwd_kernel<K, TV>;
     s->k_true = (void*)true_residual_kernel<K>;
     s->k_restart = (void*)restart_kernel<K>;
 }
@@ -1600,8 +1749,12 @@ static cudaError_t precond_apply_t(const DevFactor& F, const double* r, double* 
     a.diag = std::is_same<TV, float>::value ? (const void*)F.diag32 : (const void*)F.diag;
     a.order_f = F.order_f;
     a.order_b = F.order_b;
-    a.tasks_f = F.tasks_f;
-    a.tasks_b = F.tasks_b;
+    a.pack_f = F.pack_f;
+    a.pack_b = F.pack_b;
+    a.pf_idx = F.pf_idx;
+    a.pf_val = std::is_same<TV, float>::value ? (const void*)F.pf_val32 : (const void*)F.pf_val;
+    a.pb_idx = F.pb_idx;
+    a.pb_val = std::is_same<TV, float>::value ? (const void*)F.pb_val32 : (const void*)F.pb_val;
     a.ntasks_f = F.ntasks_f;
     a.ntasks_b = F.ntasks_b;
     a.r = const_cast<double*>(r);
@@ -1614,10 +1767,10 @@ static cudaError_t precond_apply_t(const DevFactor& F, const double* r, double* 
     const int64_t total = (int64_t)F.n * K;
     fill_pending_kernel<<<148 * 8, kBlock, 0, s>>>(y, total);
     if (K == 1) {
-        int gf = resident_blocks((void*)fwd_task_kernel<TV>, device);
-        int gb = resident_blocks((void*)bwd_task_kernel<TV>, device);
-        fwd_task_kernel<TV><<<gf, kBlock, 0, s>>>(a);
-        bwd_task_kernel<TV><<<gb, kBlock, 0, s>>>(a);
+        int gf = resident_blocks((void*)fwd_pack_kernel<TV>, device);
+        int gb = resident_blocks((void*)bwd_pack_kernel<TV>, device);
+        fwd_pack_kernel<TV><<<gf, kBlock, 0, s>>>(a);
+        bwd_pack_kernel<TV><<<gb, kBlock, 0, s>>>(a);
     } else {
         int gf = resident_blocks((void*)fwd_kernel<K, TV>, device);
         int gb = resident_blocks((void*)bwd_kernel<K, TV>, device);
@@ -1706,8 +1859,12 @@ cudaError_t precond_apply_noalloc_t(const DevFactor& F, const double* r, double*
     a.diag = std::is_same<TV, float>::value ? (const void*)F.diag32 : (const void*)F.diag;
     a.order_f = F.order_f;
     a.order_b = F.order_b;
-    a.tasks_f = F.tasks_f;
-    a.tasks_b = F.tasks_b;
+    a.pack_f = F.pack_f;
+    a.pack_b = F.pack_b;
+    a.pf_idx = F.pf_idx;
+    a.pf_val = std::is_same<TV, float>::value ? (const void*)F.pf_val32 : (const void*)F.pf_val;
+    a.pb_idx = F.pb_idx;
+    a.pb_val = std::is_same<TV, float>::value ? (const void*)F.pb_val32 : (const void*)F.pb_val;
     a.ntasks_f = F.ntasks_f;
     a.ntasks_b = F.ntasks_b;
     a.r = const_cast<double*>(r);
@@ -1719,8 +1876,8 @@ cudaError_t precond_apply_noalloc_t(const DevFactor& F, const double* r, double*
     a.timeout_ns = (unsigned long long)(timeout_s * 1e9);
     fill_pending_kernel<<<148 * 8, kBlock, 0, s>>>(y, (int64_t)F.n * K);
     if (K == 1) {
-        fwd_task_kernel<TV><<<resident_blocks((void*)fwd_task_kernel<TV>, device), kBlock, 0, s>>>(a);
-        bwd_task_kernel<TV><<<resident_blocks((void*)bwd_task_kernel<TV>, device), kBlock, 0, s>>>(a);
+        fwd_pack_kernel<TV><<<resident_blocks((void*)fwd_pack_kernel<TV>, device), kBlock, 0, s>>>(a);
+        bwd_pack_kernel<TV><<<resident_blocks((void*)bwd_pack_kernel<TV>, device), kBlock, 0, s>>>(a);
     } else {
         fwd_kernel<K, TV><<<resident_blocks((void*)fwd_kernel<K, TV>, device), kBlock, 0, s>>>(a);
         bwd_kernel<K, TV><<<resident_blocks((void*)bwd_kernel<K, TV>, device), kBlock, 0, s>>>(a);
