@@ -190,12 +190,21 @@ __device__ __forceinline__ int sched_key(int level, int64_t len, int epl) {
     return kLaneClasses * level + lane_class(len, epl);
 }
 
+// bucket key of every row and the bucket sizes (warp-aggregated counts)
 __global__ void sched_hist_kernel(const int32_t* __restrict__ level, const int64_t* __restrict__ ptr, int32_t n,
-                                  int32_t depth, int backward, int epl, int32_t* hist) {
+                                  int32_t depth, int backward, int epl, int32_t* key, int32_t* hist) {
+    const int lane = threadIdx.x & 31;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        int l = backward ? depth - 1 - level[i] : level[i];
-        atomicAdd(hist + sched_key(l, ptr[i + 1] - ptr[i], epl), 1);
+    const int64_t n_up = ((int64_t)n + 31) / 32 * 32;  // whole warps iterate together
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_up; i += stride) {
+        int k = -1;
+        if (i < n) {
+            const int l = backward ? depth - 1 - level[i] : level[i];
+            k = sched_key(l, ptr[i + 1] - ptr[i], epl);
+            key[i] = k;
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, k);
+        if (k >= 0 && (peers & ((1u << lane) - 1u)) == 0) atomicAdd(hist + k, __popc(peers));
     }
 }
 
@@ -230,17 +239,6 @@ __global__ void bwd_level_kernel(int32_t n, const int64_t* __restrict__ ptr, con
         for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(kFull, m, o));
         if (lane == 0) atomicExch(levb + j, m + 1);
         ok = __all_sync(kFull, ok);
-    }
-}
-
-__global__ void sched_scatter_kernel(const int32_t* __restrict__ level, const int64_t* __restrict__ ptr, int32_t n,
-                                     int32_t depth, int backward, int epl, const int32_t* __restrict__ start,
-                                     int32_t* cursor, int32_t* order) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        int l = backward ? depth - 1 - level[i] : level[i];
-        int k = sched_key(l, ptr[i + 1] - ptr[i], epl);
-        order[start[k] + atomicAdd(cursor + k, 1)] = (int32_t)i;
     }
 }
 
@@ -435,12 +433,6 @@ cudaError_t dmalloc(T** p, int64_t n) {
 
 }  // namespace
 
-#define RCHOL_TRY(x)                        \
-    do {                                    \
-        cudaError_t e__ = (x);              \
-        if (e__ != cudaSuccess) return e__; \
-    } while (0)
-
 // (Re)allocate a persistent buffer that shares the capacity `cap` with its
 // siblings: kept when present and the shared capacity did not grow.
 template <typename T>
@@ -562,21 +554,23 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
     return cudaSuccess;
 }
 
-// Orders the rows by (level, lane class) into `order` (capacity n, owned by
-// the factor) and emits the task list into `*tasks` (grown as needed).
+// Orders the rows by (level, lane class, row) into `order` (capacity n,
+// owned by the factor) and emits the task list into `*tasks` (grown as
+// needed).
 static cudaError_t build_one_schedule(const int32_t* level, const int64_t* ptr, int32_t n, int32_t depth, int backward,
                                       int epl, Scratch& sc, int32_t* order, int2** tasks, int64_t& tcap,
                                       int32_t* ntasks, cudaStream_t s) {
     const int32_t nb = kLaneClasses * depth;
-    int32_t *hist = nullptr, *start = nullptr, *tcount = nullptr, *tstart = nullptr;
+    int32_t *hist = nullptr, *start = nullptr, *tcount = nullptr, *tstart = nullptr, *key = nullptr;
     void* tmp = nullptr;
+    RCHOL_TRY(sc.get(&key, std::max<int32_t>(n, 1)));
     RCHOL_TRY(sc.get(&hist, nb));
     RCHOL_TRY(sc.get(&start, (int64_t)nb + 1));
     RCHOL_TRY(sc.get(&tcount, nb));
     RCHOL_TRY(sc.get(&tstart, (int64_t)nb + 1));
     RCHOL_TRY(sc.get((char**)&tmp, (int64_t)scan_tmp_bytes(nb)));
     RCHOL_TRY(cudaMemsetAsync(hist, 0, sizeof(int32_t) * (size_t)nb, s));
-    sched_hist_kernel<<<grid_for(n, 256), 256, 0, s>>>(level, ptr, n, depth, backward, epl, hist);
+    sched_hist_kernel<<<grid_for(n, 256), 256, 0, s>>>(level, ptr, n, depth, backward, epl, key, hist);
     RCHOL_TRY(exclusive_scan_i32_to_i32(hist, start, nb, tmp, s));
     sched_task_count_kernel<<<grid_for(nb, 256), 256, 0, s>>>(hist, nb, tcount);
     RCHOL_TRY(exclusive_scan_i32_to_i32(tcount, tstart, nb, tmp, s));
@@ -586,9 +580,8 @@ static cudaError_t build_one_schedule(const int32_t* level, const int64_t* ptr, 
     *ntasks = nt;
     RCHOL_TRY(ensure(tasks, tcap, (int64_t)nt));
     sched_task_emit_kernel<<<grid_for(nt, 256), 256, 0, s>>>(hist, start, tstart, nb, nt, *tasks);
-    RCHOL_TRY(cudaMemsetAsync(tcount, 0, sizeof(int32_t) * (size_t)nb, s));
-    sched_scatter_kernel<<<grid_for(n, 256), 256, 0, s>>>(level, ptr, n, depth, backward, epl, start, tcount, order);
-    return cudaGetLastError();
+    RCHOL_TRY(cudaGetLastError());
+    return stable_key_order(key, n, nb, order, sc, s);
 }
 
 static cudaError_t build_layout(int32_t n, const int32_t* order, const int64_t* ptr, const int32_t* idx,

@@ -213,6 +213,18 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
 // Drop the last row/column of A (ground vertex) into a new DevCsc.
 cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, cudaStream_t s);
 
+// Return the CUDA error of `x` from the enclosing function.
+#define RCHOL_TRY(x)                        \
+    do {                                    \
+        cudaError_t e__ = (x);              \
+        if (e__ != cudaSuccess) return e__; \
+    } while (0)
+
+// Stable order of 0..n-1 by key (0 <= key < nkeys) into `order`; rows with
+// equal keys keep ascending index order (bucket_sort.cu).
+cudaError_t stable_key_order(const int32_t* key, int32_t n, int32_t nkeys, int32_t* order, Scratch& sc,
+                             cudaStream_t s);
+
 // ---- scans (scan.cu) -------------------------------------------------------
 // out[0] = 0, out[i+1] = sum(in[0..i]); out has n+1 entries.  Uses `tmp`
 // scratch of scan_tmp_bytes(n).

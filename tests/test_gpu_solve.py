@@ -128,6 +128,30 @@ def test_pcg_without_graph(problem):
     np.testing.assert_array_equal(x, x2)  # same kernels, same order: identical bits
 
 
+@pytest.mark.parametrize("precision", [R.PREC_FP64, R.PREC_FP32_FACTOR])
+def test_pcg_bitwise_reproducible_across_factorizations(precision):
+    """Two factorizations with one seed give bit-identical solves: the
+    solve schedules (and so the order of every reduction) are independent
+    of thread timing."""
+    n, r, c, v, g = grid_laplacian((18, 17, 16), seed=31, excess_frac=0.05, wlo=1e-3, whi=1e3)
+    b = None
+    results = []
+    for _ in range(2):
+        ctx = R.Context(seed=8, precision=precision, tol=1e-8)
+        ctx.set_triplets(n, r, c, v, trim_ground=g)
+        f = ctx.factor()
+        ns = f.info().n
+        if b is None:
+            b = zero_sum_normal(ns, 12)
+        x, info = ctx.pcg_solve(f, b)
+        results.append((x, info["iterations"], info["relres_true"]))
+        f.free()
+        ctx.close()
+    assert results[0][1] == results[1][1]
+    np.testing.assert_array_equal(results[0][0], results[1][0])
+    assert results[0][2] == results[1][2]
+
+
 def test_laplacian_without_ground():
     n, r, c, v, g = grid_laplacian((64, 64), seed=31)
     P = OracleProblem(n, r, c, v)
