@@ -392,6 +392,90 @@ __global__ void __launch_bounds__(kBlock) spmv_update_kernel(SolveArgs a) {
     }
 }
 
+// One right-hand side: a warp takes 32 consecutive rows at a time.  Their
+// matrix entries form one contiguous range, read coalesced kSpmvChunk at a
+// time; the products val * z[idx] go to shared memory, and each lane then
+// adds the products of its own row in entry order (round the product, then
+// add, as a plain row loop without fused multiply-add does).
+#ifndef RCHOL_SPMV_CHUNK
+#define RCHOL_SPMV_CHUNK 128
+#endif
+constexpr int kSpmvChunk = RCHOL_SPMV_CHUNK;  // entries staged per warp and chunk
+
+__global__ void __launch_bounds__(kBlock) spmv_update_tile_kernel(SolveArgs a) {
+    if (ld_relaxed(&a.sc->done)) return;
+    __shared__ double stage_all[kBlock / 32][kSpmvChunk];
+    const int lane = threadIdx.x & 31;
+    double* stage = stage_all[threadIdx.x >> 5];
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t ntiles = ((int64_t)a.n + 31) / 32;
+    const double beta = a.sc->beta[0];
+    double acc = 0.0;
+    for (int64_t tile = gw; tile < ntiles; tile += nw) {
+        const int64_t r0 = tile * 32;
+        const int rows = (int)(((int64_t)a.n - r0) < 32 ? ((int64_t)a.n - r0) : 32);
+        const bool row = lane < rows;
+        const int64_t i = r0 + lane;
+        const int ps = row ? a.a_ptr[i] : 0;
+        const int tile_end = a.a_ptr[r0 + rows];
+        const int nb = __shfl_down_sync(kFull, ps, 1);
+        const int pe = lane + 1 < rows ? nb : tile_end;
+        const int tile_begin = __shfl_sync(kFull, ps, 0);
+        // row vectors in flight while the products are formed
+        double qo = 0.0, po = 0.0, zi = 0.0;
+        if (row) {
+            qo = a.q[i];
+            po = a.p[i];
+            zi = a.z[i];
+        }
+        double sum = 0.0;
+        for (int c0 = tile_begin; c0 < tile_end; c0 += kSpmvChunk) {
+            const int cn = min(kSpmvChunk, tile_end - c0);
+            int32_t idx[kSpmvChunk / 32];
+            double val[kSpmvChunk / 32], zv[kSpmvChunk / 32];
+#pragma unroll
+            for (int k = 0; k < kSpmvChunk / 32; ++k) {
+                const int e = k * 32 + lane;
+                if (e < cn) {
+                    idx[k] = a.a_idx[c0 + e];
+                    val[k] = a.a_val[c0 + e];
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kSpmvChunk / 32; ++k)
+                if (k * 32 + lane < cn) zv[k] = a.z[idx[k]];
+#pragma unroll
+            for (int k = 0; k < kSpmvChunk / 32; ++k) {
+                const int e = k * 32 + lane;
+                if (e < cn) stage[e] = __dmul_rn(val[k], zv[k]);
+            }
+            __syncwarp();
+            const int lo = max(ps, c0), hi = min(pe, c0 + cn);
+            if (row)
+                for (int p = lo; p < hi; ++p) sum += stage[p - c0];
+            __syncwarp();
+        }
+        if (row) {
+            const double qi = sum + beta * qo;
+            const double pi = zi + beta * po;
+            a.q[i] = qi;
+            a.p[i] = pi;
+            a.y[i] = pending_value();
+            acc += pi * qi;
+        }
+    }
+    block_partials_lane<1>(acc, a.part + (size_t)blockIdx.x);
+    if (last_block(&a.sc->ticket[1])) {
+        sum_partials<1>(a.part, gridDim.x, a.sc->pq);
+        if (threadIdx.x == 0) {
+            const double pq = a.sc->pq[0];
+            a.sc->alpha[0] = (a.sc->active[0] && pq != 0.0) ? a.sc->rz[0] / pq : 0.0;
+            a.sc->ticket[1] = 0;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // fwd: x += alpha p; r -= alpha q; (r.r); y = L^{-1} r  (rows ascending)
 // ---------------------------------------------------------------------------
@@ -966,7 +1050,7 @@ class PcgSolver {
 template <int K, typename TV>
 static void bind_kernels(PcgSolver* s) {
     s->k_init = (void*)init_kernel<K>;
-    s->k_spmv = (void*)spmv_update_kernel<K>;
+    s->k_spmv = K == 1 ? (void*)spmv_update_tile_kernel : (void*)spmv_update_kernel<K>;
     s->k_fwd = K == 1 ? (void*)fwd_pack_kernel<TV> : (void*)fwd_kernel<K, TV>;
     s->k_bwd = K == 1 ? (void*)bwd_pack_kernel<TV> : (void*)bwd_kernel<K, TV>;
     s->k_true = (void*)true_residual_kernel<K>;
