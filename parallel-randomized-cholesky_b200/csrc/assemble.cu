@@ -723,6 +723,11 @@ cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bo
     return cudaStreamSynchronize(s);
 }
 
+cudaError_t max_i32(const int32_t* v, int64_t n, int32_t* out, cudaStream_t s) {
+    max_kernel<<<grid_for(n, 256), 256, 0, s>>>(v, n, out);
+    return cudaGetLastError();
+}
+
 cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, cudaStream_t s) {
     const int32_t nout = A.n - 1;
     out.n = nout;

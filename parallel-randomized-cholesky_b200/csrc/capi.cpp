@@ -30,7 +30,7 @@ struct rchol_ctx {
     DevCsc At;       // the matrix of the solve (A itself when not trimmed)
     bool trim = false;
     bool have = false;
-    int32_t max_col = 0;  // largest column length of A
+    int32_t max_lower = 0;  // largest strict-lower column of A (bounds the first gathers)
     FactorWork w;
     bool w_ready = false;
     // solver cache
@@ -90,7 +90,7 @@ void free_csc(DevCsc& a) {
 void free_work(FactorWork& w) {
     void* ps[] = {w.lcolptr, w.lrow,  w.lval, w.dep,  w.queue,  w.fcnt,   w.brow,     w.bval,       w.chead,
                   w.cnext,   w.crow,  w.cval, w.prow, w.pval,   w.pstart, w.pcnt,     w.diag,       w.gscratch,
-                  w.counters, w.counters64, w.scan_tmp, w.level};
+                  w.counters, w.counters64, w.scan_tmp, w.level, w.hscratch, w.hlock};
     for (void* p : ps) cudaFree(p);
     w = FactorWork();
 }
@@ -121,6 +121,7 @@ struct PoolPlan {
     int32_t nchunks;
     int64_t pool_cap;
     int64_t gscratch_entries;
+    int64_t hscratch_entries;
     int grid, block;
 };
 
@@ -132,6 +133,7 @@ rchol_status alloc_work(rchol_ctx* ctx, const PoolPlan& pp) {
     w.nchunks = pp.nchunks;
     w.pool_cap = pp.pool_cap;
     w.gscratch_entries = pp.gscratch_entries;
+    w.hscratch_entries = pp.hscratch_entries;
     const int64_t warps = (int64_t)pp.grid * (pp.block / 32);
     CK(dalloc(&w.lcolptr, (int64_t)n + 1), "alloc lcolptr");
     CK(dalloc(&w.lrow, w.lnnz), "alloc lrow");
@@ -152,6 +154,10 @@ rchol_status alloc_work(rchol_ctx* ctx, const PoolPlan& pp) {
     CK(dalloc(&w.diag, n), "alloc diag");
     CK(dalloc(&w.level, n), "alloc levels");
     CK(cudaMalloc((void**)&w.gscratch, (size_t)warps * (size_t)w.gscratch_entries * 32), "alloc slab scratch");
+    CK(cudaMalloc((void**)&w.hscratch, (size_t)rchol::kHugeSlabs * (size_t)w.hscratch_entries * 32),
+       "alloc shared slabs");
+    CK(dalloc(&w.hlock, rchol::kHugeSlabs), "alloc slab locks");
+    CK(cudaMemset(w.hlock, 0, sizeof(int32_t) * rchol::kHugeSlabs), "clear slab locks");
     CK(dalloc(&w.counters, 16), "alloc counters");
     CK(dalloc(&w.counters64, 4), "alloc counters64");
     CK(cudaMalloc(&w.scan_tmp, rchol::scan_tmp_bytes(n)), "alloc scan scratch");
@@ -171,6 +177,14 @@ rchol_status lower_nnz(rchol_ctx* ctx, int64_t* out) {
     CK(rchol::exclusive_scan_i32_to_i64(cnt, ptr, n, tmp, ctx->stream), "scan lower");
     CK(cudaMemcpyAsync(out, ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream), "copy lnnz");
     CK(cudaStreamSynchronize(ctx->stream), "sync lnnz");
+    // the largest strict-lower column (the scan scratch's first word holds it)
+    int32_t* dmax = reinterpret_cast<int32_t*>(tmp);
+    int32_t hmax = 0;
+    CK(cudaMemsetAsync(dmax, 0, sizeof(int32_t), ctx->stream), "clear max");
+    CK(rchol::max_i32(cnt, n, dmax, ctx->stream), "max lower");
+    CK(cudaMemcpyAsync(&hmax, dmax, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream), "copy max");
+    CK(cudaStreamSynchronize(ctx->stream), "sync max");
+    ctx->max_lower = hmax;
     cudaFree(cnt);
     cudaFree(ptr);
     cudaFree(tmp);
@@ -376,23 +390,12 @@ extern "C" rchol_status rchol_set_csc(rchol_ctx* ctx, int n, const int* colptr, 
         ctx->At = ctx->A;
     }
     CK(cudaStreamSynchronize(ctx->stream), "sync upload");
-    // largest column (bounds the gather of early vertices)
-    int32_t mx = 0;
-    if (on_device) {
-        std::vector<int32_t> cp((size_t)n + 1);
-        CK(cudaMemcpy(cp.data(), ctx->A.colptr, sizeof(int32_t) * ((size_t)n + 1), cudaMemcpyDeviceToHost),
-           "read colptr");
-        for (int i = 0; i < n; ++i) mx = std::max(mx, cp[(size_t)i + 1] - cp[(size_t)i]);
-    } else {
-        for (int i = 0; i < n; ++i) mx = std::max(mx, colptr[i + 1] - colptr[i]);
-    }
-    ctx->max_col = mx;
     ctx->have = true;
     if (same && ctx->w_ready) {
         int64_t lnnz = 0;
         rchol_status s = lower_nnz(ctx, &lnnz);
         if (s != RCHOL_OK) return s;
-        if (lnnz != old_lnnz || 4 * (int64_t)mx > ctx->w.gscratch_entries) {
+        if (lnnz != old_lnnz || 4 * (int64_t)ctx->max_lower > ctx->w.hscratch_entries) {
             free_work(ctx->w);
             ctx->w_ready = false;
         }
@@ -468,7 +471,10 @@ extern "C" rchol_status rchol_factor(rchol_ctx* ctx, rchol_factor_t** out) {
         pp.c0 = o.bucket_cap;
         pp.nchunks = (int32_t)std::min<int64_t>(INT32_MAX / 64, std::max<int64_t>(4096, lnnz / 16 + ctx->A.n / 8));
         pp.pool_cap = (int64_t)(o.pool_mult * (double)lnnz) + ctx->A.n + (int64_t)max_grid * (block / 32) * 1024;
-        pp.gscratch_entries = std::max<int64_t>(1024, pow2_ge(4 * (int64_t)ctx->max_col));
+        // per-warp scratch up to 4096 entries; larger gathers share kHugeSlabs slabs
+        const int64_t want = std::max<int64_t>(1024, pow2_ge(4 * (int64_t)ctx->max_lower));
+        pp.gscratch_entries = std::min<int64_t>(want, 4096);
+        pp.hscratch_entries = want;
         pp.grid = max_grid;
         pp.block = block;
         s = alloc_work(ctx, pp);
@@ -502,18 +508,18 @@ extern "C" rchol_status rchol_factor(rchol_ctx* ctx, rchol_factor_t** out) {
         const int st = counters[3];
         if (st == 0) break;
         if (st == rchol::kDevTimeout) return fail(ctx, RCHOL_ERR_TIMEOUT, "factor: a device wait timed out");
-        if (st != rchol::kDevCapacity || attempt >= 3)
+        if (st != rchol::kDevCapacity || attempt >= 6)
             return fail(ctx, st == rchol::kDevCapacity ? RCHOL_ERR_CAPACITY : RCHOL_ERR_INVALID,
                         "factor: device status " + std::to_string(st));
         // grow the pool that ran out and retry from scratch
-        PoolPlan pp{w.c0, w.nchunks, w.pool_cap, w.gscratch_entries, max_grid, block};
+        PoolPlan pp{w.c0, w.nchunks, w.pool_cap, w.gscratch_entries, w.hscratch_entries, max_grid, block};
         if (counters[2] >= w.nchunks) pp.nchunks = (int32_t)std::min<int64_t>(INT32_MAX / 64, 2ll * w.nchunks + 1024);
         if ((int64_t)c64[0] > w.pool_cap) pp.pool_cap = 2 * w.pool_cap;
-        if ((int64_t)counters[6] > w.gscratch_entries) pp.gscratch_entries = pow2_ge(2 * (int64_t)counters[6]);
-        if (pp.nchunks == w.nchunks && pp.pool_cap == w.pool_cap && pp.gscratch_entries == w.gscratch_entries) {
+        if ((int64_t)counters[6] > w.hscratch_entries) pp.hscratch_entries = pow2_ge(2 * (int64_t)counters[6]);
+        if (pp.nchunks == w.nchunks && pp.pool_cap == w.pool_cap && pp.hscratch_entries == w.hscratch_entries) {
             pp.nchunks = (int32_t)std::min<int64_t>(INT32_MAX / 64, 2ll * w.nchunks);
             pp.pool_cap *= 2;
-            pp.gscratch_entries *= 2;
+            pp.hscratch_entries *= 2;
         }
         int64_t lnnz = w.lnnz;
         free_work(w);

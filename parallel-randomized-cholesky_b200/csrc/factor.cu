@@ -138,6 +138,9 @@ struct FactorArgs {
     int32_t* level;  // forward level of each row of L (depth in the L-solve DAG)
     unsigned char* gscratch;
     int64_t gscratch_entries;
+    unsigned char* hscratch;
+    int64_t hscratch_entries;
+    int32_t* hlock;
     int32_t* counters;
     unsigned long long* pool_cursor;
     uint64_t seed;
@@ -376,6 +379,40 @@ __device__ bool eliminate_small(const FactorArgs& a, int32_t k, int nf, int o0, 
     return true;
 }
 
+__device__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, int no, Slab s, int lane,
+                               int64_t& pool_cur, int64_t& pool_end, long long& fills, int32_t& next);
+
+// Takes one of the shared large slabs (lane 0 tries the lock words; the
+// wait is bounded).  Holders never wait on other vertices, so a slab is
+// always released.  Returns the slab index, or -1 when the kernel stops.
+__device__ int acquire_huge(const FactorArgs& a, int lane) {
+    int got = -1;
+    if (lane == 0) {
+        const unsigned long long t0 = global_timer_ns();
+        unsigned spins = 0;
+        while (got < 0) {
+            for (int i = 0; i < kHugeSlabs && got < 0; ++i)
+                if (atomicCAS(a.hlock + i, 0, 1) == 0) got = i;
+            if (got >= 0 || aborted(a)) break;
+            if ((++spins & 63u) == 0 && global_timer_ns() - t0 > a.timeout_ns) {
+                fail(a, kDevTimeout);
+                break;
+            }
+            __nanosleep(200);
+        }
+        __threadfence();
+    }
+    return __shfl_sync(kFull, got, 0);
+}
+
+__device__ void release_huge(const FactorArgs& a, int lane, int h) {
+    __syncwarp();
+    if (lane == 0) {
+        __threadfence();
+        atomicExch(a.hlock + h, 0);
+    }
+}
+
 // Eliminate vertex k with one warp.  Returns false if the kernel must stop.
 // `next` receives one neighbour this elimination released (or stays -1);
 // the other released neighbours go to the global queue.
@@ -396,16 +433,30 @@ __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_glob
     if (total > max_gather) max_gather = total;
     if (total <= kWarp && nf <= a.c0)
         return eliminate_small(a, k, nf, o0, no, lane, pool_cur, pool_end, fills, next);
-    Slab s = sm;
-    if (total > a.smem_slab) {
-        if ((int64_t)total > a.gscratch_entries) {
-            if (lane == 0) fail(a, kDevCapacity);
-            return false;
-        }
-        s = make_slab(a.gscratch + (size_t)warp_global * (size_t)a.gscratch_entries * kSlabBytesPerEntry,
-                      (int)a.gscratch_entries);
-        if (lane == 0) atomicAdd(a.counters + kBigCount, 1);
+    if (total <= a.smem_slab) return eliminate_slab(a, k, nf, o0, no, sm, lane, pool_cur, pool_end, fills, next);
+    if (lane == 0) atomicAdd(a.counters + kBigCount, 1);
+    if ((int64_t)total <= a.gscratch_entries) {
+        Slab s = make_slab(a.gscratch + (size_t)warp_global * (size_t)a.gscratch_entries * kSlabBytesPerEntry,
+                           (int)a.gscratch_entries);
+        return eliminate_slab(a, k, nf, o0, no, s, lane, pool_cur, pool_end, fills, next);
     }
+    if ((int64_t)total > a.hscratch_entries) {
+        if (lane == 0) fail(a, kDevCapacity);
+        return false;
+    }
+    const int h = acquire_huge(a, lane);
+    if (h < 0) return false;
+    Slab s = make_slab(a.hscratch + (size_t)h * (size_t)a.hscratch_entries * kSlabBytesPerEntry,
+                       (int)a.hscratch_entries);
+    const bool ok = eliminate_slab(a, k, nf, o0, no, s, lane, pool_cur, pool_end, fills, next);
+    release_huge(a, lane, h);
+    return ok;
+}
+
+// Elimination of vertex k (total = nf + no > 0 gathered entries) in slab s.
+__device__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, int no, Slab s, int lane,
+                               int64_t& pool_cur, int64_t& pool_end, long long& fills, int32_t& next) {
+    const int total = nf + no;
     const int P = pow2_at_least(total);
 
     // ---- gather: fills (first chunk, then overflow chunks), original column
@@ -578,11 +629,20 @@ __global__ void __launch_bounds__(256) factor_kernel(FactorArgs a) {
             idx = __shfl_sync(kFull, idx, 0);
             if (idx >= a.n) break;
             if (lane == 0) {
+                // the limit bounds a wait without progress: it restarts
+                // whenever the count of eliminated vertices moves
                 unsigned spins = 0;
+                int seen = -1;
+                unsigned long long since = t0;
                 while ((k = ld_acquire(a.queue + idx)) < 0) {
                     if ((++spins & 63u) == 0) {
-                        if (ld_relaxed(a.counters + kDone) >= a.n || aborted(a)) break;
-                        if (global_timer_ns() - t0 > a.timeout_ns) {
+                        const int done = ld_relaxed(a.counters + kDone);
+                        if (done >= a.n || aborted(a)) break;
+                        const unsigned long long now = global_timer_ns();
+                        if (done != seen) {
+                            seen = done;
+                            since = now;
+                        } else if (now - since > a.timeout_ns) {
                             fail(a, kDevTimeout);
                             break;
                         }
@@ -706,6 +766,7 @@ cudaError_t launch_init_factor_state(FactorWork& w, cudaStream_t s) {
     if ((e = cudaMemsetAsync(w.level, 0, sizeof(int32_t) * (size_t)w.n, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.counters, 0, sizeof(int32_t) * 16, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.counters64, 0, sizeof(unsigned long long) * 4, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(w.hlock, 0, sizeof(int32_t) * kHugeSlabs, s)) != cudaSuccess) return e;
     init_queue_kernel<<<grid_for(w.n, 256), 256, 0, s>>>(w.n, w.dep, w.queue, w.counters);
     return cudaGetLastError();
 }
@@ -751,6 +812,9 @@ cudaError_t launch_factor(FactorWork& w, const FactorLaunch& cfg, cudaStream_t s
     a.level = w.level;
     a.gscratch = w.gscratch;
     a.gscratch_entries = w.gscratch_entries;
+    a.hscratch = w.hscratch;
+    a.hscratch_entries = w.hscratch_entries;
+    a.hlock = w.hlock;
     a.counters = w.counters;
     a.pool_cursor = w.counters64;
     a.seed = cfg.seed;

@@ -106,6 +106,11 @@ struct FactorWork {
     // per-warp scratch for vertices that do not fit the shared-memory slab
     int64_t gscratch_entries = 0; // entries per warp
     unsigned char* gscratch = nullptr;
+    // a few shared slabs for vertices larger than the per-warp scratch,
+    // each taken with a lock word (hlock[i] = 1 while held)
+    int64_t hscratch_entries = 0; // entries per shared slab
+    unsigned char* hscratch = nullptr;
+    int32_t* hlock = nullptr;
     // counters: [0] queue head, [1] queue tail, [2] chunk cursor, [3] status,
     // [4] abort, [5] big-vertex count, [6] max gather, [7] overflow fills;
     // pool cursor is int64 in counters64[0]
@@ -219,6 +224,12 @@ cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, cudaStream_t s);
         cudaError_t e__ = (x);              \
         if (e__ != cudaSuccess) return e__; \
     } while (0)
+
+// Shared large slabs of the elimination kernel.
+constexpr int kHugeSlabs = 8;
+
+// *out = max(v[0..n-1]) (device, *out must start at 0).
+cudaError_t max_i32(const int32_t* v, int64_t n, int32_t* out, cudaStream_t s);
 
 // Stable order of 0..n-1 by key (0 <= key < nkeys) into `order`; rows with
 // equal keys keep ascending index order (bucket_sort.cu).

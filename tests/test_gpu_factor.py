@@ -84,6 +84,33 @@ def test_factor_independent_of_launch_shape_and_pools(opts):
         assert info.attempts >= 1
 
 
+def _hub_laplacian(leaves, seed):
+    """Vertex 0 joined to every leaf, leaves joined in a ring: in natural
+    order vertex 0 gathers all `leaves` entries at once."""
+    rng = np.random.default_rng(seed)
+    n = leaves + 1
+    a = np.concatenate([np.zeros(leaves, np.int64), np.arange(1, n)])
+    b = np.concatenate([np.arange(1, n), np.roll(np.arange(1, n), -1)])
+    w = np.exp(rng.uniform(np.log(1e-2), np.log(1e2), len(a)))
+    d = np.zeros(n)
+    np.add.at(d, a, w)
+    np.add.at(d, b, w)
+    rows = np.concatenate([a, b, np.arange(n)]).astype(np.int32)
+    cols = np.concatenate([b, a, np.arange(n)]).astype(np.int32)
+    vals = np.concatenate([-w, -w, d])
+    return n, rows, cols, vals
+
+
+def test_factor_large_gather_uses_shared_slab():
+    """A gather larger than the per-warp scratch (4096 entries) runs in one
+    of the shared slabs and stays bit-exact."""
+    n, r, c, v = _hub_laplacian(6000, seed=5)
+    P = OracleProblem(n, r, c, v, trim=False)
+    gpu, info = _gpu_factor(n, r, c, v, False, seed=6)
+    _compare(gpu, P.factor(seed=6))
+    assert info.max_gather >= 6000
+
+
 def test_factor_repeatable_in_one_context():
     n, r, c, v, _ = grid_laplacian((30, 30), seed=8)
     ctx = R.Context(seed=3)
