@@ -241,18 +241,14 @@ __device__ __forceinline__ bool row_value_gt(int32_t r1, unsigned long long v1, 
 // entries, all fills in the first bucket chunk): one entry per lane; sorts,
 // merge, compaction, scan and CDF search as warp shuffles.  Same arithmetic
 // in the same order as the slab path (and the oracle), so the bits agree.
-__device__ bool eliminate_small(const FactorArgs& a, int32_t k, int nf, int o0, int no, int lane,
-                                int64_t& pool_cur, int64_t& pool_end, long long& fills, int32_t& next) {
-    const int total = nf + no;
+__device__ bool eliminate_small(const FactorArgs& a, int32_t k, int total, int32_t brow_l, double bval_l, int lvl,
+                                int lane, int64_t& pool_cur, int64_t& pool_end, long long& fills, int32_t& next) {
+    // all `total` entries sit in the bucket, entry `lane` in this lane
     int32_t row = INT_MAX;
     unsigned long long vb = kInfBits;
-    if (lane < nf) {
-        const size_t o = (size_t)k * (size_t)a.c0 + (size_t)lane;
-        row = __ldcg(a.brow + o);
-        vb = (unsigned long long)__double_as_longlong(__ldcg(a.bval + o));
-    } else if (lane < total) {
-        row = a.lrow[o0 + lane - nf];
-        vb = (unsigned long long)__double_as_longlong(a.lval[o0 + lane - nf]);
+    if (lane < total) {
+        row = brow_l;
+        vb = (unsigned long long)__double_as_longlong(bval_l);
     }
     // bitonic sort of the 32 lanes by (row, value bits); padding sorts last
 #pragma unroll
@@ -371,7 +367,7 @@ __device__ bool eliminate_small(const FactorArgs& a, int32_t k, int nf, int o0, 
         if (lane == 0) fail(a, kDevCapacity);
         return false;
     }
-    const int lk = ld_relaxed(a.level + k) + 1;
+    const int lk = lvl + 1;
     __threadfence();
     __syncwarp();
     release_chunk(a, lk, lane, lane < m, mrow, mcnt, next);
@@ -379,7 +375,7 @@ __device__ bool eliminate_small(const FactorArgs& a, int32_t k, int nf, int o0, 
     return true;
 }
 
-__device__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, int no, Slab s, int lane,
+__device__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, int no, int lvl, Slab s, int lane,
                                int64_t& pool_cur, int64_t& pool_end, long long& fills, int32_t& next);
 
 // Takes one of the shared large slabs (lane 0 tries the lock words; the
@@ -418,9 +414,22 @@ __device__ void release_huge(const FactorArgs& a, int lane, int h) {
 // the other released neighbours go to the global queue.
 __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_global, int lane,
                           int64_t& pool_cur, int64_t& pool_end, long long& fills, int32_t& next, int& max_gather) {
+    // One round trip: the bucket count (original entries pre-filled at set-up
+    // plus fills), the bucket's first 32 slots, the original column range
+    // (entries beyond the bucket stay there) and the vertex's level.
     const int nf = ld_relaxed(a.fcnt + k);
-    const int o0 = a.lcolptr[k];
-    const int no = a.lcolptr[k + 1] - o0;
+    const int oc0 = a.lcolptr[k];
+    const int ocnt = a.lcolptr[k + 1] - oc0;
+    int32_t brow_l = INT_MAX;
+    double bval_l = 0.0;
+    if (lane < a.c0) {
+        const size_t o = (size_t)k * (size_t)a.c0 + (size_t)lane;
+        brow_l = __ldcg(a.brow + o);
+        bval_l = __ldcg(a.bval + o);
+    }
+    const int lvl = ld_relaxed(a.level + k);
+    const int o0 = oc0 + min(ocnt, a.c0);  // originals not in the bucket
+    const int no = ocnt - min(ocnt, a.c0);
     const int total = nf + no;
     if (total == 0) {  // driver_local.cpp:470-477: empty column, D = 0
         if (lane == 0) {
@@ -431,14 +440,15 @@ __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_glob
         return true;
     }
     if (total > max_gather) max_gather = total;
-    if (total <= kWarp && nf <= a.c0)
-        return eliminate_small(a, k, nf, o0, no, lane, pool_cur, pool_end, fills, next);
-    if (total <= a.smem_slab) return eliminate_slab(a, k, nf, o0, no, sm, lane, pool_cur, pool_end, fills, next);
+    if (no == 0 && nf <= a.c0 && total <= kWarp)  // every entry is in the bucket
+        return eliminate_small(a, k, total, brow_l, bval_l, lvl, lane, pool_cur, pool_end, fills, next);
+    if (total <= a.smem_slab)
+        return eliminate_slab(a, k, nf, o0, no, lvl, sm, lane, pool_cur, pool_end, fills, next);
     if (lane == 0) atomicAdd(a.counters + kBigCount, 1);
     if ((int64_t)total <= a.gscratch_entries) {
         Slab s = make_slab(a.gscratch + (size_t)warp_global * (size_t)a.gscratch_entries * kSlabBytesPerEntry,
                            (int)a.gscratch_entries);
-        return eliminate_slab(a, k, nf, o0, no, s, lane, pool_cur, pool_end, fills, next);
+        return eliminate_slab(a, k, nf, o0, no, lvl, s, lane, pool_cur, pool_end, fills, next);
     }
     if ((int64_t)total > a.hscratch_entries) {
         if (lane == 0) fail(a, kDevCapacity);
@@ -448,13 +458,14 @@ __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_glob
     if (h < 0) return false;
     Slab s = make_slab(a.hscratch + (size_t)h * (size_t)a.hscratch_entries * kSlabBytesPerEntry,
                        (int)a.hscratch_entries);
-    const bool ok = eliminate_slab(a, k, nf, o0, no, s, lane, pool_cur, pool_end, fills, next);
+    const bool ok = eliminate_slab(a, k, nf, o0, no, lvl, s, lane, pool_cur, pool_end, fills, next);
     release_huge(a, lane, h);
     return ok;
 }
 
-// Elimination of vertex k (total = nf + no > 0 gathered entries) in slab s.
-__device__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, int no, Slab s, int lane,
+// Elimination of vertex k in slab s: nf bucket entries (slots, then
+// overflow chunks) and no original entries from lrow[o0..], level lvl.
+__device__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, int no, int lvl, Slab s, int lane,
                                int64_t& pool_cur, int64_t& pool_end, long long& fills, int32_t& next) {
     const int total = nf + no;
     const int P = pow2_at_least(total);
@@ -586,7 +597,7 @@ __device__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, i
     // row r of L depends on column k: level[r] >= level[k] + 1.  level[k]
     // is final here: every column with an entry in row k was eliminated
     // before k was released.
-    const int lk = ld_relaxed(a.level + k) + 1;
+    const int lk = lvl + 1;
     // fills, pool writes and levels must be visible before any neighbour is
     // released
     __threadfence();
@@ -663,6 +674,24 @@ __global__ void __launch_bounds__(256) factor_kernel(FactorArgs a) {
 }
 
 // ---- setup kernels --------------------------------------------------------
+
+// The first c0 strict-lower entries of each column go into its fill bucket
+// (fcnt = their count), so that a vertex's gather usually reads one place.
+__global__ void prefill_bucket_kernel(int32_t n, int c0, const int32_t* __restrict__ lcolptr,
+                                      const int32_t* __restrict__ lrow, const double* __restrict__ lval,
+                                      int32_t* fcnt, int32_t* brow, double* bval) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < n; c += warps) {
+        const int s = lcolptr[c];
+        const int cnt = min(lcolptr[c + 1] - s, c0);
+        for (int t = lane; t < cnt; t += 32) {
+            brow[(size_t)c * (size_t)c0 + t] = lrow[s + t];
+            bval[(size_t)c * (size_t)c0 + t] = lval[s + t];
+        }
+        if (lane == 0) fcnt[c] = cnt;
+    }
+}
 
 // Per column: entries below the diagonal (lower_cnt) and above it (dep,
 // count_minimum_dependencies, pre_process.hpp:474-496).  One warp/column.
@@ -767,6 +796,9 @@ cudaError_t launch_init_factor_state(FactorWork& w, cudaStream_t s) {
     if ((e = cudaMemsetAsync(w.counters, 0, sizeof(int32_t) * 16, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.counters64, 0, sizeof(unsigned long long) * 4, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.hlock, 0, sizeof(int32_t) * kHugeSlabs, s)) != cudaSuccess) return e;
+    prefill_bucket_kernel<<<grid_for((int64_t)w.n * 32, 256), 256, 0, s>>>(w.n, w.c0, w.lcolptr, w.lrow, w.lval,
+                                                                            w.fcnt, w.brow, w.bval);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     init_queue_kernel<<<grid_for(w.n, 256), 256, 0, s>>>(w.n, w.dep, w.queue, w.counters);
     return cudaGetLastError();
 }
