@@ -153,8 +153,9 @@ rchol_status alloc_work(rchol_ctx* ctx, const PoolPlan& pp) {
     CK(dalloc(&w.pcnt, n), "alloc pool counts");
     CK(dalloc(&w.diag, n), "alloc diag");
     CK(dalloc(&w.level, n), "alloc levels");
-    CK(cudaMalloc((void**)&w.gscratch, (size_t)warps * (size_t)w.gscratch_entries * 32), "alloc slab scratch");
-    CK(cudaMalloc((void**)&w.hscratch, (size_t)rchol::kHugeSlabs * (size_t)w.hscratch_entries * 32),
+    CK(cudaMalloc((void**)&w.gscratch, (size_t)warps * (size_t)w.gscratch_entries * rchol::kGlobalSlabBytes),
+       "alloc slab scratch");
+    CK(cudaMalloc((void**)&w.hscratch, (size_t)rchol::kHugeSlabs * (size_t)w.hscratch_entries * rchol::kGlobalSlabBytes),
        "alloc shared slabs");
     CK(dalloc(&w.hlock, rchol::kHugeSlabs), "alloc slab locks");
     CK(cudaMemset(w.hlock, 0, sizeof(int32_t) * rchol::kHugeSlabs), "clear slab locks");

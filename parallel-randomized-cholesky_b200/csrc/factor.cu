@@ -25,7 +25,7 @@ namespace rchol {
 
 namespace {
 
-constexpr int kChunk = 64;                 // overflow chunk entries
+constexpr int kChunk = 64;                 // overflow pool unit (entries); chunk lvl spans 2^lvl units
 constexpr int kPoolGrab = 1024;            // L-pool entries grabbed per warp at once
 constexpr unsigned long long kInfBits = 0x7ff0000000000000ull;
 constexpr int kSlabBytesPerEntry = 32;     // 8 (a_val) + 8 (b_val) + 8 (b_aux) + 4 + 4
@@ -40,13 +40,17 @@ __device__ __forceinline__ int pow2_at_least(int x) {
 }
 
 // One warp's staging area: a_* hold the gathered entries and, after the
-// value sort, the prefix sums; b_* hold the merged neighbours.
+// value sort, the prefix sums; b_* hold the merged neighbours.  Slabs in
+// global memory add t_* as the second buffer of their radix sorts.
 struct Slab {
     double* a_val;
     int32_t* a_row;
     double* b_val;
     int32_t* b_row;
     long long* b_aux;  // (multiplicity << 32) | row-order position
+    double* t_val;
+    int32_t* t_row;
+    long long* t_aux;
 };
 
 __device__ __forceinline__ Slab make_slab(unsigned char* base, int cap) {
@@ -56,6 +60,18 @@ __device__ __forceinline__ Slab make_slab(unsigned char* base, int cap) {
     s.b_aux = reinterpret_cast<long long*>(s.b_val + cap);
     s.a_row = reinterpret_cast<int32_t*>(s.b_aux + cap);
     s.b_row = s.a_row + cap;
+    s.t_val = nullptr;
+    s.t_row = nullptr;
+    s.t_aux = nullptr;
+    return s;
+}
+
+// kGlobalSlabBytes per entry: the shared-memory layout plus t_val, t_aux, t_row.
+__device__ __forceinline__ Slab make_global_slab(unsigned char* base, int cap) {
+    Slab s = make_slab(base, cap);
+    s.t_val = reinterpret_cast<double*>(s.b_row + cap);
+    s.t_aux = reinterpret_cast<long long*>(s.t_val + cap);
+    s.t_row = reinterpret_cast<int32_t*>(s.t_aux + cap);
     return s;
 }
 
@@ -113,6 +129,151 @@ __device__ void sort_value_row(double* val, int32_t* row, long long* aux, int P,
     }
 }
 
+// ---- warp radix sorts for slabs in global memory ------------------------
+// Stable LSD passes over 8-bit digits: a histogram pass, then a scatter pass
+// in which each 32-entry round ranks equal digits with a match mask, so equal
+// digits keep their order.  A pass whose entries all share the digit moves
+// nothing.  `hist` is 256 ints of the warp's shared memory.  The result is
+// the unique order of the keys, the same as the bitonic sorts give.
+
+constexpr int kRadixBatch = 1;  // entries per lane per round (more costs the common paths registers)
+
+// digit d of (row, value bits): bytes 0-7 of the value bits, then bytes 0-3 of the row
+__device__ __forceinline__ int rv_digit(int32_t r, double v, int d) {
+    return d < 8 ? (int)(((unsigned long long)__double_as_longlong(v) >> (8 * d)) & 255ull)
+                 : (int)(((unsigned)r >> (8 * (d - 8))) & 255u);
+}
+// digit d of (value bits, row): bytes 0-3 of the row, then bytes 0-7 of the value bits
+__device__ __forceinline__ int vr_digit(int32_t r, double v, int d) { return rv_digit(r, v, (d + 8) % 12); }
+
+// Histogram of digit d over n entries; returns true when every entry has
+// the same digit (the pass can be skipped).  Leaves exclusive offsets in hist.
+template <bool VR>
+__device__ bool radix_hist(const int32_t* row, const double* val, int n, int d, int* hist, int lane) {
+    for (int i = lane; i < 256; i += kWarp) hist[i] = 0;
+    __syncwarp();
+    for (int base = 0; base < n; base += kWarp * kRadixBatch) {
+        int32_t r[kRadixBatch];
+        double v[kRadixBatch];
+#pragma unroll
+        for (int q = 0; q < kRadixBatch; ++q) {
+            const int i = base + q * kWarp + lane;
+            if (i < n) {
+                r[q] = row[i];
+                v[q] = val[i];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kRadixBatch; ++q)
+            if (base + q * kWarp + lane < n) atomicAdd(&hist[VR ? vr_digit(r[q], v[q], d) : rv_digit(r[q], v[q], d)], 1);
+    }
+    __syncwarp();
+    // exclusive scan: lane l owns buckets 8l..8l+7
+    int c[8], tot = 0;
+    bool one = false;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        c[q] = hist[8 * lane + q];
+        tot += c[q];
+        one |= c[q] == n;
+    }
+    const bool all = __any_sync(kFull, one);
+    int incl = tot;
+#pragma unroll
+    for (int o = 1; o < kWarp; o <<= 1) {
+        const int t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+    }
+    int run = incl - tot;
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        hist[8 * lane + q] = run;
+        run += c[q];
+    }
+    __syncwarp();
+    return all;
+}
+
+// One stable scatter pass of (row, val[, aux]) by digit d; hist holds the offsets.
+template <bool VR, bool AUX>
+__device__ void radix_scatter(const int32_t* row, const double* val, const long long* aux, int32_t* orow, double* oval,
+                              long long* oaux, int n, int d, int* hist, int lane) {
+    const unsigned lt = (1u << lane) - 1u;
+    for (int base = 0; base < n; base += kWarp * kRadixBatch) {
+        int32_t r[kRadixBatch];
+        double v[kRadixBatch];
+        long long x[kRadixBatch];
+#pragma unroll
+        for (int q = 0; q < kRadixBatch; ++q) {
+            const int i = base + q * kWarp + lane;
+            if (i < n) {
+                r[q] = row[i];
+                v[q] = val[i];
+                if (AUX) x[q] = aux[i];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kRadixBatch; ++q) {
+            const bool valid = base + q * kWarp + lane < n;
+            const int dig = valid ? (VR ? vr_digit(r[q], v[q], d) : rv_digit(r[q], v[q], d)) : 256;
+            const unsigned peers = __match_any_sync(kFull, dig);
+            const int rank = __popc(peers & lt);
+            const int at = valid ? hist[dig] + rank : 0;
+            __syncwarp();
+            if (valid && rank == 0) hist[dig] += __popc(peers);
+            __syncwarp();
+            if (valid) {
+                orow[at] = r[q];
+                oval[at] = v[q];
+                if (AUX) oaux[at] = x[q];
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// (a_row, a_val) ascending by (row, value bits), result in a_*.
+__device__ void radix_sort_rv(const Slab& s, int n, int* hist, int lane) {
+    int32_t *r0 = s.a_row, *r1 = s.t_row;
+    double *v0 = s.a_val, *v1 = s.t_val;
+    for (int d = 0; d < 12; ++d) {
+        if (radix_hist<false>(r0, v0, n, d, hist, lane)) continue;
+        radix_scatter<false, false>(r0, v0, nullptr, r1, v1, nullptr, n, d, hist, lane);
+        int32_t* tr = r0; r0 = r1; r1 = tr;
+        double* tv = v0; v0 = v1; v1 = tv;
+    }
+    if (r0 != s.a_row) {
+        for (int i = lane; i < n; i += kWarp) {
+            s.a_row[i] = r0[i];
+            s.a_val[i] = v0[i];
+        }
+        __syncwarp();
+    }
+}
+
+// (b_val, b_row, b_aux) ascending by (value, row), result in b_*.
+__device__ void radix_sort_vr(const Slab& s, int n, int* hist, int lane) {
+    int32_t *r0 = s.b_row, *r1 = s.t_row;
+    double *v0 = s.b_val, *v1 = s.t_val;
+    long long *x0 = s.b_aux, *x1 = s.t_aux;
+    for (int d = 0; d < 12; ++d) {
+        if (radix_hist<true>(r0, v0, n, d, hist, lane)) continue;
+        radix_scatter<true, true>(r0, v0, x0, r1, v1, x1, n, d, hist, lane);
+        int32_t* tr = r0; r0 = r1; r1 = tr;
+        double* tv = v0; v0 = v1; v1 = tv;
+        long long* tx = x0; x0 = x1; x1 = tx;
+    }
+    if (r0 != s.b_row) {
+        for (int i = lane; i < n; i += kWarp) {
+            s.b_row[i] = r0[i];
+            s.b_val[i] = v0[i];
+            s.b_aux[i] = x0[i];
+        }
+        __syncwarp();
+    }
+}
+
 struct FactorArgs {
     int32_t n;
     const int32_t* __restrict__ lcolptr;
@@ -145,6 +306,7 @@ struct FactorArgs {
     unsigned long long* pool_cursor;
     uint64_t seed;
     int smem_slab;
+    int smem_region;  // bytes of shared memory per warp (slab, or radix histogram + CDF index)
     unsigned long long timeout_ns;
 };
 
@@ -166,16 +328,20 @@ __device__ bool append_fill(const FactorArgs& a, int32_t col, int32_t row, doubl
         return true;
     }
     atomicAdd(a.counters + kOverflowFills, 1);
-    int t = s - a.c0;
-    int ci = t / kChunk, off = t % kChunk;
+    // overflow chunk number lvl of a column spans kChunk << lvl slots (2^lvl
+    // pool units), so slot t is at most log2(t / kChunk + 1) links away
+    const int t = s - a.c0;
+    const int ci = 31 - __clz(t / kChunk + 1);
+    const int off = t - kChunk * ((1 << ci) - 1);
     int32_t* link = a.chead + col;
     int cur = -1;
     for (int lvl = 0;; ++lvl) {
         cur = ld_relaxed(link);
         if (cur < 0) {
-            int nc = atomicAdd(a.counters + kChunkCursor, 1);
-            if (nc >= a.nchunks) return false;
-            int old = atomicCAS(link, -1, nc);
+            const int units = 1 << lvl;
+            const int nc = atomicAdd(a.counters + kChunkCursor, units);
+            if (nc > a.nchunks - units) return false;
+            const int old = atomicCAS(link, -1, nc);
             cur = (old == -1) ? nc : old;
         }
         if (lvl == ci) break;
@@ -375,8 +541,17 @@ __device__ bool eliminate_small(const FactorArgs& a, int32_t k, int total, int32
     return true;
 }
 
-__device__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, int no, int lvl, Slab s, int lane,
-                               int64_t& pool_cur, int64_t& pool_end, long long& fills, int32_t& next);
+template <bool GLOBAL>
+__device__ __forceinline__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, int no, int lvl,
+                                               Slab s, unsigned char* wsm, int lane, int64_t& pool_cur,
+                                               int64_t& pool_end, long long& fills, int32_t& next);
+
+// The global-slab elimination (radix sorts, indexed CDF search).
+__device__ __forceinline__ bool eliminate_global(const FactorArgs& a, int32_t k, int nf, int o0, int no, int lvl,
+                                              Slab s, unsigned char* wsm, int lane, int64_t& pool_cur,
+                                              int64_t& pool_end, long long& fills, int32_t& next) {
+    return eliminate_slab<true>(a, k, nf, o0, no, lvl, s, wsm, lane, pool_cur, pool_end, fills, next);
+}
 
 // Takes one of the shared large slabs (lane 0 tries the lock words; the
 // wait is bounded).  Holders never wait on other vertices, so a slab is
@@ -412,7 +587,7 @@ __device__ void release_huge(const FactorArgs& a, int lane, int h) {
 // Eliminate vertex k with one warp.  Returns false if the kernel must stop.
 // `next` receives one neighbour this elimination released (or stays -1);
 // the other released neighbours go to the global queue.
-__device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_global, int lane,
+__device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, unsigned char* wsm, int warp_global, int lane,
                           int64_t& pool_cur, int64_t& pool_end, long long& fills, int32_t& next, int& max_gather) {
     // One round trip: the bucket count (original entries pre-filled at set-up
     // plus fills), the bucket's first 32 slots, the original column range
@@ -443,12 +618,12 @@ __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_glob
     if (no == 0 && nf <= a.c0 && total <= kWarp)  // every entry is in the bucket
         return eliminate_small(a, k, total, brow_l, bval_l, lvl, lane, pool_cur, pool_end, fills, next);
     if (total <= a.smem_slab)
-        return eliminate_slab(a, k, nf, o0, no, lvl, sm, lane, pool_cur, pool_end, fills, next);
+        return eliminate_slab<false>(a, k, nf, o0, no, lvl, sm, wsm, lane, pool_cur, pool_end, fills, next);
     if (lane == 0) atomicAdd(a.counters + kBigCount, 1);
     if ((int64_t)total <= a.gscratch_entries) {
-        Slab s = make_slab(a.gscratch + (size_t)warp_global * (size_t)a.gscratch_entries * kSlabBytesPerEntry,
-                           (int)a.gscratch_entries);
-        return eliminate_slab(a, k, nf, o0, no, lvl, s, lane, pool_cur, pool_end, fills, next);
+        Slab s = make_global_slab(a.gscratch + (size_t)warp_global * (size_t)a.gscratch_entries * kGlobalSlabBytes,
+                                  (int)a.gscratch_entries);
+        return eliminate_global(a, k, nf, o0, no, lvl, s, wsm, lane, pool_cur, pool_end, fills, next);
     }
     if ((int64_t)total > a.hscratch_entries) {
         if (lane == 0) fail(a, kDevCapacity);
@@ -456,17 +631,23 @@ __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, int warp_glob
     }
     const int h = acquire_huge(a, lane);
     if (h < 0) return false;
-    Slab s = make_slab(a.hscratch + (size_t)h * (size_t)a.hscratch_entries * kSlabBytesPerEntry,
-                       (int)a.hscratch_entries);
-    const bool ok = eliminate_slab(a, k, nf, o0, no, lvl, s, lane, pool_cur, pool_end, fills, next);
+    Slab s = make_global_slab(a.hscratch + (size_t)h * (size_t)a.hscratch_entries * kGlobalSlabBytes,
+                              (int)a.hscratch_entries);
+    const bool ok = eliminate_global(a, k, nf, o0, no, lvl, s, wsm, lane, pool_cur, pool_end, fills, next);
     release_huge(a, lane, h);
     return ok;
 }
 
 // Elimination of vertex k in slab s: nf bucket entries (slots, then
 // overflow chunks) and no original entries from lrow[o0..], level lvl.
-__device__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, int no, int lvl, Slab s, int lane,
-                               int64_t& pool_cur, int64_t& pool_end, long long& fills, int32_t& next) {
+template <bool GLOBAL>
+__device__ __forceinline__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, int no, int lvl,
+                                               Slab s, unsigned char* wsm, int lane, int64_t& pool_cur,
+                                               int64_t& pool_end, long long& fills, int32_t& next) {
+    // slabs in global memory sort with radix passes (one round trip per 32
+    // entries and pass) instead of bitonic stages (one per entry pair)
+    constexpr bool global = GLOBAL;
+    int* hist = reinterpret_cast<int*>(wsm);
     const int total = nf + no;
     const int P = pow2_at_least(total);
 
@@ -479,12 +660,12 @@ __device__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, i
     }
     int rem = nf - n0, pos = n0;
     int chunk = rem > 0 ? ld_relaxed(a.chead + k) : -1;
-    while (rem > 0) {
-        if (chunk < 0 || chunk >= a.nchunks) {
+    for (int lvl = 0; rem > 0; ++lvl) {
+        if (chunk < 0 || chunk > a.nchunks - (1 << lvl)) {
             if (lane == 0) fail(a, kDevBadInput);
             return false;
         }
-        int cnt = min(rem, kChunk);
+        const int cnt = min(rem, kChunk << lvl);
         for (int t = lane; t < cnt; t += kWarp) {
             s.a_row[pos + t] = __ldcg(a.crow + (size_t)chunk * kChunk + t);
             s.a_val[pos + t] = __ldcg(a.cval + (size_t)chunk * kChunk + t);
@@ -497,14 +678,17 @@ __device__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, i
         s.a_row[nf + t] = a.lrow[o0 + t];
         s.a_val[nf + t] = a.lval[o0 + t];
     }
-    for (int t = total + lane; t < P; t += kWarp) {
-        s.a_row[t] = INT_MAX;
-        s.a_val[t] = __longlong_as_double((long long)kInfBits);
+    if (!global) {
+        for (int t = total + lane; t < P; t += kWarp) {
+            s.a_row[t] = INT_MAX;
+            s.a_val[t] = __longlong_as_double((long long)kInfBits);
+        }
     }
     __syncwarp();
 
     // ---- sort by row and merge duplicates (driver_local.cpp:511-568)
-    sort_row_value(s.a_row, s.a_val, P, lane);
+    if (global) radix_sort_rv(s, total, hist, lane);
+    else sort_row_value(s.a_row, s.a_val, P, lane);
     int m = 0;
     const unsigned lt_mask = (1u << lane) - 1u;
     for (int base = 0; base < total; base += kWarp) {
@@ -528,15 +712,18 @@ __device__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, i
         m += __popc(bal);
     }
     const int P2 = pow2_at_least(m);
-    for (int t = m + lane; t < P2; t += kWarp) {
-        s.b_val[t] = __longlong_as_double((long long)kInfBits);
-        s.b_row[t] = INT_MAX;
-        s.b_aux[t] = 0;
+    if (!global) {
+        for (int t = m + lane; t < P2; t += kWarp) {
+            s.b_val[t] = __longlong_as_double((long long)kInfBits);
+            s.b_row[t] = INT_MAX;
+            s.b_aux[t] = 0;
+        }
     }
     __syncwarp();
 
     // ---- sort by value, chunked prefix sum (driver_local.cpp:573-593)
-    sort_value_row(s.b_val, s.b_row, s.b_aux, P2, lane);
+    if (global) radix_sort_vr(s, m, hist, lane);
+    else sort_value_row(s.b_val, s.b_row, s.b_aux, P2, lane);
     double carry = 0.0;
     for (int c0 = 0; c0 < m; c0 += kWarp) {
         double v = (c0 + lane < m) ? s.b_val[c0 + lane] : 0.0;
@@ -571,15 +758,42 @@ __device__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, i
     }
 
     // ---- clique sampling (driver_local.cpp:598-631, auxilliary.hpp:543-592)
+    // Global slabs first search a shared-memory copy of every q-th prefix
+    // sum (all of them when they fit), then the at most q entries between
+    // two copies; the predicate is monotone in j, so the first j found is
+    // the same as a plain binary search's.
+    const double* C = s.a_val;
+    const double* cidx = reinterpret_cast<const double*>(wsm + 1024);
+    int q = 1, nidx = 0;
+    if (global) {
+        double* ci_w = reinterpret_cast<double*>(wsm + 1024);
+        const int cap = (a.smem_region - 1024) / 8;
+        while ((m + q - 1) / q > cap) q <<= 1;
+        nidx = (m + q - 1) / q;
+        for (int t = lane; t < nidx; t += kWarp) ci_w[t] = s.a_val[t * q];
+        __syncwarp();
+        if (q == 1) C = cidx;
+    }
     bool ok = true;
     for (int i = lane; i < m - 1; i += kWarp) {
-        const double ci = s.a_val[i];
+        const double ci = C[i];
         const double rem_i = __dsub_rn(S, ci);
         const double target = __dmul_rn(sample_uniform(a.seed, k, i), rem_i);
         int lo = i + 1, hi = m;
+        if (q > 1) {
+            int tl = (lo + q - 1) / q, th = nidx;
+            const int tfirst = tl;
+            while (tl < th) {
+                const int mid = (tl + th) >> 1;
+                if (__dsub_rn(cidx[mid], ci) < target) tl = mid + 1;
+                else th = mid;
+            }
+            if (tl < nidx) hi = tl * q + 1;
+            if (tl > tfirst) lo = max(lo, (tl - 1) * q + 1);
+        }
         while (lo < hi) {
             int mid = lo + ((hi - lo) >> 1);
-            if (__dsub_rn(s.a_val[mid], ci) < target) lo = mid + 1;
+            if (__dsub_rn(C[mid], ci) < target) lo = mid + 1;
             else hi = mid;
         }
         const int j = lo < m ? lo : m - 1;
@@ -611,12 +825,15 @@ __device__ bool eliminate_slab(const FactorArgs& a, int32_t k, int nf, int o0, i
     return true;
 }
 
-__global__ void __launch_bounds__(256) factor_kernel(FactorArgs a) {
+// at most 85 registers (3 CTAs per SM): the rare large-vertex paths spill
+// rather than costing the common path its occupancy
+__global__ void __launch_bounds__(256, 3) factor_kernel(FactorArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & (kWarp - 1);
     const int wib = threadIdx.x >> 5;
     const int warp_global = blockIdx.x * (blockDim.x >> 5) + wib;
-    Slab sm = make_slab(smem + (size_t)wib * (size_t)a.smem_slab * kSlabBytesPerEntry, a.smem_slab);
+    unsigned char* wsm = smem + (size_t)wib * (size_t)a.smem_region;
+    Slab sm = make_slab(wsm, a.smem_slab);
     const unsigned long long t0 = global_timer_ns();
     int64_t pool_cur = 0, pool_end = 0;
     long long fills = 0;
@@ -664,7 +881,7 @@ __global__ void __launch_bounds__(256) factor_kernel(FactorArgs a) {
             if (k < 0) break;
         }
         __threadfence();
-        if (!eliminate(a, k, sm, warp_global, lane, pool_cur, pool_end, fills, next, max_gather)) break;
+        if (!eliminate(a, k, sm, wsm, warp_global, lane, pool_cur, pool_end, fills, next, max_gather)) break;
         ++done_local;
         if (aborted(a)) break;
     }
@@ -803,8 +1020,11 @@ cudaError_t launch_init_factor_state(FactorWork& w, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// per warp: the shared-memory slab, at least 2 KB (radix histogram + CDF index of global slabs)
+static int smem_region_bytes(int smem_slab) { return (smem_slab > 64 ? smem_slab : 64) * kSlabBytesPerEntry; }
+
 size_t factor_smem_bytes(int block, int smem_slab) {
-    return (size_t)(block / kWarp) * (size_t)smem_slab * kSlabBytesPerEntry;
+    return (size_t)(block / kWarp) * (size_t)smem_region_bytes(smem_slab);
 }
 
 int factor_resident_grid(int block, int smem_slab, int device) {
@@ -851,6 +1071,7 @@ cudaError_t launch_factor(FactorWork& w, const FactorLaunch& cfg, cudaStream_t s
     a.pool_cursor = w.counters64;
     a.seed = cfg.seed;
     a.smem_slab = cfg.smem_slab;
+    a.smem_region = smem_region_bytes(cfg.smem_slab);
     a.timeout_ns = (unsigned long long)(cfg.timeout_s * 1e9);
     size_t smem = factor_smem_bytes(cfg.block, cfg.smem_slab);
     cudaError_t e = cudaFuncSetAttribute(factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

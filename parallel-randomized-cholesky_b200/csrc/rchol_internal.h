@@ -91,7 +91,7 @@ struct FactorWork {
     int32_t* brow = nullptr;      // [n*c0]
     double* bval = nullptr;       // [n*c0]
     int32_t* chead = nullptr;     // [n] first overflow chunk of each column (-1)
-    int32_t* cnext = nullptr;     // [nchunks] next chunk (-1)
+    int32_t* cnext = nullptr;     // [nchunks] next chunk (-1), by the chunk's first pool unit
     int32_t* crow = nullptr;      // [nchunks*64]
     double* cval = nullptr;       // [nchunks*64]
     int32_t nchunks = 0;
@@ -227,6 +227,8 @@ cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, cudaStream_t s);
 
 // Shared large slabs of the elimination kernel.
 constexpr int kHugeSlabs = 8;
+// Bytes per entry of elimination slabs in global memory (with radix-sort buffers).
+constexpr int kGlobalSlabBytes = 56;
 
 // *out = max(v[0..n-1]) (device, *out must start at 0).
 cudaError_t max_i32(const int32_t* v, int64_t n, int32_t* out, cudaStream_t s);

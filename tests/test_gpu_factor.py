@@ -111,6 +111,18 @@ def test_factor_large_gather_uses_shared_slab():
     assert info.max_gather >= 6000
 
 
+@pytest.mark.parametrize("opts", [dict(), dict(bucket_cap=2, slab_entries=32)])
+def test_factor_power_law_bitexact(opts):
+    """Power-law graph: hub columns take long overflow chunk chains and
+    gathers in global slabs (radix-sorted, searched through the shared
+    index); the factor still equals the oracle's bit for bit."""
+    n, r, c, v, g = R.generate("chunglu", [6000, 30000, 2, 1500], wlo=1.0, whi=10.0, seed=7)
+    P = OracleProblem(n, r, c, v, trim=g)
+    gpu, info = _gpu_factor(n, r, c, v, g, seed=12, **opts)
+    _compare(gpu, P.factor(seed=12))
+    assert info.max_gather > 256
+
+
 def test_factor_repeatable_in_one_context():
     n, r, c, v, _ = grid_laplacian((30, 30), seed=8)
     ctx = R.Context(seed=3)
