@@ -210,10 +210,11 @@ __global__ void sched_hist_kernel(const int32_t* __restrict__ level, const int64
 
 // Longest path from each row to a sink of the L^T solve DAG:
 // levb[j] = 1 + max over i in column j of levb[i] (0 for an empty column).
-// Rows are visited in a topological order (`order`) by persistent warps
-// round-robin; each waits for the levels it needs (-1 = pending), bounded.
+// Rows are visited in the reverse of the forward schedule (a topological
+// order of the L^T DAG) by persistent warps round-robin; each waits for the
+// levels it needs (-1 = pending), bounded.
 __global__ void bwd_level_kernel(int32_t n, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                 const int32_t* __restrict__ order, int32_t* levb, int32_t* status,
+                                 const int32_t* __restrict__ order_f, int32_t* levb, int32_t* status,
                                  unsigned long long timeout_ns) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -221,7 +222,7 @@ __global__ void bwd_level_kernel(int32_t n, const int64_t* __restrict__ ptr, con
     const unsigned long long t0 = global_timer_ns();
     bool ok = true;
     for (int64_t t = warp; t < n && ok; t += nwarps) {
-        const int32_t j = order[t];
+        const int32_t j = order_f[n - 1 - t];
         int m = -1;
         for (int64_t p = ptr[j] + lane; p < ptr[j + 1]; p += 32) {
             int v;
@@ -690,15 +691,15 @@ cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bo
     // forward: rows of Lr; backward: rows of L^T = columns of Lc
     RCHOL_TRY(build_one_schedule(level, f.lr_ptr, f.n, f.depth, 0, epl, sc, f.order_f, &f.tasks_f, f.cap_tf,
                                  &f.ntasks_f, s));
-    RCHOL_TRY(build_one_schedule(level, f.lc_ptr, f.n, f.depth, 1, epl, sc, f.order_b, &f.tasks_b, f.cap_tb,
-                                 &f.ntasks_b, s));
     f.depth_b = f.depth;
     if (!exact_bwd || f.n == 0) {
+        RCHOL_TRY(build_one_schedule(level, f.lc_ptr, f.n, f.depth, 1, epl, sc, f.order_b, &f.tasks_b, f.cap_tb,
+                                     &f.ntasks_b, s));
         // reversed forward levels: the backward gate is the dependency of least forward level
         RCHOL_TRY(build_layouts(f, level, level, -1, sc, s));
         return cudaStreamSynchronize(s);
     }
-    // true backward levels, visited in the reversed-forward order just built
+    // true backward levels, visited in the reversed forward order
     int32_t *levb = nullptr, *st = nullptr;
     RCHOL_TRY(sc.get(&levb, f.n));
     RCHOL_TRY(sc.get(&st, 2));
@@ -708,7 +709,7 @@ cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bo
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bwd_level_kernel, 256, 0);
-    bwd_level_kernel<<<std::max(1, per_sm * sms), 256, 0, s>>>(f.n, f.lc_ptr, f.lc_idx, f.order_b, levb, st,
+    bwd_level_kernel<<<std::max(1, per_sm * sms), 256, 0, s>>>(f.n, f.lc_ptr, f.lc_idx, f.order_f, levb, st,
                                                               (unsigned long long)(timeout_s * 1e9));
     RCHOL_TRY(cudaGetLastError());
     max_kernel<<<grid_for(f.n, 256), 256, 0, s>>>(levb, f.n, st + 1);
