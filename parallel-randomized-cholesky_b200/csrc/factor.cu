@@ -130,13 +130,12 @@ __device__ void sort_value_row(double* val, int32_t* row, long long* aux, int P,
 }
 
 // ---- warp radix sorts for slabs in global memory ------------------------
-// Stable LSD passes over 8-bit digits: a histogram pass, then a scatter pass
-// in which each 32-entry round ranks equal digits with a match mask, so equal
-// digits keep their order.  A pass whose entries all share the digit moves
-// nothing.  `hist` is 256 ints of the warp's shared memory.  The result is
-// the unique order of the keys, the same as the bitonic sorts give.
-
-constexpr int kRadixBatch = 1;  // entries per lane per round (more costs the common paths registers)
+// Stable LSD passes over 8-bit digits.  In a scatter pass each 32-entry
+// round ranks equal digits with a match mask, so equal digits keep their
+// order, and the next digit is counted on the way; a digit shared by every
+// entry moves nothing.  `hist` is 2 x 256 ints of the warp's shared memory.
+// The result is the unique order of the keys, the same as the bitonic sorts
+// give.
 
 // digit d of (row, value bits): bytes 0-7 of the value bits, then bytes 0-3 of the row
 __device__ __forceinline__ int rv_digit(int32_t r, double v, int d) {
@@ -146,29 +145,18 @@ __device__ __forceinline__ int rv_digit(int32_t r, double v, int d) {
 // digit d of (value bits, row): bytes 0-3 of the row, then bytes 0-7 of the value bits
 __device__ __forceinline__ int vr_digit(int32_t r, double v, int d) { return rv_digit(r, v, (d + 8) % 12); }
 
-// Histogram of digit d over n entries; returns true when every entry has
-// the same digit (the pass can be skipped).  Leaves exclusive offsets in hist.
+// Counts of digit d over n entries into hist (256 ints, zeroed here).
 template <bool VR>
-__device__ bool radix_hist(const int32_t* row, const double* val, int n, int d, int* hist, int lane) {
+__device__ void radix_count(const int32_t* row, const double* val, int n, int d, int* hist, int lane) {
     for (int i = lane; i < 256; i += kWarp) hist[i] = 0;
     __syncwarp();
-    for (int base = 0; base < n; base += kWarp * kRadixBatch) {
-        int32_t r[kRadixBatch];
-        double v[kRadixBatch];
-#pragma unroll
-        for (int q = 0; q < kRadixBatch; ++q) {
-            const int i = base + q * kWarp + lane;
-            if (i < n) {
-                r[q] = row[i];
-                v[q] = val[i];
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < kRadixBatch; ++q)
-            if (base + q * kWarp + lane < n) atomicAdd(&hist[VR ? vr_digit(r[q], v[q], d) : rv_digit(r[q], v[q], d)], 1);
-    }
+    for (int i = lane; i < n; i += kWarp) atomicAdd(&hist[VR ? vr_digit(row[i], val[i], d) : rv_digit(row[i], val[i], d)], 1);
     __syncwarp();
-    // exclusive scan: lane l owns buckets 8l..8l+7
+}
+
+// Turns the counts in hist into exclusive offsets; true when one digit holds
+// all n entries (the pass would move nothing).
+__device__ bool radix_offsets(int* hist, int n, int lane) {
     int c[8], tot = 0;
     bool one = false;
 #pragma unroll
@@ -195,83 +183,81 @@ __device__ bool radix_hist(const int32_t* row, const double* val, int n, int d, 
     return all;
 }
 
-// One stable scatter pass of (row, val[, aux]) by digit d; hist holds the offsets.
+// One stable scatter pass of (row, val[, aux]) by digit d (hist holds the
+// offsets), counting digit d + 1 of the moved entries into hnext (zeroed here).
 template <bool VR, bool AUX>
 __device__ void radix_scatter(const int32_t* row, const double* val, const long long* aux, int32_t* orow, double* oval,
-                              long long* oaux, int n, int d, int* hist, int lane) {
+                              long long* oaux, int n, int d, int* hist, int* hnext, int lane) {
     const unsigned lt = (1u << lane) - 1u;
-    for (int base = 0; base < n; base += kWarp * kRadixBatch) {
-        int32_t r[kRadixBatch];
-        double v[kRadixBatch];
-        long long x[kRadixBatch];
-#pragma unroll
-        for (int q = 0; q < kRadixBatch; ++q) {
-            const int i = base + q * kWarp + lane;
-            if (i < n) {
-                r[q] = row[i];
-                v[q] = val[i];
-                if (AUX) x[q] = aux[i];
-            }
+    for (int i = lane; i < 256; i += kWarp) hnext[i] = 0;
+    __syncwarp();
+    for (int base = 0; base < n; base += kWarp) {
+        const int i = base + lane;
+        const bool valid = i < n;
+        int32_t r = 0;
+        double v = 0.0;
+        long long x = 0;
+        if (valid) {
+            r = row[i];
+            v = val[i];
+            if (AUX) x = aux[i];
         }
-#pragma unroll
-        for (int q = 0; q < kRadixBatch; ++q) {
-            const bool valid = base + q * kWarp + lane < n;
-            const int dig = valid ? (VR ? vr_digit(r[q], v[q], d) : rv_digit(r[q], v[q], d)) : 256;
-            const unsigned peers = __match_any_sync(kFull, dig);
-            const int rank = __popc(peers & lt);
-            const int at = valid ? hist[dig] + rank : 0;
-            __syncwarp();
-            if (valid && rank == 0) hist[dig] += __popc(peers);
-            __syncwarp();
-            if (valid) {
-                orow[at] = r[q];
-                oval[at] = v[q];
-                if (AUX) oaux[at] = x[q];
-            }
+        const int dig = valid ? (VR ? vr_digit(r, v, d) : rv_digit(r, v, d)) : 256;
+        const unsigned peers = __match_any_sync(kFull, dig);
+        const int rank = __popc(peers & lt);
+        const int at = valid ? hist[dig] + rank : 0;
+        __syncwarp();
+        if (valid && rank == 0) hist[dig] += __popc(peers);
+        if (valid && d + 1 < 12) atomicAdd(&hnext[VR ? vr_digit(r, v, d + 1) : rv_digit(r, v, d + 1)], 1);
+        __syncwarp();
+        if (valid) {
+            orow[at] = r;
+            oval[at] = v;
+            if (AUX) oaux[at] = x;
         }
     }
     __syncwarp();
 }
 
-// (a_row, a_val) ascending by (row, value bits), result in a_*.
-__device__ void radix_sort_rv(const Slab& s, int n, int* hist, int lane) {
-    int32_t *r0 = s.a_row, *r1 = s.t_row;
-    double *v0 = s.a_val, *v1 = s.t_val;
+// LSD radix sort of n entries through the ping-pong buffers; the result is
+// copied back into (r_out, v_out[, x_out]) when it ends in the other buffer.
+template <bool VR, bool AUX>
+__device__ void radix_sort(int32_t* r_out, double* v_out, long long* x_out, int32_t* r_tmp, double* v_tmp,
+                           long long* x_tmp, int n, int* hist, int* hnext, int lane) {
+    int32_t *r0 = r_out, *r1 = r_tmp;
+    double *v0 = v_out, *v1 = v_tmp;
+    long long *x0 = x_out, *x1 = x_tmp;
+    radix_count<VR>(r0, v0, n, 0, hist, lane);
     for (int d = 0; d < 12; ++d) {
-        if (radix_hist<false>(r0, v0, n, d, hist, lane)) continue;
-        radix_scatter<false, false>(r0, v0, nullptr, r1, v1, nullptr, n, d, hist, lane);
+        if (radix_offsets(hist, n, lane)) {
+            // nothing moves: count the next digit from the current buffer
+            if (d + 1 < 12) radix_count<VR>(r0, v0, n, d + 1, hist, lane);
+            continue;
+        }
+        radix_scatter<VR, AUX>(r0, v0, x0, r1, v1, x1, n, d, hist, hnext, lane);
+        int* th = hist; hist = hnext; hnext = th;
         int32_t* tr = r0; r0 = r1; r1 = tr;
         double* tv = v0; v0 = v1; v1 = tv;
+        long long* tx = x0; x0 = x1; x1 = tx;
     }
-    if (r0 != s.a_row) {
+    if (r0 != r_out) {
         for (int i = lane; i < n; i += kWarp) {
-            s.a_row[i] = r0[i];
-            s.a_val[i] = v0[i];
+            r_out[i] = r0[i];
+            v_out[i] = v0[i];
+            if (AUX) x_out[i] = x0[i];
         }
         __syncwarp();
     }
 }
 
+// (a_row, a_val) ascending by (row, value bits), result in a_*.
+__device__ __forceinline__ void radix_sort_rv(const Slab& s, int n, int* hist, int lane) {
+    radix_sort<false, false>(s.a_row, s.a_val, nullptr, s.t_row, s.t_val, nullptr, n, hist, hist + 256, lane);
+}
+
 // (b_val, b_row, b_aux) ascending by (value, row), result in b_*.
-__device__ void radix_sort_vr(const Slab& s, int n, int* hist, int lane) {
-    int32_t *r0 = s.b_row, *r1 = s.t_row;
-    double *v0 = s.b_val, *v1 = s.t_val;
-    long long *x0 = s.b_aux, *x1 = s.t_aux;
-    for (int d = 0; d < 12; ++d) {
-        if (radix_hist<true>(r0, v0, n, d, hist, lane)) continue;
-        radix_scatter<true, true>(r0, v0, x0, r1, v1, x1, n, d, hist, lane);
-        int32_t* tr = r0; r0 = r1; r1 = tr;
-        double* tv = v0; v0 = v1; v1 = tv;
-        long long* tx = x0; x0 = x1; x1 = tx;
-    }
-    if (r0 != s.b_row) {
-        for (int i = lane; i < n; i += kWarp) {
-            s.b_row[i] = r0[i];
-            s.b_val[i] = v0[i];
-            s.b_aux[i] = x0[i];
-        }
-        __syncwarp();
-    }
+__device__ __forceinline__ void radix_sort_vr(const Slab& s, int n, int* hist, int lane) {
+    radix_sort<true, true>(s.b_row, s.b_val, s.b_aux, s.t_row, s.t_val, s.t_aux, n, hist, hist + 256, lane);
 }
 
 struct FactorArgs {
@@ -701,9 +687,32 @@ __device__ __forceinline__ bool eliminate_slab(const FactorArgs& a, int32_t k, i
             int rank = m + __popc(bal & lt_mask);
             double acc = s.a_val[i];
             int cnt = 1;
-            for (int j = i + 1; j < total && s.a_row[j] == ri; ++j) {
-                acc = __dadd_rn(acc, s.a_val[j]);
-                ++cnt;
+            if (global) {
+                // runs in global slabs: read 8 entries per round trip, add in order
+                bool more = true;
+                for (int j0 = i + 1; more && j0 < total; j0 += 8) {
+                    int32_t rr[8];
+                    double vv[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        rr[q] = j0 + q < total ? s.a_row[j0 + q] : -1;
+                        vv[q] = j0 + q < total ? s.a_val[j0 + q] : 0.0;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        if (more && rr[q] == ri) {
+                            acc = __dadd_rn(acc, vv[q]);
+                            ++cnt;
+                        } else {
+                            more = false;
+                        }
+                    }
+                }
+            } else {
+                for (int j = i + 1; j < total && s.a_row[j] == ri; ++j) {
+                    acc = __dadd_rn(acc, s.a_val[j]);
+                    ++cnt;
+                }
             }
             s.b_val[rank] = acc;
             s.b_row[rank] = ri;
