@@ -273,25 +273,72 @@ __global__ void sched_task_emit_kernel(const int32_t* __restrict__ hist, const i
     }
 }
 
-// slots per lane of each task: the longest of its rows over G lanes
-__global__ void pack_m_kernel(const int2* __restrict__ tasks, int32_t ntasks, const int64_t* __restrict__ optr,
-                              int32_t* m) {
+__global__ void mask_mul_kernel(const int32_t* __restrict__ a, const int32_t* __restrict__ mask, int32_t* out,
+                                int32_t n) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) out[t] = mask[t] ? a[t] : 0;
+}
+
+// Parts of each scheduled task: 1, or ceil(len / kSplitLen) for a one-row
+// task of the widest class whose row is longer than kSplitMin.
+__global__ void pack_nsub_kernel(const int2* __restrict__ tasks, int32_t ntasks, const int64_t* __restrict__ optr,
+                                 int32_t* nsub, int32_t* issplit) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntasks; t += stride) {
         const int2 d = tasks[t];
         const int cls = d.y >> 8, cnt = d.y & 0xff;
-        int64_t longest = 0;
-        for (int r = 0; r < cnt; ++r) longest = max(longest, optr[d.x + r + 1] - optr[d.x + r]);
+        const int64_t len = cnt == 1 ? optr[d.x + 1] - optr[d.x] : 0;
+        const int np = (cls == kLaneClasses - 1 && len > kSplitMin) ? (int)((len + kSplitLen - 1) / kSplitLen) : 1;
+        nsub[t] = np;
+        issplit[t] = np > 1 ? 1 : 0;
+    }
+}
+
+// Expanded tasks {position, d.z bits, part count, part length or 0} and the
+// split bookkeeping of part tasks.
+__global__ void pack_expand_kernel(const int2* __restrict__ tasks, int32_t ntasks, const int64_t* __restrict__ optr,
+                                   const int32_t* __restrict__ order, const int32_t* __restrict__ nsub,
+                                   const int32_t* __restrict__ tbase, const int32_t* __restrict__ sid,
+                                   const int32_t* __restrict__ pbase, int4* etask, int2* split, int32_t* srow) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntasks; t += stride) {
+        const int2 d = tasks[t];
+        const int np = nsub[t];
+        if (np == 1) {
+            etask[tbase[t]] = make_int4(d.x, d.y, 1, 0);
+            continue;
+        }
+        const int64_t len = optr[d.x + 1] - optr[d.x];
+        srow[sid[t]] = order[d.x];
+        for (int q = 0; q < np; ++q) {
+            const int plen = (int)min((int64_t)kSplitLen, len - (int64_t)q * kSplitLen);
+            etask[tbase[t] + q] = make_int4(d.x, d.y | (1 << 11) | (q << 12), np, plen);
+            split[tbase[t] + q] = make_int2(sid[t], pbase[t]);
+        }
+    }
+}
+
+// slots per lane of each expanded task: the longest of its rows (or the
+// part's length) over G lanes
+__global__ void pack_m_kernel(const int4* __restrict__ etask, int32_t ntasks, const int64_t* __restrict__ optr,
+                              int32_t* m) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntasks; t += stride) {
+        const int4 e = etask[t];
+        const int cls = (e.y >> 8) & 7, cnt = e.y & 0xff;
+        int64_t longest = e.w;
+        if (!((e.y >> 11) & 1))
+            for (int r = 0; r < cnt; ++r) longest = max(longest, optr[e.x + r + 1] - optr[e.x + r]);
         m[t] = (int32_t)((longest + (1 << cls) - 1) >> cls);
     }
 }
 
-__global__ void pack_desc_kernel(const int2* __restrict__ tasks, int32_t ntasks, const int32_t* __restrict__ m,
+__global__ void pack_desc_kernel(const int4* __restrict__ etask, int32_t ntasks, const int32_t* __restrict__ m,
                                  const int64_t* __restrict__ base, int4* pack) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntasks; t += stride) {
-        const int2 d = tasks[t];
-        pack[t] = make_int4(d.x, (int32_t)base[t], d.y, m[t]);
+        const int4 e = etask[t];
+        pack[t] = make_int4(e.x, (int32_t)base[t], e.y, m[t] | (((e.y >> 11) & 1) ? e.z << 8 : 0));
     }
 }
 
@@ -314,6 +361,11 @@ __global__ void pack_fill_kernel(const int4* __restrict__ pack, int32_t ntasks, 
         if (r < cnt) {
             s = optr[d.x + r];
             len = optr[d.x + r + 1] - s;
+            if ((d.z >> 11) & 1) {  // part task: its window of the row
+                const int64_t q0 = (int64_t)(d.z >> 12) * kSplitLen;
+                s += q0;
+                len = min((int64_t)kSplitLen, len - q0);
+            }
         }
         // gate of the row: best (key, entry) over the lane's entries, then over the G lanes
         long long best_key = LLONG_MIN, best_e = 0;
@@ -332,7 +384,8 @@ __global__ void pack_fill_kernel(const int4* __restrict__ pack, int32_t ntasks, 
                 best_e = oe;
             }
         }
-        for (int k = 0; k < d.w; ++k) {
+        const int mslots = d.w & 0xff;
+        for (int k = 0; k < mslots; ++k) {
             int64_t e = ((int64_t)k << cls) + gl;
             const size_t o = ((size_t)d.y + k) * 32 + lane;
             const bool have = e < len;
@@ -599,43 +652,106 @@ static cudaError_t build_layout(int32_t n, const int32_t* order, const int64_t* 
     return cudaGetLastError();
 }
 
-// Task slabs of one direction from its task list and schedule-ordered layout.
-static cudaError_t build_pack(int32_t ntasks, const int2* tasks, const int64_t* optr, const int32_t* sidx,
-                              const double* sval, const float* sval32, const int32_t* level, int sign, int4** pack, int64_t& cap_d, int32_t** pidx,
-                              int64_t& cap_i, double** pval, int64_t& cap_v, float** pval32, int64_t& cap_w,
-                              int64_t* slots, Scratch& sc, cudaStream_t s) {
-    int32_t* m = nullptr;
-    int64_t* base = nullptr;
-    void* tmp = nullptr;
+// Output arrays of one direction's task slabs.
+struct PackOut {
+    int4** pack;
+    int64_t* cap_d;
+    int32_t** pidx;
+    int64_t* cap_i;
+    double** pval;
+    int64_t* cap_v;
+    float** pval32;
+    int64_t* cap_w;
+    int64_t* slots;
+    int32_t* npt;
+    int32_t* nsplit;
+    int2** split;
+    int64_t* cap_s;
+    double** psum;
+    int64_t* cap_q;
+    int32_t** pcount;
+    int64_t* cap_c;
+    int32_t** srow;
+    int64_t* cap_r;
+};
+
+// Task slabs of one direction from its task list and schedule-ordered
+// layout; rows longer than kSplitMin are split into part tasks first.
+static cudaError_t build_pack(int32_t ntasks, const int2* tasks, const int32_t* order, const int64_t* optr,
+                              const int32_t* sidx, const double* sval, const float* sval32, const int32_t* level,
+                              int sign, const PackOut& o, Scratch& sc, cudaStream_t s) {
     const int64_t nt = std::max<int32_t>(ntasks, 1);
-    RCHOL_TRY(sc.get(&m, nt));
-    RCHOL_TRY(sc.get(&base, nt + 1));
+    int32_t *nsub = nullptr, *issplit = nullptr, *tbase = nullptr, *sid = nullptr, *pbase = nullptr;
+    void* tmp = nullptr;
+    RCHOL_TRY(sc.get(&nsub, nt));
+    RCHOL_TRY(sc.get(&issplit, nt));
+    RCHOL_TRY(sc.get(&tbase, nt + 1));
+    RCHOL_TRY(sc.get(&sid, nt + 1));
+    RCHOL_TRY(sc.get(&pbase, nt + 1));
     RCHOL_TRY(sc.get((char**)&tmp, (int64_t)scan_tmp_bytes(nt)));
-    RCHOL_TRY(ensure(pack, cap_d, nt));
+    *o.npt = 0;
+    *o.nsplit = 0;
+    *o.slots = 0;
     if (ntasks == 0) {
-        *slots = 0;
+        RCHOL_TRY(ensure(o.pack, *o.cap_d, 1));
         return cudaSuccess;
     }
-    pack_m_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(tasks, ntasks, optr, m);
-    RCHOL_TRY(exclusive_scan_i32_to_i64(m, base, ntasks, tmp, s));
+    pack_nsub_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(tasks, ntasks, optr, nsub, issplit);
+    RCHOL_TRY(exclusive_scan_i32_to_i32(nsub, tbase, ntasks, tmp, s));
+    RCHOL_TRY(exclusive_scan_i32_to_i32(issplit, sid, ntasks, tmp, s));
+    int32_t hs[2] = {0, 0};
+    RCHOL_TRY(cudaMemcpyAsync(&hs[0], tbase + ntasks, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    RCHOL_TRY(cudaMemcpyAsync(&hs[1], sid + ntasks, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    RCHOL_TRY(cudaStreamSynchronize(s));
+    const int32_t ne = hs[0], nsp = hs[1];
+    // first partial of each split task: exclusive scan of its part count
+    int32_t nparts = 0;
+    if (nsp > 0) {
+        int32_t* psub = nullptr;
+        RCHOL_TRY(sc.get(&psub, nt));
+        mask_mul_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(nsub, issplit, psub, ntasks);
+        RCHOL_TRY(exclusive_scan_i32_to_i32(psub, pbase, ntasks, tmp, s));
+        RCHOL_TRY(cudaMemcpyAsync(&nparts, pbase + ntasks, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        RCHOL_TRY(cudaStreamSynchronize(s));
+    }
+    int4* etask = nullptr;
+    int32_t* m = nullptr;
+    int64_t* base = nullptr;
+    void* tmp2 = nullptr;
+    RCHOL_TRY(sc.get(&etask, ne));
+    RCHOL_TRY(sc.get(&m, ne));
+    RCHOL_TRY(sc.get(&base, (int64_t)ne + 1));
+    RCHOL_TRY(sc.get((char**)&tmp2, (int64_t)scan_tmp_bytes(ne)));
+    RCHOL_TRY(ensure(o.pack, *o.cap_d, (int64_t)ne));
+    RCHOL_TRY(ensure(o.split, *o.cap_s, std::max<int64_t>(ne, 1)));
+    RCHOL_TRY(ensure(o.psum, *o.cap_q, std::max<int64_t>(nparts, 1)));
+    RCHOL_TRY(ensure(o.pcount, *o.cap_c, std::max<int64_t>(nsp, 1)));
+    RCHOL_TRY(ensure(o.srow, *o.cap_r, std::max<int64_t>(nsp, 1)));
+    RCHOL_TRY(cudaMemsetAsync(*o.pcount, 0, sizeof(int32_t) * (size_t)std::max<int32_t>(nsp, 1), s));
+    pack_expand_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(tasks, ntasks, optr, order, nsub, tbase, sid, pbase, etask,
+                                                             *o.split, *o.srow);
+    pack_m_kernel<<<grid_for(ne, 256), 256, 0, s>>>(etask, ne, optr, m);
+    RCHOL_TRY(exclusive_scan_i32_to_i64(m, base, ne, tmp2, s));
     int64_t units = 0;
-    RCHOL_TRY(cudaMemcpyAsync(&units, base + ntasks, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RCHOL_TRY(cudaMemcpyAsync(&units, base + ne, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     RCHOL_TRY(cudaStreamSynchronize(s));
     if (units >= (int64_t)INT32_MAX) return cudaErrorInvalidValue;  // slab offsets are int32 units
     const int64_t nslots = std::max<int64_t>(units * 32, 32);
-    *slots = units * 32;
-    RCHOL_TRY(ensure(pidx, cap_i, nslots));
-    RCHOL_TRY(ensure(pval, cap_v, nslots));
+    *o.slots = units * 32;
+    *o.npt = ne;
+    *o.nsplit = nsp;
+    RCHOL_TRY(ensure(o.pidx, *o.cap_i, nslots));
+    RCHOL_TRY(ensure(o.pval, *o.cap_v, nslots));
     if (sval32) {
-        RCHOL_TRY(ensure(pval32, cap_w, nslots));
+        RCHOL_TRY(ensure(o.pval32, *o.cap_w, nslots));
     } else {
-        cudaFree(*pval32);
-        *pval32 = nullptr;
-        cap_w = 0;
+        cudaFree(*o.pval32);
+        *o.pval32 = nullptr;
+        *o.cap_w = 0;
     }
-    pack_desc_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(tasks, ntasks, m, base, *pack);
-    pack_fill_kernel<<<grid_for((int64_t)ntasks * 32, 256), 256, 0, s>>>(
-        *pack, ntasks, optr, sidx, sval, sval32, level, sign, *pidx, *pval, sval32 ? *pval32 : nullptr);
+    pack_desc_kernel<<<grid_for(ne, 256), 256, 0, s>>>(etask, ne, m, base, *o.pack);
+    pack_fill_kernel<<<grid_for((int64_t)ne * 32, 256), 256, 0, s>>>(
+        *o.pack, ne, optr, sidx, sval, sval32, level, sign, *o.pidx, *o.pval, sval32 ? *o.pval32 : nullptr);
     return cudaGetLastError();
 }
 
@@ -668,12 +784,16 @@ static cudaError_t build_layouts(DevFactor& f, const int32_t* level_f, const int
                            f.sf_val32, sc, s));
     RCHOL_TRY(build_layout(f.n, f.order_b, f.lc_ptr, f.lc_idx, f.lc_val, f.lc_val32, f.sb_ptr, f.sb_idx, f.sb_val,
                            f.sb_val32, sc, s));
-    RCHOL_TRY(build_pack(f.ntasks_f, f.tasks_f, f.sf_ptr, f.sf_idx, f.sf_val, f.sf_val32, level_f, 1, &f.pack_f,
-                         f.cap_pdf,
-                         &f.pf_idx, f.cap_pif, &f.pf_val, f.cap_pvf, &f.pf_val32, f.cap_pwf, &f.slots_f, sc, s));
-    RCHOL_TRY(build_pack(f.ntasks_b, f.tasks_b, f.sb_ptr, f.sb_idx, f.sb_val, f.sb_val32, level_b, sign_b, &f.pack_b,
-                         f.cap_pdb,
-                         &f.pb_idx, f.cap_pib, &f.pb_val, f.cap_pvb, &f.pb_val32, f.cap_pwb, &f.slots_b, sc, s));
+    const PackOut of{&f.pack_f, &f.cap_pdf, &f.pf_idx, &f.cap_pif, &f.pf_val, &f.cap_pvf, &f.pf_val32, &f.cap_pwf,
+                     &f.slots_f, &f.npt_f, &f.nsplit_f, &f.split_f, &f.cap_sf, &f.psum_f, &f.cap_qf, &f.pcount_f,
+                     &f.cap_cf, &f.srow_f, &f.cap_rf};
+    const PackOut ob{&f.pack_b, &f.cap_pdb, &f.pb_idx, &f.cap_pib, &f.pb_val, &f.cap_pvb, &f.pb_val32, &f.cap_pwb,
+                     &f.slots_b, &f.npt_b, &f.nsplit_b, &f.split_b, &f.cap_sb, &f.psum_b, &f.cap_qb, &f.pcount_b,
+                     &f.cap_cb, &f.srow_b, &f.cap_rb};
+    RCHOL_TRY(build_pack(f.ntasks_f, f.tasks_f, f.order_f, f.sf_ptr, f.sf_idx, f.sf_val, f.sf_val32, level_f, 1, of,
+                         sc, s));
+    RCHOL_TRY(build_pack(f.ntasks_b, f.tasks_b, f.order_b, f.sb_ptr, f.sb_idx, f.sb_val, f.sb_val32, level_b, sign_b,
+                         ob, sc, s));
     return cudaSuccess;
 }
 

@@ -99,7 +99,8 @@ void free_factor(DevFactor& f) {
     void* ps[] = {f.lc_ptr, f.lc_idx,  f.lc_val,  f.lc_val32, f.lr_ptr,  f.lr_idx, f.lr_val,
                   f.lr_val32, f.diag, f.diag32, f.order_f, f.order_b, f.tasks_f, f.tasks_b,
                   f.sf_ptr, f.sf_idx, f.sf_val, f.sf_val32, f.sb_ptr, f.sb_idx, f.sb_val, f.sb_val32,
-                  f.pack_f, f.pack_b, f.pf_idx, f.pf_val, f.pf_val32, f.pb_idx, f.pb_val, f.pb_val32};
+                  f.pack_f, f.pack_b, f.pf_idx, f.pf_val, f.pf_val32, f.pb_idx, f.pb_val, f.pb_val32,
+                  f.split_f, f.split_b, f.psum_f, f.psum_b, f.pcount_f, f.pcount_b, f.srow_f, f.srow_b};
     for (void* p : ps) cudaFree(p);
     f = DevFactor();
 }

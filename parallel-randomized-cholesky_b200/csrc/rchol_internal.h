@@ -172,6 +172,21 @@ struct DevFactor {
     double* pb_val = nullptr;
     float* pb_val32 = nullptr;
     int64_t slots_f = 0, slots_b = 0;
+    // Rows longer than kSplitMin entries run as several part tasks (flag
+    // 1 << 11 in d.z, part index in d.z >> 12, part count in d.w >> 8); part
+    // tasks carry {split row id, first partial} in split_*, write partial
+    // sums to psum_*, and the last part to finish (pcount_*) publishes the row.
+    int32_t npt_f = 0, npt_b = 0;        // task count after the split
+    int32_t nsplit_f = 0, nsplit_b = 0;  // split rows
+    int2* split_f = nullptr;
+    int2* split_b = nullptr;
+    double* psum_f = nullptr;
+    double* psum_b = nullptr;
+    int32_t* pcount_f = nullptr;
+    int32_t* pcount_b = nullptr;
+    int32_t* srow_f = nullptr;
+    int32_t* srow_b = nullptr;
+    int64_t cap_sf = 0, cap_sb = 0, cap_qf = 0, cap_qb = 0, cap_cf = 0, cap_cb = 0, cap_rf = 0, cap_rb = 0;
     int64_t cap_pdf = 0, cap_pdb = 0, cap_pif = 0, cap_pib = 0, cap_pvf = 0, cap_pvb = 0, cap_pwf = 0,
             cap_pwb = 0;
     int32_t depth = 0;        // number of levels of the forward solve DAG
@@ -179,6 +194,11 @@ struct DevFactor {
     // allocated capacities (buffers of a released factor are reused)
     int64_t cap_n = 0, cap_nnz = 0, cap_tf = 0, cap_tb = 0, cap_ln = 0, cap_lz = 0;
 };
+
+// Rows longer than kSplitMin entries run in the K = 1 solves as part tasks
+// of kSplitLen entries (shorter rows are faster in one warp).
+constexpr int kSplitMin = 1024;
+constexpr int kSplitLen = 512;
 
 // Lane classes of the K = 1 solves: a row gets G = 1, 2, 4, ..., 32 lanes,
 // the smallest G that leaves at most `epl` entries per lane (rows longer

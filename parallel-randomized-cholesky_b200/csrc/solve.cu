@@ -89,6 +89,15 @@ struct SolveArgs {
     const int32_t* __restrict__ pb_idx;
     const void* __restrict__ pb_val;
     int32_t ntasks_f, ntasks_b;
+    // split rows (part tasks) of the K = 1 solves
+    const int2* __restrict__ split_f;
+    const int2* __restrict__ split_b;
+    double* psum_f;
+    double* psum_b;
+    int32_t* pcount_f;
+    int32_t* pcount_b;
+    const int32_t* __restrict__ srow_b;
+    int32_t nsplit_b;
     // vectors (n x K row-major)
     const double* __restrict__ b;
     double* x;
@@ -592,10 +601,9 @@ constexpr int kPackM = 4;  // slab slots per lane held in registers
 #define RCHOL_TRICKLE 2
 #endif
 constexpr unsigned kTrickle = RCHOL_TRICKLE;
-// 4 CTAs of 256 threads per SM (64 registers): more warps for the wide
-// levels outweigh the few spilled registers
+// 3 CTAs of 256 threads per SM (85 registers, no spills in the poll loops)
 #ifndef RCHOL_PACK_MINB
-#define RCHOL_PACK_MINB 4
+#define RCHOL_PACK_MINB 3
 #endif  // gate rounds per re-read of the other pending slots (0: none)
 
 template <typename TV>
@@ -615,7 +623,7 @@ __device__ __forceinline__ void pack_load(PackLane<TV>& L, const int4 d, int lan
     const size_t o = (size_t)d.y * 32 + lane;
 #pragma unroll
     for (int k = 0; k < kPackM; ++k) {
-        if (k < d.w) {
+        if (k < (d.w & 0xff)) {
             L.idx[k] = pidx[o + 32 * k];
             L.val[k] = pval[o + 32 * k];
         } else {
@@ -672,7 +680,7 @@ __device__ __forceinline__ void slab_chunk(const PackLane<TV>& L, int k0, int la
     const size_t o = ((size_t)L.d.y + k0) * 32 + lane;
 #pragma unroll
     for (int k = 0; k < kPackM; ++k) {
-        if (k0 + k < L.d.w) {
+        if (k0 + k < (L.d.w & 0xff)) {
             idx[k] = pidx[o + 32 * k];
             val[k] = pval[o + 32 * k];
         } else {
@@ -689,7 +697,8 @@ __device__ __forceinline__ double pack_dot(const PackLane<TV>& L, int lane, int 
     // slots kPackM..2*kPackM-1 of long rows: fetched now, waited on with the rest
     int32_t idx2[kPackM];
     TV val2[kPackM];
-    const bool two = L.d.w > kPackM;
+    const int mslots = L.d.w & 0xff;
+    const bool two = mslots > kPackM;
     if (two) slab_chunk(L, kPackM, lane, pidx, pval, idx2, val2);
     double v[kPackM], v2[kPackM];
 #pragma unroll
@@ -735,7 +744,7 @@ __device__ __forceinline__ double pack_dot(const PackLane<TV>& L, int lane, int 
 #pragma unroll
         for (int k = 0; k < kPackM; ++k) sum += to_d(val2[k]) * v2[k];
     }
-    for (int k0 = 2 * kPackM; k0 < L.d.w && ok; k0 += kPackM) {
+    for (int k0 = 2 * kPackM; k0 < mslots && ok; k0 += kPackM) {
         int32_t idx[kPackM];
         TV val[kPackM];
         slab_chunk(L, k0, lane, pidx, pval, idx, val);
@@ -777,10 +786,13 @@ __global__ void __launch_bounds__(kBlock, RCHOL_PACK_MINB) fwd_pack_kernel(Solve
         const int cls = (cur.d.z >> 8) & 7, cnt = cur.d.z & 0xff;
         const int G = 1 << cls;
         const bool lead = (lane >> cls) < cnt && (lane & (G - 1)) == 0;
+        const bool part = (cur.d.z >> 11) & 1;
+        const int ipart = cur.d.z >> 12;
         const int32_t i = cur.row;
-        // row data and the x / r update do not depend on the dot product
+        // row data and the x / r update do not depend on the dot product;
+        // a split row's update belongs to its part 0
         double ri = 0.0;
-        if (lead) {
+        if (lead && (!part || ipart == 0)) {
             ri = a.r[i];
             if (a.update) {
                 const double al = a.seg ? a.seg_alpha[a.seg[i]] : alpha;
@@ -796,7 +808,19 @@ __global__ void __launch_bounds__(kBlock, RCHOL_PACK_MINB) fwd_pack_kernel(Solve
         if (t + 2 * nwarps < a.ntasks_f) dn = a.pack_f[t + 2 * nwarps];
         double sum = pack_dot<TV>(cur, lane, G, a.pf_idx, pval, a.y, t0, a.timeout_ns, &a.sc->status, ok, a.poll_ns);
         sum = group_sum(sum, G);
-        if (lead) st_relaxed_f64(a.y + i, ri - sum);
+        if (lead && !part) st_relaxed_f64(a.y + i, ri - sum);
+        if (lead && part) {
+            // partial sum; the last part to finish adds them in part order
+            const int2 sp = a.split_f[t];
+            const int np = cur.d.w >> 8;
+            a.psum_f[sp.y + ipart] = sum;
+            if (atom_add_acq_rel(a.pcount_f + sp.x, 1) == np - 1) {
+                double tot = 0.0;
+                for (int q = 0; q < np; ++q) tot += ld_relaxed_f64(a.psum_f + sp.y + q);
+                st_relaxed_f64(a.y + i, ld_relaxed_f64(a.r + i) - tot);
+                a.pcount_f[sp.x] = 0;
+            }
+        }
         ok = __all_sync(kFull, ok);
         cur = nxt;
     }
@@ -846,10 +870,23 @@ __global__ void __launch_bounds__(kBlock, RCHOL_PACK_MINB) bwd_pack_kernel(Solve
         if (t + 2 * nwarps < a.ntasks_b) dn = a.pack_b[t + 2 * nwarps];
         double sum = pack_dot<TV>(cur, lane, G, a.pb_idx, pval, a.z, t0, a.timeout_ns, &a.sc->status, ok, a.poll_ns);
         sum = group_sum(sum, G);
-        if (lead) {
+        if (lead && !((cur.d.z >> 11) & 1)) {
             const double zj = tj - sum;
             st_relaxed_f64(a.z + j, zj);
             if (a.reduce) acc[0] += rj * zj;
+        } else if (lead) {
+            // partial sum; the last part to finish adds them in part order.
+            // Split rows' r.z terms are added by the reducing block.
+            const int2 sp = a.split_b[t];
+            const int np = cur.d.w >> 8;
+            const int ipart = cur.d.z >> 12;
+            a.psum_b[sp.y + ipart] = sum;
+            if (atom_add_acq_rel(a.pcount_b + sp.x, 1) == np - 1) {
+                double tot = 0.0;
+                for (int q = 0; q < np; ++q) tot += ld_relaxed_f64(a.psum_b + sp.y + q);
+                st_relaxed_f64(a.z + j, tj - tot);
+                a.pcount_b[sp.x] = 0;
+            }
         }
         ok = __all_sync(kFull, ok);
         cur = nxt;
@@ -862,7 +899,17 @@ __global__ void __launch_bounds__(kBlock, RCHOL_PACK_MINB) bwd_pack_kernel(Solve
     block_partials<1>(acc, a.part + (size_t)(2 * a.grid_max + blockIdx.x));
     if (last_block(&a.sc->ticket[3])) {
         sum_partials<1>(a.part + (size_t)2 * a.grid_max, gridDim.x, a.sc->pq);
-        if (threadIdx.x == 0) bwd_scalars(a, 1);
+        if (threadIdx.x == 0) {
+            if (a.nsplit_b) {  // split rows in id order
+                double extra = a.sc->pq[0];
+                for (int q = 0; q < a.nsplit_b; ++q) {
+                    const int32_t j = a.srow_b[q];
+                    extra += a.r[j] * ld_relaxed_f64(a.z + j);
+                }
+                a.sc->pq[0] = extra;
+            }
+            bwd_scalars(a, 1);
+        }
     }
 }
 
@@ -998,8 +1045,16 @@ class PcgSolver {
         a.pf_val = cfg.fp32_factor ? (const void*)F.pf_val32 : (const void*)F.pf_val;
         a.pb_idx = F.pb_idx;
         a.pb_val = cfg.fp32_factor ? (const void*)F.pb_val32 : (const void*)F.pb_val;
-        a.ntasks_f = F.ntasks_f;
-        a.ntasks_b = F.ntasks_b;
+        a.ntasks_f = F.npt_f;
+        a.ntasks_b = F.npt_b;
+        a.split_f = F.split_f;
+        a.split_b = F.split_b;
+        a.psum_f = F.psum_f;
+        a.psum_b = F.psum_b;
+        a.pcount_f = F.pcount_f;
+        a.pcount_b = F.pcount_b;
+        a.srow_b = F.srow_b;
+        a.nsplit_b = F.nsplit_b;
         a.b = b;
         a.x = x;
         a.r = r;
@@ -1839,8 +1894,16 @@ static cudaError_t precond_apply_t(const DevFactor& F, const double* r, double* 
     a.pf_val = std::is_same<TV, float>::value ? (const void*)F.pf_val32 : (const void*)F.pf_val;
     a.pb_idx = F.pb_idx;
     a.pb_val = std::is_same<TV, float>::value ? (const void*)F.pb_val32 : (const void*)F.pb_val;
-    a.ntasks_f = F.ntasks_f;
-    a.ntasks_b = F.ntasks_b;
+    a.ntasks_f = F.npt_f;
+    a.ntasks_b = F.npt_b;
+    a.split_f = F.split_f;
+    a.split_b = F.split_b;
+    a.psum_f = F.psum_f;
+    a.psum_b = F.psum_b;
+    a.pcount_f = F.pcount_f;
+    a.pcount_b = F.pcount_b;
+    a.srow_b = F.srow_b;
+    a.nsplit_b = F.nsplit_b;
     a.r = const_cast<double*>(r);
     a.y = y;
     a.z = z;
@@ -1949,8 +2012,16 @@ cudaError_t precond_apply_noalloc_t(const DevFactor& F, const double* r, double*
     a.pf_val = std::is_same<TV, float>::value ? (const void*)F.pf_val32 : (const void*)F.pf_val;
     a.pb_idx = F.pb_idx;
     a.pb_val = std::is_same<TV, float>::value ? (const void*)F.pb_val32 : (const void*)F.pb_val;
-    a.ntasks_f = F.ntasks_f;
-    a.ntasks_b = F.ntasks_b;
+    a.ntasks_f = F.npt_f;
+    a.ntasks_b = F.npt_b;
+    a.split_f = F.split_f;
+    a.split_b = F.split_b;
+    a.psum_f = F.psum_f;
+    a.psum_b = F.psum_b;
+    a.pcount_f = F.pcount_f;
+    a.pcount_b = F.pcount_b;
+    a.srow_b = F.srow_b;
+    a.nsplit_b = F.nsplit_b;
     a.r = const_cast<double*>(r);
     a.y = y;
     a.z = z;

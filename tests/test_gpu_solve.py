@@ -152,6 +152,52 @@ def test_pcg_bitwise_reproducible_across_factorizations(precision):
     assert results[0][2] == results[1][2]
 
 
+def _hub_laplacian(leaves, seed):
+    rng = np.random.default_rng(seed)
+    n = leaves + 1
+    a = np.concatenate([np.zeros(leaves, np.int64), np.arange(1, n)])
+    b = np.concatenate([np.arange(1, n), np.roll(np.arange(1, n), -1)])
+    w = np.exp(rng.uniform(np.log(1e-2), np.log(1e2), len(a)))
+    d = np.zeros(n)
+    np.add.at(d, a, w)
+    np.add.at(d, b, w)
+    return (n, np.concatenate([a, b, np.arange(n)]).astype(np.int32),
+            np.concatenate([b, a, np.arange(n)]).astype(np.int32), np.concatenate([-w, -w, d]))
+
+
+@pytest.mark.parametrize("graph", ["power_law", "hub"])
+def test_split_rows_match_oracle(graph):
+    """Rows of L (power-law graph) or of L^T (hub ordered first) longer than
+    the split threshold run as several part tasks; the preconditioner and
+    PCG still match the oracle and repeat bit for bit."""
+    if graph == "power_law":
+        n, r, c, v, g = R.generate("chunglu", [20000, 150000, 2, 5000], wlo=1.0, whi=10.0, seed=7)
+    else:
+        (n, r, c, v), g = _hub_laplacian(3000, seed=3), False
+    P = OracleProblem(n, r, c, v, trim=g)
+    orc = P.factor(seed=12)
+    rowlen = np.bincount(orc["rowind"], minlength=P.ns)
+    collen = np.diff(orc["colptr"])
+    assert max(rowlen.max(), collen.max()) > 1024
+    ctx = R.Context(seed=12, precision=R.PREC_FP64, tol=1e-8)
+    try:
+        ctx.set_triplets(n, r, c, v, trim_ground=g)
+        f = ctx.factor()
+        rr = zero_sum_normal(P.ns, 21)
+        z = ctx.precond_apply(f, rr)
+        ref = O.precond_apply(P.ns, orc["colptr"], orc["rowind"], orc["val"], orc["diag"], rr)
+        np.testing.assert_allclose(z, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+        np.testing.assert_array_equal(z, ctx.precond_apply(f, rr))
+        x, info = ctx.pcg_solve(f, rr)
+        xo, io = P.pcg(orc, rr, tol=1e-8)
+        assert info["converged"] and abs(info["iterations"] - io["iterations"]) <= 1
+        x2, info2 = ctx.pcg_solve(f, rr)
+        np.testing.assert_array_equal(x, x2)
+        f.free()
+    finally:
+        ctx.close()
+
+
 def test_laplacian_without_ground():
     n, r, c, v, g = grid_laplacian((64, 64), seed=31)
     P = OracleProblem(n, r, c, v)
