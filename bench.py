@@ -129,6 +129,15 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.skip = 0
+
+    def mark(self):
+        """Samples taken before this call (priming, warm-up) are not reported."""
+        try:
+            with open(self.path) as f:
+                self.skip = sum(1 for _ in f)
+        except (OSError, TypeError):
+            self.skip = 0
 
     def start(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -151,7 +160,11 @@ class ClockSampler:
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         with open(self.path) as f:
-            for line in f:
+            lines = f.readlines()
+        if len(lines) > self.skip:
+            lines = lines[self.skip:]
+        if True:
+            for line in lines:
                 parts = [x.strip() for x in line.split(",")]
                 if len(parts) < 9:
                     continue
@@ -256,6 +269,11 @@ def run_b200(args, cfg, rank, world, local):
         fi = f.info()
         return ms, f, fi, info
 
+    # nvidia-smi samples the clocks from here on (its start-up stalls the
+    # driver briefly, so it starts before the untimed priming); only samples
+    # from the timed region are reported
+    clocks = ClockSampler(local)
+    clocks.start()
     # the first factorizations of a context allocate its device buffers
     # (slow, memory-mapping dependent); prime both forms before the warm-up
     for _ in range(2):
@@ -269,8 +287,8 @@ def run_b200(args, cfg, rank, world, local):
             flush.random_()
     barrier(world)
     torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
+    time.sleep(0.5)
+    clocks.mark()
     times = {"mixed": [], "fp64": []}
     last = {}
     launches = 0

@@ -18,6 +18,7 @@ struct Scratch {
     size_t cap = 0, used = 0;
     void* overflow[64] = {};
     int noverflow = 0;
+    size_t overflow_bytes = 0;  // requests the arena could not serve since the last reset
     cudaError_t reserve(size_t bytes) {
         if (bytes <= cap) return cudaSuccess;
         cudaFree(base);
@@ -27,10 +28,17 @@ struct Scratch {
         if (e == cudaSuccess) cap = bytes;
         return e;
     }
+    // Releases everything; after an overflow the arena grows to the peak use
+    // so that the next user of the same sizes allocates nothing.
     void reset() {
+        const size_t peak = used + overflow_bytes;
         used = 0;
         for (int i = 0; i < noverflow; ++i) cudaFree(overflow[i]);
         noverflow = 0;
+        if (overflow_bytes) {
+            overflow_bytes = 0;
+            reserve(peak + (peak >> 3));
+        }
     }
     template <typename T>
     cudaError_t get(T** p, int64_t n) {
@@ -42,7 +50,10 @@ struct Scratch {
         }
         if (noverflow == 64) return cudaErrorMemoryAllocation;
         cudaError_t e = cudaMalloc((void**)p, bytes);
-        if (e == cudaSuccess) overflow[noverflow++] = *p;
+        if (e == cudaSuccess) {
+            overflow[noverflow++] = *p;
+            overflow_bytes += bytes;
+        }
         return e;
     }
     void release() {
