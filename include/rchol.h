@@ -43,6 +43,8 @@ enum {
     RCHOL_STOP_ABS_R2 = 2   /* ||r||^2 <= tol, as custom_cg.hpp:214-223 */
 };
 
+enum { RCHOL_SPMV_AUTO = 0, RCHOL_SPMV_CSR = 1 };
+
 typedef struct rchol_ctx rchol_ctx;
 typedef struct rchol_factor rchol_factor_t;
 
@@ -66,6 +68,8 @@ typedef struct rchol_opts {
     int poll_ns;              /* back-off (ns) between polls in the triangular solves */
     int sched_epl;            /* triangular-solve schedule: matrix entries per lane (1..64) */
     int exact_bwd_levels;     /* order the backward solve by its true DAG levels (default 1) */
+    int spmv_layout;          /* one-RHS PCG SpMV: RCHOL_SPMV_AUTO (sliced-ELL copy of A
+                                 when its padding is at most 25%, else CSR) or RCHOL_SPMV_CSR */
 } rchol_opts;
 
 typedef struct rchol_factor_info {

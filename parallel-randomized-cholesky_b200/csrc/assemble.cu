@@ -849,29 +849,40 @@ cudaError_t max_i32(const int32_t* v, int64_t n, int32_t* out, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, cudaStream_t s) {
+cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, Scratch& sc, cudaStream_t s) {
     const int32_t nout = A.n - 1;
-    out.n = nout;
     int32_t* cnt = nullptr;
     void* tmp = nullptr;
-    RCHOL_TRY(dmalloc(&cnt, nout));
-    RCHOL_TRY(cudaMalloc(&tmp, scan_tmp_bytes(nout)));
-    RCHOL_TRY(dmalloc(&out.colptr, (int64_t)nout + 1));
+    RCHOL_TRY(sc.get(&cnt, nout));
+    RCHOL_TRY(sc.get((char**)&tmp, (int64_t)scan_tmp_bytes(nout)));
+    // colptr keeps its size for a matrix of the same order; rowind / val are
+    // sized for all of A's entries, so any matrix with as many fits
+    if (out.colptr && out.n != nout) {
+        cudaFree(out.colptr);
+        out.colptr = nullptr;
+    }
+    out.n = nout;
+    if (!out.colptr) RCHOL_TRY(dmalloc(&out.colptr, (int64_t)nout + 1));
+    if (out.cap < A.nnz) {
+        cudaFree(out.rowind);
+        cudaFree(out.val);
+        out.rowind = nullptr;
+        out.val = nullptr;
+        out.cap = 0;
+        RCHOL_TRY(dmalloc(&out.rowind, A.nnz));
+        RCHOL_TRY(dmalloc(&out.val, A.nnz));
+        out.cap = A.nnz;
+    }
     trim_count_kernel<<<grid_for((int64_t)nout * 32, 256), 256, 0, s>>>(nout, A.colptr, A.rowind, cnt);
     RCHOL_TRY(cudaGetLastError());
     RCHOL_TRY(exclusive_scan_i32_to_i32(cnt, out.colptr, nout, tmp, s));
     int32_t nnz = 0;
     RCHOL_TRY(cudaMemcpyAsync(&nnz, out.colptr + nout, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    RCHOL_TRY(cudaStreamSynchronize(s));
-    out.nnz = nnz;
-    RCHOL_TRY(dmalloc(&out.rowind, nnz));
-    RCHOL_TRY(dmalloc(&out.val, nnz));
     trim_scatter_kernel<<<grid_for((int64_t)nout * 32, 256), 256, 0, s>>>(nout, A.colptr, A.rowind, A.val,
                                                                           out.colptr, out.rowind, out.val);
     RCHOL_TRY(cudaGetLastError());
     RCHOL_TRY(cudaStreamSynchronize(s));
-    cudaFree(cnt);
-    cudaFree(tmp);
+    out.nnz = nnz;
     return cudaSuccess;
 }
 

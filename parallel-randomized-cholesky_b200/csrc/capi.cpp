@@ -28,6 +28,8 @@ struct rchol_ctx {
     std::string err;
     DevCsc A;        // as loaded (ground vertex included when trim)
     DevCsc At;       // the matrix of the solve (A itself when not trimmed)
+    rchol::DevSell sell;     // sliced-ELL copy of At for the one-RHS SpMV (built on first use)
+    bool sell_tried = false;
     bool trim = false;
     bool have = false;
     int32_t max_lower = 0;  // largest strict-lower column of A (bounds the first gathers)
@@ -201,6 +203,11 @@ rchol_status install_host_csc(rchol_ctx* ctx, const rchol::HostCsc& h, int trim_
     return rchol_set_csc(ctx, h.n, h.colptr.data(), h.rowind.data(), h.val.data(), 0, trim_ground);
 }
 
+void drop_sell(rchol_ctx* ctx) {
+    rchol::free_sell(ctx->sell);
+    ctx->sell_tried = false;
+}
+
 void drop_solver(rchol_ctx* ctx) {
     if (ctx->solver) rchol::pcg_destroy(ctx->solver);
     ctx->solver = nullptr;
@@ -249,6 +256,7 @@ extern "C" rchol_status rchol_opts_default(rchol_opts* o) {
     o->poll_ns = 0;
     o->sched_epl = 2;
     o->exact_bwd_levels = 1;
+    o->spmv_layout = RCHOL_SPMV_AUTO;
     return RCHOL_OK;
 }
 
@@ -265,6 +273,7 @@ static rchol_status check_opts(const rchol_opts* o, std::string& why) {
     else if (!(o->timeout_s > 0.0)) why = "timeout_s must be positive";
     else if (o->poll_ns < 0 || o->poll_ns > 100000) why = "poll_ns must be 0..100000";
     else if (o->sched_epl < 1 || o->sched_epl > 64) why = "sched_epl must be 1..64";
+    else if (o->spmv_layout != RCHOL_SPMV_AUTO && o->spmv_layout != RCHOL_SPMV_CSR) why = "spmv_layout";
     else return RCHOL_OK;
     return RCHOL_ERR_INVALID;
 }
@@ -294,6 +303,7 @@ extern "C" void rchol_destroy(rchol_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     drop_solver(ctx);
+    drop_sell(ctx);
     free_work(ctx->w);
     free_factor(ctx->spare);
     ctx->scratch.release();
@@ -363,13 +373,20 @@ extern "C" rchol_status rchol_set_csc(rchol_ctx* ctx, int n, const int* colptr, 
     // lower triangle keeps its size
     const bool same = ctx->have && ctx->A.n == n && ctx->A.nnz == nnz32 && ctx->trim == (trim_ground != 0);
     const int64_t old_lnnz = ctx->w.lnnz;
-    drop_solver(ctx);
+    // the PCG solver, the trimmed matrix and the sliced-ELL copy keep their
+    // buffers for a matrix of the same shape (refilled below / on first use)
+    ctx->sell_tried = false;
+    ctx->solver_f = nullptr;
     ctx->batch_off.clear();
-    if (ctx->trim) free_csc(ctx->At);
+    if (ctx->bsolver) drop_solver(ctx);
     DevCsc A;
     if (same) {
         A = ctx->A;
     } else {
+        drop_solver(ctx);
+        drop_sell(ctx);
+        if (ctx->trim) free_csc(ctx->At);
+        ctx->At = DevCsc();
         free_work(ctx->w);
         ctx->w_ready = false;
         free_csc(ctx->A);
@@ -387,7 +404,11 @@ extern "C" rchol_status rchol_set_csc(rchol_ctx* ctx, int n, const int* colptr, 
     ctx->A = A;
     ctx->trim = trim_ground != 0;
     if (ctx->trim) {
-        CK(rchol::trim_matrix(ctx->A, ctx->At, ctx->stream), "trim matrix");
+        rchol::DevCsc At = ctx->At;
+        const cudaError_t et = rchol::trim_matrix(ctx->A, At, ctx->scratch, ctx->stream);
+        ctx->scratch.reset();
+        ctx->At = At;
+        CK(et, "trim matrix");
     } else {
         ctx->At = ctx->A;
     }
@@ -775,7 +796,9 @@ extern "C" void rchol_factor_free(rchol_factor_t* f) {
     rchol_ctx* ctx = f->ctx;
     if (ctx) {
         cudaSetDevice(ctx->device);
-        if (ctx->solver_f == f || ctx->bsolver_f == f) drop_solver(ctx);
+        // the PCG solver stays for the next factor (rchol::pcg_rebind)
+        if (ctx->solver_f == f) ctx->solver_f = nullptr;
+        if (ctx->bsolver_f == f) drop_solver(ctx);
         if (!ctx->spare.lc_ptr && f->F.cap_n > 0) {  // keep the buffers for the next factor
             ctx->spare = f->F;
             f->F = DevFactor();
@@ -796,10 +819,30 @@ bool valid_k(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || 
 rchol_status get_solver(rchol_ctx* ctx, const rchol_factor_t* f, int k) {
     const rchol_opts& o = ctx->o;
     const int fp32 = o.precision == RCHOL_PREC_FP32_FACTOR;
-    if (ctx->solver && ctx->solver_f == f && ctx->solver_k == k && ctx->solver_fp32 == fp32 &&
-        ctx->solver_stop == o.stop_rule && ctx->solver_maxit == o.max_iter && ctx->solver_tol == o.tol &&
-        ctx->solver_poll == o.poll_ns)
-        return RCHOL_OK;
+    const bool want_sell = k == 1 && o.spmv_layout == RCHOL_SPMV_AUTO;
+    if (want_sell && !ctx->sell_tried) {
+        ctx->sell_tried = true;
+        cudaError_t e = rchol::build_sell(ctx->At, 1.25, ctx->sell, ctx->scratch, ctx->stream);
+        ctx->scratch.reset();
+        if (e == cudaErrorMemoryAllocation) {  // no room for the copy: CSR SpMV
+            cudaGetLastError();
+            drop_sell(ctx);
+            ctx->sell_tried = true;
+        } else if (e != cudaSuccess) {
+            return cuda_fail(ctx, e, "sliced-ELL copy");
+        }
+    }
+    const rchol::DevSell* sell = want_sell && ctx->sell.slots > 0 ? &ctx->sell : nullptr;
+    if (ctx->solver && ctx->solver_k == k && ctx->solver_fp32 == fp32 && ctx->solver_stop == o.stop_rule &&
+        ctx->solver_maxit == o.max_iter && ctx->solver_tol == o.tol && ctx->solver_poll == o.poll_ns) {
+        if (ctx->solver_f == f) return RCHOL_OK;
+        // another factor, or a new matrix of the same shape: keep the
+        // solver's vectors and graph
+        if (rchol::pcg_rebind(ctx->solver, ctx->At, sell, f->F) == cudaSuccess) {
+            ctx->solver_f = f;
+            return RCHOL_OK;
+        }
+    }
     drop_solver(ctx);
     rchol::SolveConfig cfg;
     cfg.k = k;
@@ -814,7 +857,7 @@ rchol_status get_solver(rchol_ctx* ctx, const rchol_factor_t* f, int k) {
     if (cfg.fp32_factor && !f->F.lr_val32)
         return fail(ctx, RCHOL_ERR_INVALID, "factor has no FP32 copy (factor with RCHOL_PREC_FP32_FACTOR)");
     cudaError_t e = cudaSuccess;
-    ctx->solver = rchol::pcg_create(ctx->At, f->F, cfg, ctx->device, ctx->stream, &e);
+    ctx->solver = rchol::pcg_create(ctx->At, f->F, cfg, ctx->device, ctx->stream, &e, sell);
     if (!ctx->solver) return cuda_fail(ctx, e, "create solver");
     ctx->solver_f = f;
     ctx->solver_k = k;

@@ -82,6 +82,21 @@ struct DevCsc {
     int32_t* colptr = nullptr;  // [n+1]
     int32_t* rowind = nullptr;  // [nnz]
     double* val = nullptr;      // [nnz]
+    int64_t cap = 0;            // entries allocated in rowind / val (trim_matrix output)
+};
+
+// Sliced-ELL copy of a DevCsc for the one-RHS SpMV (sell.cu): slice s of
+// 32 rows owns slots [sptr[s] * 32, sptr[s + 1] * 32), column-major (slot
+// (sptr[s] + k) * 32 + lane = entry k of row 32 s + lane; index -1 past the
+// row's end).
+struct DevSell {
+    int32_t n = 0;
+    int32_t nslices = 0;
+    int64_t slots = 0;          // 0: no copy (the CSR SpMV is used)
+    int64_t* sptr = nullptr;    // [nslices + 1], in units of 32 slots
+    int32_t* sidx = nullptr;    // [slots]
+    double* sval = nullptr;     // [slots]
+    int64_t cap_slices = 0, cap_slots = 0;  // allocated sizes, reused by the next build
 };
 
 // Working state of one factorization (all device pointers).
@@ -246,8 +261,9 @@ size_t factor_smem_bytes(int block, int smem_slab);
 // enough.
 cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp32, int epl, bool exact_bwd,
                             double timeout_s, Scratch& sc, DevFactor& f, cudaStream_t s);
-// Drop the last row/column of A (ground vertex) into a new DevCsc.
-cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, cudaStream_t s);
+// Drop the last row/column of A (ground vertex) into `out`, whose buffers
+// are reused when large enough (else reallocated).
+cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, Scratch& sc, cudaStream_t s);
 
 // Return the CUDA error of `x` from the enclosing function.
 #define RCHOL_TRY(x)                        \
@@ -309,8 +325,14 @@ struct SolveResult {
 // Solves A X = B for k columns stored row-major (n x k, ldx = k) in device
 // memory; X is overwritten.  `A` and `F` must have the same n.
 class PcgSolver;
+// `sell` (may be null) is a sliced-ELL copy of A used by the one-RHS SpMV.
 PcgSolver* pcg_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cfg, int device,
-                      cudaStream_t stream, cudaError_t* err);
+                      cudaStream_t stream, cudaError_t* err, const DevSell* sell = nullptr);
+// Points the solver at another matrix of the same size (with its sliced-ELL
+// copy, null for none) and another factor; its vectors, and its captured
+// iteration graph when the launch arguments come out equal, are kept.
+// Fails (cudaErrorInvalidValue) when the sizes or the SpMV form differ.
+cudaError_t pcg_rebind(PcgSolver* s, const DevCsc& A, const DevSell* sell, const DevFactor& F);
 cudaError_t pcg_solve(PcgSolver* s, const double* dB, double* dX, SolveResult* res);
 void pcg_destroy(PcgSolver* s);
 // Mean device time of spmv_update / fwd / bwd over `reps` iterations.
@@ -331,6 +353,12 @@ BatchSolver* batch_create(const DevCsc& A, const DevFactor& F, const SolveConfig
                           cudaStream_t stream, const int64_t* h_off, int nsys, cudaError_t* err);
 cudaError_t batch_solve(BatchSolver* s, const double* dB, double* dX, BatchResult* res);
 void batch_destroy(BatchSolver* s);
+
+// Builds `out` from A when the padded slot count is at most max_fill * nnz
+// (otherwise out.slots = 0).  The buffers of `out` are reused when large
+// enough.  Reads one scalar back (synchronizes `s`).
+cudaError_t build_sell(const DevCsc& A, double max_fill, DevSell& out, Scratch& sc, cudaStream_t s);
+void free_sell(DevSell& m);
 
 // Kernel-level entry points used by tests/bench (one operator application).
 cudaError_t spmv_f64(const DevCsc& A, const double* x, double* y, int k, cudaStream_t s);

@@ -69,6 +69,10 @@ struct SolveArgs {
     const int32_t* __restrict__ a_ptr;
     const int32_t* __restrict__ a_idx;
     const double* __restrict__ a_val;
+    // sliced-ELL copy of A (null when the CSR SpMV is used)
+    const int64_t* __restrict__ s_ptr;
+    const int32_t* __restrict__ s_idx;
+    const double* __restrict__ s_val;
     // factor
     // forward / backward solve layouts: position p of order_f / order_b
     // owns entries lr_ptr[p]..lr_ptr[p+1] / lc_ptr[p]..lc_ptr[p+1]
@@ -473,6 +477,85 @@ __global__ void __launch_bounds__(kBlock) spmv_update_tile_kernel(SolveArgs a) {
             a.y[i] = pending_value();
             acc += pi * qi;
         }
+    }
+    block_partials_lane<1>(acc, a.part + (size_t)blockIdx.x);
+    if (last_block(&a.sc->ticket[1])) {
+        sum_partials<1>(a.part, gridDim.x, a.sc->pq);
+        if (threadIdx.x == 0) {
+            const double pq = a.sc->pq[0];
+            a.sc->alpha[0] = (a.sc->active[0] && pq != 0.0) ? a.sc->rz[0] / pq : 0.0;
+            a.sc->ticket[1] = 0;
+        }
+    }
+}
+
+// One right-hand side on the sliced-ELL copy of A: a warp per slice of 32
+// rows, a lane per row.  A slice's columns are read 8 at a time (index and
+// value loads all in flight before the z gathers), streamed past L2 so that
+// the vectors stay resident.  Each lane adds its row's rounded products in
+// entry order, so q and p equal those of spmv_update_tile_kernel bit for
+// bit; the launch is one resident wave (the p.q partials follow its grid).
+constexpr int kSellCols = 8;
+
+__global__ void __launch_bounds__(kBlock) spmv_update_sell_kernel(SolveArgs a) {
+    if (ld_relaxed(&a.sc->done)) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t ntiles = ((int64_t)a.n + 31) / 32;
+    const double beta = a.sc->beta[0];
+    double acc = 0.0;
+    int64_t s0 = 0, s1 = 0;
+    if (gw < ntiles) {
+        s0 = a.s_ptr[gw];
+        s1 = a.s_ptr[gw + 1];
+    }
+    for (int64_t tile = gw; tile < ntiles; tile += nw) {
+        const int64_t i = tile * 32 + lane;
+        const bool row = i < a.n;
+        double qo = 0.0, po = 0.0, zi = 0.0;
+        if (row) {
+            qo = a.q[i];
+            po = a.p[i];
+            zi = a.z[i];
+        }
+        // the next slice's column range is in flight during this one
+        int64_t n0 = 0, n1 = 0;
+        if (tile + nw < ntiles) {
+            n0 = a.s_ptr[tile + nw];
+            n1 = a.s_ptr[tile + nw + 1];
+        }
+        double sum = 0.0;
+        for (int64_t k0 = s0; k0 < s1; k0 += kSellCols) {
+            const int m = (int)min((int64_t)kSellCols, s1 - k0);
+            int32_t idx[kSellCols];
+            double val[kSellCols], zv[kSellCols];
+#pragma unroll
+            for (int k = 0; k < kSellCols; ++k) {
+                idx[k] = -1;
+                if (k < m) {
+                    const int64_t slot = (k0 + k) * 32 + lane;
+                    idx[k] = __ldcs(a.s_idx + slot);
+                    val[k] = __ldcs(a.s_val + slot);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kSellCols; ++k)
+                if (idx[k] >= 0) zv[k] = a.z[idx[k]];
+#pragma unroll
+            for (int k = 0; k < kSellCols; ++k)
+                if (idx[k] >= 0) sum = __dadd_rn(sum, __dmul_rn(val[k], zv[k]));
+        }
+        if (row) {
+            const double qi = sum + beta * qo;
+            const double pi = zi + beta * po;
+            a.q[i] = qi;
+            a.p[i] = pi;
+            a.y[i] = pending_value();
+            acc += pi * qi;
+        }
+        s0 = n0;
+        s1 = n1;
     }
     block_partials_lane<1>(acc, a.part + (size_t)blockIdx.x);
     if (last_block(&a.sc->ticket[1])) {
@@ -1004,6 +1087,7 @@ class PcgSolver {
    public:
     DevCsc A;
     DevFactor F;
+    DevSell S;  // sliced-ELL copy of A (empty: CSR SpMV)
     SolveConfig cfg;
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -1016,8 +1100,7 @@ class PcgSolver {
     PcgScalars* sc_host = nullptr;  // pinned
     int* react = nullptr;          // device [kMaxK]
     cudaGraphExec_t graph_exec = nullptr;
-    const double* graph_b = nullptr;
-    double* graph_x = nullptr;
+    SolveArgs graph_args;  // the arguments the graph was captured with
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
     void *k_init = nullptr, *k_spmv = nullptr, *k_fwd = nullptr, *k_bwd = nullptr, *k_true = nullptr,
          *k_restart = nullptr;
@@ -1029,6 +1112,9 @@ class PcgSolver {
         a.a_ptr = A.colptr;
         a.a_idx = A.rowind;
         a.a_val = A.val;
+        a.s_ptr = S.sptr;
+        a.s_idx = S.sidx;
+        a.s_val = S.sval;
         // the solves read the schedule-ordered layouts (row ranges by position)
         a.lr_ptr = F.sf_ptr;
         a.lr_idx = F.sf_idx;
@@ -1126,7 +1212,7 @@ static bool bind_for_k(PcgSolver* s, int K) {
 }
 
 PcgSolver* pcg_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cfg, int device, cudaStream_t stream,
-                      cudaError_t* err) {
+                      cudaError_t* err, const DevSell* sell) {
     *err = cudaSuccess;
     if (A.n != F.n) {
         *err = cudaErrorInvalidValue;
@@ -1145,11 +1231,17 @@ PcgSolver* pcg_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cf
         *err = cudaErrorInvalidValue;
         return nullptr;
     }
+    bool sell_spmv = false;
+    if (cfg.k == 1 && sell && sell->slots > 0 && sell->n == A.n) {
+        s->S = *sell;
+        s->k_spmv = (void*)spmv_update_sell_kernel;
+        sell_spmv = true;
+    }
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     s->grid_fwd = resident_blocks(s->k_fwd, device);
     s->grid_bwd = resident_blocks(s->k_bwd, device);
-    s->grid_spmv = sms * 8;
+    s->grid_spmv = sell_spmv ? resident_blocks(s->k_spmv, device) : sms * 8;
     s->grid_vec = sms * 8;
     s->grid_max = std::max(std::max(s->grid_fwd, s->grid_bwd), std::max(s->grid_spmv, s->grid_vec));
     const size_t nv = (size_t)A.n * (size_t)cfg.k;
@@ -1175,6 +1267,17 @@ PcgSolver* pcg_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cf
     return s;
 }
 
+cudaError_t pcg_rebind(PcgSolver* s, const DevCsc& A, const DevSell* sell, const DevFactor& F) {
+    const bool want_sell = s->K == 1 && sell && sell->slots > 0 && sell->n == A.n;
+    const bool has_sell = s->k_spmv == (void*)spmv_update_sell_kernel;
+    if (A.n != s->A.n || F.n != A.n || want_sell != has_sell || (s->cfg.fp32_factor && !F.sf_val32))
+        return cudaErrorInvalidValue;
+    s->A = A;
+    s->S = want_sell ? *sell : DevSell();
+    s->F = F;
+    return cudaSuccess;
+}
+
 void pcg_destroy(PcgSolver* s) {
     if (!s) return;
     if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
@@ -1194,11 +1297,8 @@ void pcg_destroy(PcgSolver* s) {
 }
 
 static cudaError_t build_graph(PcgSolver* s, const double* b, double* x) {
-    if (s->graph_exec && s->graph_b == b && s->graph_x == x) return cudaSuccess;
-    if (s->graph_exec) {
-        cudaGraphExecDestroy(s->graph_exec);
-        s->graph_exec = nullptr;
-    }
+    const SolveArgs want = s->args(b, x);  // zero-filled, so padding compares equal
+    if (s->graph_exec && memcmp(&want, &s->graph_args, sizeof(want)) == 0) return cudaSuccess;
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
@@ -1207,12 +1307,23 @@ static cudaError_t build_graph(PcgSolver* s, const double* b, double* x) {
         if (e != cudaSuccess) break;
     }
     cudaError_t e2 = cudaStreamEndCapture(s->stream, &g);
-    if (e != cudaSuccess) return e;
-    if (e2 != cudaSuccess) return e2;
-    e = cudaGraphInstantiate(&s->graph_exec, g, 0);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return e != cudaSuccess ? e : e2;
+    }
+    // same launch sequence with new arguments (another factor or vectors):
+    // update the instantiated graph in place, else instantiate anew
+    if (s->graph_exec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(s->graph_exec, g, &info) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(s->graph_exec);
+            s->graph_exec = nullptr;
+        }
+    }
+    if (!s->graph_exec) e = cudaGraphInstantiate(&s->graph_exec, g, 0);
     cudaGraphDestroy(g);
-    s->graph_b = b;
-    s->graph_x = x;
+    if (e == cudaSuccess) memcpy(&s->graph_args, &want, sizeof(want));
     return e;
 }
 

@@ -23,6 +23,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "i/o error", 3: "CUDA error", 4: "c
           5: "timeout", 6: "not converged", 7: "no CUDA device", 8: "numeric", 9: "no matrix"}
 PREC_FP64, PREC_FP32_FACTOR = 0, 1
 STOP_RELRES, STOP_PRECOND, STOP_ABS_R2 = 0, 1, 2
+SPMV_AUTO, SPMV_CSR = 0, 1
 
 # every symbol include/rchol.h declares
 EXPORTS = [
@@ -48,7 +49,7 @@ class Opts(C.Structure):
                 ("pool_mult", C.c_double), ("max_iter", C.c_int), ("tol", C.c_double), ("stop_rule", C.c_int),
                 ("unroll", C.c_int), ("use_graph", C.c_int), ("device", C.c_int), ("timeout_s", C.c_double),
                 ("verbose", C.c_int), ("poll_ns", C.c_int),
-                ("sched_epl", C.c_int), ("exact_bwd_levels", C.c_int)]
+                ("sched_epl", C.c_int), ("exact_bwd_levels", C.c_int), ("spmv_layout", C.c_int)]
 
 
 class FactorInfo(C.Structure):

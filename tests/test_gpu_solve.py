@@ -253,3 +253,76 @@ def test_prepare_and_solve_drop_in(problem):
     xo, io = P.pcg(orc, b, tol=1e-7, max_iter=300, stop_rule=O.STOP_PRECOND)
     assert abs(info["iterations"] - io["iterations"]) <= 1
     np.testing.assert_allclose(x.cpu().numpy(), xo, rtol=0, atol=1e-6 * np.abs(xo).max())
+
+
+@pytest.mark.parametrize("dims", [(7, 9, 11), (16, 16, 24)])
+def test_sliced_ell_spmv_matches_csr(dims):
+    """The one-RHS PCG on the sliced-ELL copy of A (ragged last slice for
+    7x9x11) against the CSR SpMV: q and p agree bit for bit, only the p.q
+    partial sums follow another grid, so a few iterations agree to rounding
+    and the converged solves to the tolerance."""
+    n, r, c, v, g = grid_laplacian(dims, seed=41, excess_frac=0.05, wlo=1e-3, whi=1e3)
+    out = {}
+    for layout in (R.SPMV_AUTO, R.SPMV_CSR):
+        ctx = R.Context(seed=3, precision=R.PREC_FP32_FACTOR, tol=1e-8, spmv_layout=layout)
+        ctx.set_triplets(n, r, c, v, trim_ground=g)
+        f = ctx.factor()
+        ns = f.info().n
+        b = zero_sum_normal(ns, 5)
+        x, info = ctx.pcg_solve(f, b)
+        ctx.set_opts(max_iter=3)
+        x3, _ = ctx.pcg_solve(f, b)
+        out[layout] = (x, info, x3)
+        f.free()
+        ctx.close()
+    (xa, ia, a3), (xc, ic, c3) = out[R.SPMV_AUTO], out[R.SPMV_CSR]
+    assert ia["converged"] and ic["converged"]
+    assert abs(ia["iterations"] - ic["iterations"]) <= 1
+    np.testing.assert_allclose(a3, c3, rtol=1e-12, atol=1e-12 * np.abs(c3).max())
+    assert np.linalg.norm(xa - xc) <= 1e-6 * np.linalg.norm(xc)
+
+
+def test_solver_kept_across_factors():
+    """A context keeps its PCG solver (vectors and captured graph) when the
+    factor changes: solves alternating between two live factors, and one
+    after a factor is released and another made, equal those of a fresh
+    context bit for bit."""
+    n, r, c, v, g = grid_laplacian((14, 15, 13), seed=43, excess_frac=0.05, wlo=1e-2, whi=1e2)
+
+    def fresh():
+        ctx = R.Context(seed=6, precision=R.PREC_FP32_FACTOR, tol=1e-8)
+        ctx.set_triplets(n, r, c, v, trim_ground=g)
+        return ctx
+
+    ref_ctx = fresh()
+    f = ref_ctx.factor()
+    b = zero_sum_normal(f.info().n, 9)
+    x_ref, i_ref = ref_ctx.pcg_solve(f, b)
+    f.free()
+    ref_ctx.close()
+
+    ctx = fresh()
+    f1 = ctx.factor()
+    f2 = ctx.factor()  # other buffers, so the graph arguments change
+    for f in (f1, f2, f1):
+        x, info = ctx.pcg_solve(f, b)
+        assert info["iterations"] == i_ref["iterations"]
+        np.testing.assert_array_equal(x, x_ref)
+    f1.free()
+    f2.free()
+    f3 = ctx.factor()  # reuses a released factor's buffers
+    x, info = ctx.pcg_solve(f3, b)
+    np.testing.assert_array_equal(x, x_ref)
+    f3.free()
+
+    # a new matrix of the same shape (the solver, trimmed matrix and
+    # sliced-ELL copy keep their buffers) against a fresh context
+    v2 = v * 2.5
+    xs = []
+    for c_ in (ctx, fresh()):
+        c_.set_triplets(n, r, c, v2, trim_ground=g)
+        f = c_.factor()
+        xs.append(c_.pcg_solve(f, b)[0])
+        f.free()
+        c_.close()
+    np.testing.assert_array_equal(xs[0], xs[1])
