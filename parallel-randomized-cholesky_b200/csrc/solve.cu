@@ -308,6 +308,44 @@ __device__ __forceinline__ double row_dot(const int32_t* __restrict__ idx, const
     return sum;
 }
 
+// row_dot over the entries in descending order (e-1 down to s).  A row of
+// the L^T solve (column j of L, rows ascending) depends most recently on its
+// first entries, the rows eliminated right after j; walking it from the end
+// adds every entry that has landed while the last dependencies are still
+// being produced, so only the last few entries wait on the critical path.
+template <typename TV, int K = 1>
+__device__ __forceinline__ double row_dot_desc(const int32_t* __restrict__ idx, const TV* __restrict__ val,
+                                               int64_t s, int64_t e, const double* vec, unsigned long long t0,
+                                               unsigned long long limit, int* status, bool& ok, int poll_ns,
+                                               int c = 0) {
+    double sum = 0.0;
+    int64_t p = e;
+    for (; p - 4 >= s; p -= 4) {
+        const double* q0 = vec + (size_t)idx[p - 1] * K + c;
+        const double* q1 = vec + (size_t)idx[p - 2] * K + c;
+        const double* q2 = vec + (size_t)idx[p - 3] * K + c;
+        const double* q3 = vec + (size_t)idx[p - 4] * K + c;
+        const double l0 = to_d(val[p - 1]), l1 = to_d(val[p - 2]), l2 = to_d(val[p - 3]), l3 = to_d(val[p - 4]);
+        double v0 = ld_relaxed_f64(q0), v1 = ld_relaxed_f64(q1);
+        double v2 = ld_relaxed_f64(q2), v3 = ld_relaxed_f64(q3);
+        if (is_pending(v0)) v0 = wait_value(q0, t0, limit, status, ok, poll_ns);
+        if (is_pending(v1)) v1 = wait_value(q1, t0, limit, status, ok, poll_ns);
+        if (is_pending(v2)) v2 = wait_value(q2, t0, limit, status, ok, poll_ns);
+        if (is_pending(v3)) v3 = wait_value(q3, t0, limit, status, ok, poll_ns);
+        sum += l0 * v0;
+        sum += l1 * v1;
+        sum += l2 * v2;
+        sum += l3 * v3;
+    }
+    for (; p > s; --p) {
+        const double* q = vec + (size_t)idx[p - 1] * K + c;
+        double v = ld_relaxed_f64(q);
+        if (is_pending(v)) v = wait_value(q, t0, limit, status, ok, poll_ns);
+        sum += to_d(val[p - 1]) * v;
+    }
+    return sum;
+}
+
 // sum_p val[p] * vec[idx[p] * K + c] for final (non-pending) vectors
 template <int K = 1>
 __device__ __forceinline__ double row_dot_plain(const int32_t* __restrict__ idx, const double* __restrict__ val,
@@ -642,7 +680,7 @@ __global__ void __launch_bounds__(kBlock) bwd_kernel(SolveArgs a) {
         const size_t o = (size_t)j * K + c;
         double t = a.y[o];
         if (dj != 0.0) t = t / dj;
-        const double sum = row_dot<TV, K>(a.lc_idx, lv, s, e, a.z, t0, a.timeout_ns, &a.sc->status, ok,
+        const double sum = row_dot_desc<TV, K>(a.lc_idx, lv, s, e, a.z, t0, a.timeout_ns, &a.sc->status, ok,
                                           a.poll_ns, c);
         const double zj = t - sum;
         st_relaxed_f64(a.z + o, zj);
