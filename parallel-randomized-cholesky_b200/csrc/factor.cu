@@ -145,12 +145,29 @@ __device__ __forceinline__ int rv_digit(int32_t r, double v, int d) {
 // digit d of (value bits, row): bytes 0-3 of the row, then bytes 0-7 of the value bits
 __device__ __forceinline__ int vr_digit(int32_t r, double v, int d) { return rv_digit(r, v, (d + 8) % 12); }
 
+// Rounds of 32 entries whose loads a pass issues together (one memory
+// round trip per kRadixRounds * 32 entries).
+#ifndef RCHOL_RADIX_ROUNDS
+#define RCHOL_RADIX_ROUNDS 4
+#endif
+constexpr int kRadixRounds = RCHOL_RADIX_ROUNDS;
+
 // Counts of digit d over n entries into hist (256 ints, zeroed here).
 template <bool VR>
 __device__ void radix_count(const int32_t* row, const double* val, int n, int d, int* hist, int lane) {
     for (int i = lane; i < 256; i += kWarp) hist[i] = 0;
     __syncwarp();
-    for (int i = lane; i < n; i += kWarp) atomicAdd(&hist[VR ? vr_digit(row[i], val[i], d) : rv_digit(row[i], val[i], d)], 1);
+    for (int base = 0; base < n; base += kRadixRounds * kWarp) {
+        int dig[kRadixRounds];
+#pragma unroll
+        for (int q = 0; q < kRadixRounds; ++q) {
+            const int i = base + q * kWarp + lane;
+            dig[q] = i < n ? (VR ? vr_digit(row[i], val[i], d) : rv_digit(row[i], val[i], d)) : -1;
+        }
+#pragma unroll
+        for (int q = 0; q < kRadixRounds; ++q)
+            if (dig[q] >= 0) atomicAdd(&hist[dig[q]], 1);
+    }
     __syncwarp();
 }
 
@@ -184,57 +201,69 @@ __device__ bool radix_offsets(int* hist, int n, int lane) {
 }
 
 // One stable scatter pass of (row, val[, aux]) by digit d (hist holds the
-// offsets), counting digit d + 1 of the moved entries into hnext (zeroed here).
+// offsets), counting digit dnext (< 0: none) of the moved entries into hnext
+// (zeroed here).
 template <bool VR, bool AUX>
 __device__ void radix_scatter(const int32_t* row, const double* val, const long long* aux, int32_t* orow, double* oval,
-                              long long* oaux, int n, int d, int* hist, int* hnext, int lane) {
+                              long long* oaux, int n, int d, int dnext, int* hist, int* hnext, int lane) {
     const unsigned lt = (1u << lane) - 1u;
     for (int i = lane; i < 256; i += kWarp) hnext[i] = 0;
     __syncwarp();
-    for (int base = 0; base < n; base += kWarp) {
-        const int i = base + lane;
-        const bool valid = i < n;
-        int32_t r = 0;
-        double v = 0.0;
-        long long x = 0;
-        if (valid) {
-            r = row[i];
-            v = val[i];
-            if (AUX) x = aux[i];
+    for (int base = 0; base < n; base += kRadixRounds * kWarp) {
+        // the loads of kRadixRounds rounds first, then the rounds in order
+        int32_t r[kRadixRounds];
+        double v[kRadixRounds];
+        long long x[kRadixRounds];
+#pragma unroll
+        for (int q = 0; q < kRadixRounds; ++q) {
+            const int i = base + q * kWarp + lane;
+            r[q] = 0;
+            v[q] = 0.0;
+            x[q] = 0;
+            if (i < n) {
+                r[q] = row[i];
+                v[q] = val[i];
+                if (AUX) x[q] = aux[i];
+            }
         }
-        const int dig = valid ? (VR ? vr_digit(r, v, d) : rv_digit(r, v, d)) : 256;
-        const unsigned peers = __match_any_sync(kFull, dig);
-        const int rank = __popc(peers & lt);
-        const int at = valid ? hist[dig] + rank : 0;
-        __syncwarp();
-        if (valid && rank == 0) hist[dig] += __popc(peers);
-        if (valid && d + 1 < 12) atomicAdd(&hnext[VR ? vr_digit(r, v, d + 1) : rv_digit(r, v, d + 1)], 1);
-        __syncwarp();
-        if (valid) {
-            orow[at] = r;
-            oval[at] = v;
-            if (AUX) oaux[at] = x;
+#pragma unroll
+        for (int q = 0; q < kRadixRounds; ++q) {
+            const bool valid = base + q * kWarp + lane < n;
+            const int dig = valid ? (VR ? vr_digit(r[q], v[q], d) : rv_digit(r[q], v[q], d)) : 256;
+            const unsigned peers = __match_any_sync(kFull, dig);
+            const int rank = __popc(peers & lt);
+            const int at = valid ? hist[dig] + rank : 0;
+            __syncwarp();
+            if (valid && rank == 0) hist[dig] += __popc(peers);
+            if (valid && dnext >= 0) atomicAdd(&hnext[VR ? vr_digit(r[q], v[q], dnext) : rv_digit(r[q], v[q], dnext)], 1);
+            __syncwarp();
+            if (valid) {
+                orow[at] = r[q];
+                oval[at] = v[q];
+                if (AUX) oaux[at] = x[q];
+            }
         }
     }
     __syncwarp();
 }
 
-// LSD radix sort of n entries through the ping-pong buffers; the result is
-// copied back into (r_out, v_out[, x_out]) when it ends in the other buffer.
+// LSD radix sort of n entries by digits dlo..dhi-1 through the ping-pong
+// buffers; the result is copied back into (r_out, v_out[, x_out]) when it
+// ends in the other buffer.
 template <bool VR, bool AUX>
 __device__ void radix_sort(int32_t* r_out, double* v_out, long long* x_out, int32_t* r_tmp, double* v_tmp,
-                           long long* x_tmp, int n, int* hist, int* hnext, int lane) {
+                           long long* x_tmp, int n, int* hist, int* hnext, int lane, int dlo, int dhi) {
     int32_t *r0 = r_out, *r1 = r_tmp;
     double *v0 = v_out, *v1 = v_tmp;
     long long *x0 = x_out, *x1 = x_tmp;
-    radix_count<VR>(r0, v0, n, 0, hist, lane);
-    for (int d = 0; d < 12; ++d) {
+    radix_count<VR>(r0, v0, n, dlo, hist, lane);
+    for (int d = dlo; d < dhi; ++d) {
         if (radix_offsets(hist, n, lane)) {
             // nothing moves: count the next digit from the current buffer
-            if (d + 1 < 12) radix_count<VR>(r0, v0, n, d + 1, hist, lane);
+            if (d + 1 < dhi) radix_count<VR>(r0, v0, n, d + 1, hist, lane);
             continue;
         }
-        radix_scatter<VR, AUX>(r0, v0, x0, r1, v1, x1, n, d, hist, hnext, lane);
+        radix_scatter<VR, AUX>(r0, v0, x0, r1, v1, x1, n, d, d + 1 < dhi ? d + 1 : -1, hist, hnext, lane);
         int* th = hist; hist = hnext; hnext = th;
         int32_t* tr = r0; r0 = r1; r1 = tr;
         double* tv = v0; v0 = v1; v1 = tv;
@@ -252,12 +281,14 @@ __device__ void radix_sort(int32_t* r_out, double* v_out, long long* x_out, int3
 
 // (a_row, a_val) ascending by (row, value bits), result in a_*.
 __device__ __forceinline__ void radix_sort_rv(const Slab& s, int n, int* hist, int lane) {
-    radix_sort<false, false>(s.a_row, s.a_val, nullptr, s.t_row, s.t_val, nullptr, n, hist, hist + 256, lane);
+    radix_sort<false, false>(s.a_row, s.a_val, nullptr, s.t_row, s.t_val, nullptr, n, hist, hist + 256, lane, 0, 12);
 }
 
-// (b_val, b_row, b_aux) ascending by (value, row), result in b_*.
+// (b_val, b_row, b_aux) ascending by (value, row), result in b_*.  The input
+// is in ascending row order, so a stable sort on the value bytes alone gives
+// (value, row) order.
 __device__ __forceinline__ void radix_sort_vr(const Slab& s, int n, int* hist, int lane) {
-    radix_sort<true, true>(s.b_row, s.b_val, s.b_aux, s.t_row, s.t_val, s.t_aux, n, hist, hist + 256, lane);
+    radix_sort<true, true>(s.b_row, s.b_val, s.b_aux, s.t_row, s.t_val, s.t_aux, n, hist, hist + 256, lane, 4, 12);
 }
 
 struct FactorArgs {

@@ -111,6 +111,36 @@ def test_factor_large_gather_uses_shared_slab():
     assert info.max_gather >= 6000
 
 
+def _multi_hub_laplacian(leaves, hubs, seed):
+    """Leaves 0..leaves-1 each joined to every hub (numbered last): every
+    leaf elimination samples fills between hubs, so the hub columns gather
+    thousands of duplicates of a few rows."""
+    rng = np.random.default_rng(seed)
+    n = leaves + hubs
+    a = np.repeat(np.arange(leaves), hubs)
+    b = np.tile(np.arange(leaves, n), leaves)
+    w = np.exp(rng.uniform(np.log(1e-2), np.log(1e2), len(a)))
+    d = np.zeros(n)
+    np.add.at(d, a, w)
+    np.add.at(d, b, w)
+    rows = np.concatenate([a, b, np.arange(n)]).astype(np.int32)
+    cols = np.concatenate([b, a, np.arange(n)]).astype(np.int32)
+    vals = np.concatenate([-w, -w, d])
+    return n, rows, cols, vals
+
+
+@pytest.mark.parametrize("leaves,hubs", [(3000, 4), (1500, 12)])
+def test_factor_long_duplicate_runs_bitexact(leaves, hubs):
+    """Runs of one row longer than a lane orders in registers are ordered
+    by value and added by the whole warp; the factor equals the oracle's
+    bit for bit."""
+    n, r, c, v = _multi_hub_laplacian(leaves, hubs, seed=21)
+    P = OracleProblem(n, r, c, v, trim=False)
+    gpu, info = _gpu_factor(n, r, c, v, False, seed=22)
+    _compare(gpu, P.factor(seed=22))
+    assert info.max_gather > 1000
+
+
 @pytest.mark.parametrize("opts", [dict(), dict(bucket_cap=2, slab_entries=32)])
 def test_factor_power_law_bitexact(opts):
     """Power-law graph: hub columns take long overflow chunk chains and
