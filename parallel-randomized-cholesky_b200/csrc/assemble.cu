@@ -16,6 +16,9 @@ namespace rchol {
 namespace {
 
 constexpr int kSortSlab = 256;  // per-warp shared slab for the row sort (col, val)
+// Columns of at most kLaneSeg entries are handled by one lane each (32 in
+// flight per warp); longer ones by the whole warp, one at a time.
+constexpr int kLaneSeg = 32;
 
 __global__ void col_counts_kernel(int32_t nout, int32_t ground, const int32_t* __restrict__ pcnt,
                                   const int64_t* __restrict__ pstart, const int32_t* __restrict__ prow,
@@ -29,10 +32,11 @@ __global__ void col_counts_kernel(int32_t nout, int32_t ground, const int32_t* _
     }
 }
 
+// Lc from the pool (and, when col_of is given, the column of every entry).
 __global__ void scatter_cols_kernel(int32_t nout, const int64_t* __restrict__ lc_ptr,
                                     const int64_t* __restrict__ pstart, const int32_t* __restrict__ prow,
                                     const double* __restrict__ pval, int32_t* lc_idx, double* lc_val,
-                                    int32_t* row_cnt) {
+                                    int32_t* row_cnt, int32_t* col_of) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t k = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); k < nout; k += warps) {
@@ -41,8 +45,20 @@ __global__ void scatter_cols_kernel(int32_t nout, const int64_t* __restrict__ lc
             int32_t r = prow[src + t];
             lc_idx[o + t] = r;
             lc_val[o + t] = -pval[src + t];
+            if (col_of) col_of[o + t] = (int32_t)k;
             atomicAdd(row_cnt + r, 1);
         }
+    }
+}
+
+// Lr entry q is Lc entry order[q] (Lc's entries stably ordered by row).
+__global__ void gather_rows_kernel(int64_t nnz, const int32_t* __restrict__ order, const int32_t* __restrict__ col_of,
+                                   const double* __restrict__ lc_val, int32_t* lr_idx, double* lr_val) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nnz; q += stride) {
+        const int32_t p = order[q];
+        lr_idx[q] = col_of[p];
+        lr_val[q] = lc_val[p];
     }
 }
 
@@ -442,13 +458,28 @@ __global__ void to_f32_kernel(const double* __restrict__ in, float* out, int64_t
 __global__ void trim_count_kernel(int32_t nout, const int32_t* __restrict__ colptr, const int32_t* __restrict__ rowind,
                                   int32_t* cnt) {
     const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < nout; c += warps) {
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; c0 < nout; c0 += nw * 32) {
+        const int64_t c = c0 + lane;
+        const bool have = c < nout;
+        const int s = have ? colptr[c] : 0, e = have ? colptr[c + 1] : 0;
+        const bool wide = e - s > kLaneSeg;
         int k = 0;
-        for (int p = colptr[c] + lane; p < colptr[c + 1]; p += 32) k += rowind[p] < nout;
+        if (!wide) {
+#pragma unroll 4
+            for (int p = s; p < e; ++p) k += rowind[p] < nout;
+        }
+        for (unsigned lb = __ballot_sync(kFull, wide); lb; lb &= lb - 1u) {
+            const int sl = __ffs(lb) - 1;
+            const int ws = __shfl_sync(kFull, s, sl), we = __shfl_sync(kFull, e, sl);
+            int k2 = 0;
+#pragma unroll 8
+            for (int p = ws + lane; p < we; p += 32) k2 += rowind[p] < nout;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(kFull, k, o);
-        if (lane == 0) cnt[c] = k;
+            for (int o = 16; o > 0; o >>= 1) k2 += __shfl_xor_sync(kFull, k2, o);
+            if (lane == sl) k = k2;
+        }
+        if (have) cnt[c] = k;
     }
 }
 
@@ -456,19 +487,41 @@ __global__ void trim_scatter_kernel(int32_t nout, const int32_t* __restrict__ co
                                     const double* __restrict__ val, const int32_t* __restrict__ ocolptr,
                                     int32_t* orow, double* oval) {
     const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < nout; c += warps) {
-        int out = ocolptr[c];
-        for (int base = colptr[c]; base < colptr[c + 1]; base += 32) {
-            int p = base + lane;
-            bool take = p < colptr[c + 1] && rowind[p] < nout;
-            unsigned bal = __ballot_sync(kFull, take);
-            if (take) {
-                int q = out + __popc(bal & ((1u << lane) - 1u));
-                orow[q] = rowind[p];
-                oval[q] = val[p];
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; c0 < nout; c0 += nw * 32) {
+        const int64_t c = c0 + lane;
+        const bool have = c < nout;
+        const int s = have ? colptr[c] : 0, e = have ? colptr[c + 1] : 0;
+        const int o = have ? ocolptr[c] : 0;
+        const bool wide = e - s > kLaneSeg;
+        if (!wide) {
+            int out = o;
+#pragma unroll 4
+            for (int p = s; p < e; ++p) {
+                const int r = rowind[p];
+                if (r < nout) {
+                    orow[out] = r;
+                    oval[out] = val[p];
+                    ++out;
+                }
             }
-            out += __popc(bal);
+        }
+        for (unsigned lb = __ballot_sync(kFull, wide); lb; lb &= lb - 1u) {
+            const int sl = __ffs(lb) - 1;
+            const int ws = __shfl_sync(kFull, s, sl), we = __shfl_sync(kFull, e, sl);
+            int out = __shfl_sync(kFull, o, sl);
+#pragma unroll 8
+            for (int base = ws; base < we; base += 32) {
+                const int p = base + lane;
+                const bool take = p < we && rowind[p] < nout;
+                const unsigned bal = __ballot_sync(kFull, take);
+                if (take) {
+                    const int q = out + __popc(bal & ((1u << lane) - 1u));
+                    orow[q] = rowind[p];
+                    oval[q] = val[p];
+                }
+                out += __popc(bal);
+            }
         }
     }
 }
@@ -558,23 +611,40 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
         f.diag32 = nullptr;
     }
     f.cap_nnz = capz;
+    // Lr: a stable sort of Lc's entries (columns ascending) by row leaves
+    // every row's columns ascending, with no atomics and no row sort; the
+    // atomic transpose plus row sorts is kept for more than 2^31 - 1 entries
+    const bool by_sort = nnz <= (int64_t)INT_MAX;
+    int32_t *col_of = nullptr, *eorder = nullptr;
+    if (by_sort) {
+        RCHOL_TRY(sc.get(&col_of, nnz));
+        RCHOL_TRY(sc.get(&eorder, nnz));
+    }
     RCHOL_TRY(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (size_t)(nout > 0 ? nout : 1), s));
     scatter_cols_kernel<<<grid_for((int64_t)nout * 32, 256), 256, 0, s>>>(nout, f.lc_ptr, w.pstart, w.prow, w.pval,
-                                                                          f.lc_idx, f.lc_val, cnt);
+                                                                          f.lc_idx, f.lc_val, cnt, col_of);
     RCHOL_TRY(cudaGetLastError());
     RCHOL_TRY(exclusive_scan_i32_to_i64(cnt, f.lr_ptr, nout, tmp, s));
-    RCHOL_TRY(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (size_t)(nout > 0 ? nout : 1), s));
-    transpose_kernel<<<grid_for((int64_t)nout * 32, 256), 256, 0, s>>>(nout, f.lc_ptr, f.lc_idx, f.lc_val, f.lr_ptr,
-                                                                       cnt, f.lr_idx, f.lr_val);
-    RCHOL_TRY(cudaGetLastError());
+    if (by_sort) {
+        RCHOL_TRY(stable_key_order_carried(f.lc_idx, (int32_t)nnz, nout, eorder, sc, s));
+        gather_rows_kernel<<<grid_for(nnz, 256), 256, 0, s>>>(nnz, eorder, col_of, f.lc_val, f.lr_idx, f.lr_val);
+        RCHOL_TRY(cudaGetLastError());
+    } else {
+        RCHOL_TRY(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (size_t)(nout > 0 ? nout : 1), s));
+        transpose_kernel<<<grid_for((int64_t)nout * 32, 256), 256, 0, s>>>(nout, f.lc_ptr, f.lc_idx, f.lc_val,
+                                                                           f.lr_ptr, cnt, f.lr_idx, f.lr_val);
+        RCHOL_TRY(cudaGetLastError());
+    }
     // deterministic row order: warp sort for short rows, CTA sort for long ones
     const int sort_block = 256;
     const int sort_grid = 148 * 4;
     RCHOL_TRY(cudaMemsetAsync(dsc, 0, sizeof(int32_t) * 4, s));  // long rows, max row, max level
     max_kernel<<<grid_for(nout, 256), 256, 0, s>>>(cnt, nout, dsc + 1);
     max_kernel<<<grid_for(nout, 256), 256, 0, s>>>(w.level, nout, dsc + 2);
-    sort_rows_kernel<<<sort_grid, sort_block, 0, s>>>(nout, f.lr_ptr, f.lr_idx, f.lr_val, long_rows, dsc);
-    RCHOL_TRY(cudaGetLastError());
+    if (!by_sort) {
+        sort_rows_kernel<<<sort_grid, sort_block, 0, s>>>(nout, f.lr_ptr, f.lr_idx, f.lr_val, long_rows, dsc);
+        RCHOL_TRY(cudaGetLastError());
+    }
     int32_t hs[4] = {0, 0, 0, 0};
     RCHOL_TRY(cudaMemcpyAsync(hs, dsc, sizeof(hs), cudaMemcpyDeviceToHost, s));
     RCHOL_TRY(cudaStreamSynchronize(s));
@@ -582,7 +652,7 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
     double* gval = nullptr;
     int64_t gcap = 1;
     const int lgrid = hs[0] > 0 ? std::min(hs[0], 148 * 2) : 1;
-    if (hs[1] > kBlockSortCap) {
+    if (hs[0] > 0 && hs[1] > kBlockSortCap) {
         while (gcap < hs[1]) gcap <<= 1;
         RCHOL_TRY(sc.get(&gkey, (int64_t)lgrid * gcap));
         RCHOL_TRY(sc.get(&gval, (int64_t)lgrid * gcap));
@@ -873,13 +943,13 @@ cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, Scratch& sc, cudaStream_t 
         RCHOL_TRY(dmalloc(&out.val, A.nnz));
         out.cap = A.nnz;
     }
-    trim_count_kernel<<<grid_for((int64_t)nout * 32, 256), 256, 0, s>>>(nout, A.colptr, A.rowind, cnt);
+    trim_count_kernel<<<grid_for(nout, 256), 256, 0, s>>>(nout, A.colptr, A.rowind, cnt);
     RCHOL_TRY(cudaGetLastError());
     RCHOL_TRY(exclusive_scan_i32_to_i32(cnt, out.colptr, nout, tmp, s));
     int32_t nnz = 0;
     RCHOL_TRY(cudaMemcpyAsync(&nnz, out.colptr + nout, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    trim_scatter_kernel<<<grid_for((int64_t)nout * 32, 256), 256, 0, s>>>(nout, A.colptr, A.rowind, A.val,
-                                                                          out.colptr, out.rowind, out.val);
+    trim_scatter_kernel<<<grid_for(nout, 256), 256, 0, s>>>(nout, A.colptr, A.rowind, A.val, out.colptr,
+                                                            out.rowind, out.val);
     RCHOL_TRY(cudaGetLastError());
     RCHOL_TRY(cudaStreamSynchronize(s));
     out.nnz = nnz;

@@ -952,23 +952,54 @@ __global__ void prefill_bucket_kernel(int32_t n, int c0, const int32_t* __restri
 
 // Per column: entries below the diagonal (lower_cnt) and above it (dep,
 // count_minimum_dependencies, pre_process.hpp:474-496).  One warp/column.
+// Columns with at most kLaneCol entries are handled by one lane each (32
+// columns per warp in flight); longer ones by the whole warp, one at a time.
+constexpr int kLaneCol = 32;
+
 __global__ void count_lower_kernel(int32_t n, const int32_t* __restrict__ colptr,
                                    const int32_t* __restrict__ rowind, int32_t* lower_cnt, int32_t* dep) {
     const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < n; c += warps) {
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; c0 < n; c0 += nw * 32) {
+        const int64_t c = c0 + lane;
+        const bool have = c < n;
+        const int s = have ? colptr[c] : 0, e = have ? colptr[c + 1] : 0;
+        const bool wide = e - s > kLaneCol;
         int lo = 0, up = 0;
-        for (int p = colptr[c] + lane; p < colptr[c + 1]; p += 32) {
-            int r = rowind[p];
-            lo += r > c;
-            up += r < c;
+        if (!wide) {
+#pragma unroll 4
+            for (int p = s; p < e; ++p) {
+                const int r = rowind[p];
+                lo += r > c;
+                up += r < c;
+            }
         }
+        for (unsigned lb = __ballot_sync(kFull, wide); lb; lb &= lb - 1u) {
+            const int src = __ffs(lb) - 1;
+            const int cs = __shfl_sync(kFull, s, src), ce = __shfl_sync(kFull, e, src);
+            const int64_t cc = c0 + src;
+            int l2 = 0, u2 = 0;
+            for (int p0 = cs + lane; p0 < ce; p0 += 8 * 32) {
+                int r[8];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            lo += __shfl_xor_sync(kFull, lo, o);
-            up += __shfl_xor_sync(kFull, up, o);
+                for (int q = 0; q < 8; ++q) r[q] = p0 + 32 * q < ce ? rowind[p0 + 32 * q] : (int)cc;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    l2 += r[q] > cc;
+                    u2 += r[q] < cc;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                l2 += __shfl_xor_sync(kFull, l2, o);
+                u2 += __shfl_xor_sync(kFull, u2, o);
+            }
+            if (lane == src) {
+                lo = l2;
+                up = u2;
+            }
         }
-        if (lane == 0) {
+        if (have) {
             lower_cnt[c] = lo;
             if (dep) dep[c] = up;
         }
@@ -981,19 +1012,50 @@ __global__ void scatter_lower_kernel(int32_t n, const int32_t* __restrict__ colp
                                      const int32_t* __restrict__ rowind, const double* __restrict__ val,
                                      const int32_t* __restrict__ lcolptr, int32_t* lrow, double* lval) {
     const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < n; c += warps) {
-        int out = lcolptr[c];
-        for (int base = colptr[c]; base < colptr[c + 1]; base += 32) {
-            int p = base + lane;
-            bool take = p < colptr[c + 1] && rowind[p] > c;
-            unsigned bal = __ballot_sync(kFull, take);
-            if (take) {
-                int o = out + __popc(bal & ((1u << lane) - 1u));
-                lrow[o] = rowind[p];
-                lval[o] = fabs(val[p]);
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t c0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; c0 < n; c0 += nw * 32) {
+        const int64_t c = c0 + lane;
+        const bool have = c < n;
+        const int s = have ? colptr[c] : 0, e = have ? colptr[c + 1] : 0;
+        const int o = have ? lcolptr[c] : 0;
+        const int cnt = have ? lcolptr[c + 1] - o : 0;
+        // nothing to take (the ground column) or everything (a plain copy)
+        const bool wide = e - s > kLaneCol && cnt > 0;
+        if (!wide && cnt > 0) {
+            int out = o;
+#pragma unroll 4
+            for (int p = s; p < e; ++p) {
+                const int r = rowind[p];
+                if (r > c) {
+                    lrow[out] = r;
+                    lval[out] = fabs(val[p]);
+                    ++out;
+                }
             }
-            out += __popc(bal);
+        }
+        for (unsigned lb = __ballot_sync(kFull, wide); lb; lb &= lb - 1u) {
+            const int src = __ffs(lb) - 1;
+            const int cs = __shfl_sync(kFull, s, src), ce = __shfl_sync(kFull, e, src);
+            const int64_t cc = c0 + src;
+            int out = __shfl_sync(kFull, o, src);
+            if (__shfl_sync(kFull, cnt, src) == ce - cs) {
+                for (int p = cs + lane; p < ce; p += 32) {
+                    lrow[out + p - cs] = rowind[p];
+                    lval[out + p - cs] = fabs(val[p]);
+                }
+                continue;
+            }
+            for (int base = cs; base < ce; base += 32) {
+                const int p = base + lane;
+                const bool take = p < ce && rowind[p] > cc;
+                const unsigned bal = __ballot_sync(kFull, take);
+                if (take) {
+                    const int at = out + __popc(bal & ((1u << lane) - 1u));
+                    lrow[at] = rowind[p];
+                    lval[at] = fabs(val[p]);
+                }
+                out += __popc(bal);
+            }
         }
     }
 }
@@ -1025,21 +1087,19 @@ int grid_for(int64_t work, int block) {
 // ---------------------------------------------------------------------------
 
 cudaError_t launch_count_lower(const DevCsc& A, int32_t* lower_cnt, cudaStream_t s) {
-    count_lower_kernel<<<grid_for((int64_t)A.n * 32, 256), 256, 0, s>>>(A.n, A.colptr, A.rowind, lower_cnt,
-                                                                         nullptr);
+    count_lower_kernel<<<grid_for(A.n, 256), 256, 0, s>>>(A.n, A.colptr, A.rowind, lower_cnt, nullptr);
     return cudaGetLastError();
 }
 
 cudaError_t launch_lower_and_deps(const DevCsc& A, FactorWork& w, cudaStream_t s) {
     // lower counts go to w.pcnt (scratch), dependency counts to w.dep
-    count_lower_kernel<<<grid_for((int64_t)A.n * 32, 256), 256, 0, s>>>(A.n, A.colptr, A.rowind, w.pcnt,
-                                                                         w.dep);
+    count_lower_kernel<<<grid_for(A.n, 256), 256, 0, s>>>(A.n, A.colptr, A.rowind, w.pcnt, w.dep);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     e = exclusive_scan_i32_to_i32(w.pcnt, w.lcolptr, A.n, w.scan_tmp, s);
     if (e != cudaSuccess) return e;
-    scatter_lower_kernel<<<grid_for((int64_t)A.n * 32, 256), 256, 0, s>>>(A.n, A.colptr, A.rowind, A.val,
-                                                                           w.lcolptr, w.lrow, w.lval);
+    scatter_lower_kernel<<<grid_for(A.n, 256), 256, 0, s>>>(A.n, A.colptr, A.rowind, A.val, w.lcolptr, w.lrow,
+                                                             w.lval);
     return cudaGetLastError();
 }
 

@@ -284,6 +284,10 @@ cudaError_t max_i32(const int32_t* v, int64_t n, int32_t* out, cudaStream_t s);
 // equal keys keep ascending index order (bucket_sort.cu).
 cudaError_t stable_key_order(const int32_t* key, int32_t n, int32_t nkeys, int32_t* order, Scratch& sc,
                              cudaStream_t s);
+// The same order with the keys moved along with the items in every pass
+// (sequential key reads; two extra key buffers of scratch): for large n.
+cudaError_t stable_key_order_carried(const int32_t* key, int32_t n, int32_t nkeys, int32_t* order, Scratch& sc,
+                                     cudaStream_t s);
 
 // ---- scans (scan.cu) -------------------------------------------------------
 // out[0] = 0, out[i+1] = sum(in[0..i]); out has n+1 entries.  Uses `tmp`
