@@ -389,7 +389,8 @@ def run_b200(args, cfg, rank, world, local):
                      "all_kernels_GBps": {k: round(ab[k] / (per_launch[k] / 1000.0) / 1e9, 1) for k in ab}},
         "e2e": {"value": round(e2e_s, 6), "unit": "s",
                 "h2d_bytes_per_step": int(W["colptr"].nbytes + W["rowind"].nbytes + W["val"].nbytes + b.nbytes),
-                "d2h_bytes_per_step": int(ns * 8)},
+                "d2h_bytes_per_step": int(ns * 8), "statistic": "median of 5 calls",
+                "calls_ms": [round(x, 2) for x in e2e_ms]},
         "rhs32": {"solve_ms": round(si32k["ms_total"], 3), "iterations": si32k["iterations"],
                   "relres_true": si32k["relres_true"], "per_rhs_throughput_vs_single": round(per_rhs_speedup, 2)},
         "gpu_launches": int(launches),
