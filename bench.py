@@ -74,6 +74,7 @@ def parse():
                    help="one factorization + one PCG solve of the config (mixed form), for profilers")
     p.add_argument("--size", type=int, default=0, help="grid side override for --profile-run (small ncu cases)")
     p.add_argument("--max-iter", type=int, default=0, help="PCG iteration cap for --profile-run")
+    p.add_argument("--rhs", type=int, default=1, help="right-hand sides of the --profile-run solve")
     return p.parse_args()
 
 
@@ -642,7 +643,7 @@ def profile_run(args, cfg):
     ncu summaries under profiles/ were captured on."""
     import rchol_b200 as R
     cfg = dict(cfg)
-    if args.size:
+    if args.size and cfg["kind"].startswith("grid"):
         cfg["dims"] = [args.size] * len(cfg["dims"])
     W = build_workload(cfg)
     n, ground = W["n"], W["ground"]
@@ -654,10 +655,10 @@ def profile_run(args, cfg):
     ctx.set_csc(n, W["colptr"], W["rowind"], W["val"], trim_ground=ground)
     f = ctx.factor()
     fi = f.info()
-    b = np.random.default_rng(0).standard_normal(ns)
-    b -= b.mean()
+    b = np.random.default_rng(0).standard_normal((ns, args.rhs) if args.rhs > 1 else ns)
+    b -= b.mean(axis=0)
     x, si = ctx.pcg_solve(f, b)
-    print(json.dumps({"profile_run": args.config, "dims": cfg["dims"], "n": ns, "nnz_L": fi.nnz_strict,
+    print(json.dumps({"profile_run": args.config, "dims": cfg["dims"], "rhs": args.rhs, "n": ns, "nnz_L": fi.nnz_strict,
                       "factor_ms": fi.ms_factor, "assemble_ms": fi.ms_assemble, "solve_ms": si["ms_total"],
                       "iterations": si["iterations"], "relres": si["relres_true"]}))
     f.free()
@@ -670,14 +671,14 @@ def main():
         dist_init(1)
         run_c4(args)
         return
+    if args.profile_run:
+        profile_run(args, CONFIGS[args.config] if args.config in CONFIGS else SECONDARY[args.config])
+        return
     if args.config in SECONDARY:
         dist_init(1)
         run_secondary(args, SECONDARY[args.config], args.config)
         return
     cfg = CONFIGS[args.config]
-    if args.profile_run:
-        profile_run(args, cfg)
-        return
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         if rank != 0:
