@@ -701,31 +701,26 @@ __global__ void __launch_bounds__(kBlock) bwd_kernel(SolveArgs a) {
 
 
 // ---------------------------------------------------------------------------
-// K = 1 solves driven by the level-ordered task lists: a task is one long
-// row (the warp's lanes stride its entries) or a pack of up to 32 short rows
-// of one level (one row per lane, entries loaded four at a time so that the
-// row's gathers are in flight together).  Warps walk the task list in
-// order, so every dependency sits in an earlier task.
+// K = 1 solves over task slabs.  A task is one row group of G = 2^cls lanes
+// per row (up to 32 / G rows of one level and lane class per warp; long
+// rows take the whole warp, rows longer than 1024 entries are split into
+// part tasks).  A warp takes the tasks warp, warp + nwarps, ... in schedule
+// order, so every dependency sits in an earlier task.  While it waits on
+// the dependencies of one task, the slab entries and row indices of its
+// next task are already in flight, so a task's critical path after its last
+// dependency lands is one poll round trip, a short dot product and one store.
 // ---------------------------------------------------------------------------
 
-// Strided partial dot product of one lane of a G-lane row group: entries
-// s+gl, s+gl+G, ... fetched four at a time.
-// ---- K = 1 solves over task slabs ------------------------------------------
-// A warp takes the tasks warp, warp + nwarps, ... in schedule order.  While
-// it waits on the dependencies of one task, the slab entries, row indices
-// and row data of its next task are already in flight, so a task's critical
-// path after its last dependency lands is one poll round trip, a short
-// dot product and one store.
-
 constexpr int kPackM = 4;  // slab slots per lane held in registers
+// gate rounds per re-read of the other pending slots (0: none)
 #ifndef RCHOL_TRICKLE
 #define RCHOL_TRICKLE 2
 #endif
 constexpr unsigned kTrickle = RCHOL_TRICKLE;
-// 3 CTAs of 256 threads per SM (85 registers, no spills in the poll loops)
+// 3 CTAs of 256 threads per SM (80 registers, no spills in the poll loops)
 #ifndef RCHOL_PACK_MINB
 #define RCHOL_PACK_MINB 3
-#endif  // gate rounds per re-read of the other pending slots (0: none)
+#endif
 
 template <typename TV>
 struct PackLane {
