@@ -174,9 +174,14 @@ rchol_status lower_nnz(rchol_ctx* ctx, int64_t* out) {
     int32_t* cnt = nullptr;
     int64_t* ptr = nullptr;
     void* tmp = nullptr;
-    CK(dalloc(&cnt, n), "alloc counts");
-    CK(dalloc(&ptr, (int64_t)n + 1), "alloc ptr");
-    CK(cudaMalloc(&tmp, rchol::scan_tmp_bytes(n)), "alloc scan");
+    // temporaries from the context's scratch arena (released on return)
+    struct Release {
+        rchol::Scratch& sc;
+        ~Release() { sc.reset(); }
+    } release{ctx->scratch};
+    CK(ctx->scratch.get(&cnt, n), "alloc counts");
+    CK(ctx->scratch.get(&ptr, (int64_t)n + 1), "alloc ptr");
+    CK(ctx->scratch.get((char**)&tmp, (int64_t)rchol::scan_tmp_bytes(n)), "alloc scan");
     CK(rchol::launch_count_lower(ctx->A, cnt, ctx->stream), "count lower");
     CK(rchol::exclusive_scan_i32_to_i64(cnt, ptr, n, tmp, ctx->stream), "scan lower");
     CK(cudaMemcpyAsync(out, ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream), "copy lnnz");
@@ -189,9 +194,6 @@ rchol_status lower_nnz(rchol_ctx* ctx, int64_t* out) {
     CK(cudaMemcpyAsync(&hmax, dmax, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream), "copy max");
     CK(cudaStreamSynchronize(ctx->stream), "sync max");
     ctx->max_lower = hmax;
-    cudaFree(cnt);
-    cudaFree(ptr);
-    cudaFree(tmp);
     return RCHOL_OK;
 }
 
