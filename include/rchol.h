@@ -66,7 +66,8 @@ typedef struct rchol_opts {
     double timeout_s;         /* bound on every device-side wait */
     int verbose;              /* print phase timings (the reference's stdout) */
     int poll_ns;              /* back-off (ns) between polls in the triangular solves */
-    int sched_epl;            /* triangular-solve schedule: matrix entries per lane (1..64) */
+    int sched_epl;            /* triangular-solve schedule: matrix entries per lane (1..64), or 0:
+                                 automatic (3 when every row of L has at most 1024 entries, else 2) */
     int exact_bwd_levels;     /* order the backward solve by its true DAG levels (default 1) */
     int spmv_layout;          /* one-RHS PCG SpMV: RCHOL_SPMV_AUTO (sliced-ELL copy of A
                                  when its padding is at most 25%, else CSR) or RCHOL_SPMV_CSR */

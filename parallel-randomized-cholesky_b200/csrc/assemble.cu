@@ -665,6 +665,7 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
         RCHOL_TRY(cudaGetLastError());
     }
     f.depth = hs[2] + 1;
+    if (epl <= 0) epl = auto_sched_epl(hs[1]);
     RCHOL_TRY(cudaMemcpyAsync(f.diag, w.diag, sizeof(double) * (size_t)nout, cudaMemcpyDeviceToDevice, s));
     if (make_fp32) {
         to_f32_kernel<<<grid_for(nnz, 256), 256, 0, s>>>(f.lc_val, f.lc_val32, nnz);

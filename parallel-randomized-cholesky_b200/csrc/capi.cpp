@@ -256,7 +256,7 @@ extern "C" rchol_status rchol_opts_default(rchol_opts* o) {
     o->timeout_s = 30.0;
     o->verbose = 0;
     o->poll_ns = 0;
-    o->sched_epl = 2;
+    o->sched_epl = 0;
     o->exact_bwd_levels = 1;
     o->spmv_layout = RCHOL_SPMV_AUTO;
     return RCHOL_OK;
@@ -274,7 +274,7 @@ static rchol_status check_opts(const rchol_opts* o, std::string& why) {
     else if (o->unroll < 1 || o->unroll > 64) why = "unroll must be 1..64";
     else if (!(o->timeout_s > 0.0)) why = "timeout_s must be positive";
     else if (o->poll_ns < 0 || o->poll_ns > 100000) why = "poll_ns must be 0..100000";
-    else if (o->sched_epl < 1 || o->sched_epl > 64) why = "sched_epl must be 1..64";
+    else if (o->sched_epl < 0 || o->sched_epl > 64) why = "sched_epl must be 0 (automatic) or 1..64";
     else if (o->spmv_layout != RCHOL_SPMV_AUTO && o->spmv_layout != RCHOL_SPMV_CSR) why = "spmv_layout";
     else return RCHOL_OK;
     return RCHOL_ERR_INVALID;
@@ -692,7 +692,13 @@ rchol_status factor_from_host_csc(rchol_ctx* ctx, int32_t n, const std::vector<i
     if (e == cudaSuccess) e = up(&dlev, lev);
     if (e == cudaSuccess) {
         ctx->scratch.reset();
-        e = rchol::build_solve_schedule(F, dlev, ctx->o.sched_epl, ctx->o.exact_bwd_levels != 0, ctx->o.timeout_s,
+        int epl = ctx->o.sched_epl;
+        if (epl <= 0) {
+            int64_t longest = 0;
+            for (int32_t i = 0; i < n; ++i) longest = std::max(longest, rp[(size_t)i + 1] - rp[(size_t)i]);
+            epl = rchol::auto_sched_epl(longest);
+        }
+        e = rchol::build_solve_schedule(F, dlev, epl, ctx->o.exact_bwd_levels != 0, ctx->o.timeout_s,
                                         ctx->scratch, ctx->stream);
         ctx->scratch.reset();
     }
