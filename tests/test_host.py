@@ -42,6 +42,30 @@ def test_create_without_device_fails_loudly():
     assert e.value.status == 7  # RCHOL_ERR_NO_DEVICE: no CPU fallback
 
 
+def test_option_defaults_and_validation():
+    """rchol_create checks the options before it looks for a device: bad
+    values are RCHOL_ERR_INVALID (1) on any machine, good ones get as far as
+    the device check (RCHOL_ERR_NO_DEVICE, 7, without a GPU)."""
+    import torch
+    o = R.default_opts()
+    assert o.sched_epl == 0  # automatic schedule width
+    assert o.spmv_layout == R.SPMV_AUTO
+    lib = R.lib()
+    good = 0 if torch.cuda.is_available() else 7
+
+    def create(**kw):
+        h = ctypes.c_void_p()
+        st = lib.rchol_create(ctypes.byref(h), ctypes.byref(R.default_opts(**kw)))
+        if st == 0:
+            lib.rchol_destroy(h)
+        return st
+
+    for kw in (dict(sched_epl=0), dict(sched_epl=3), dict(sched_epl=64), dict(spmv_layout=R.SPMV_CSR)):
+        assert create(**kw) == good, kw
+    for kw in (dict(sched_epl=-1), dict(sched_epl=65), dict(spmv_layout=2), dict(spmv_layout=-1)):
+        assert create(**kw) == 1, kw
+
+
 @pytest.mark.parametrize("case", ["grid2d", "grid3d_sddm", "with_duplicates", "no_diagonal", "positive_offdiag"])
 def test_preprocessing_matches_oracle(case):
     rng = np.random.default_rng(1)
