@@ -20,6 +20,7 @@ MKL dependency is absent here, so the oracle's FP64 port of
 experiment/custom_cg.hpp stands in for it.
 """
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -189,14 +190,41 @@ class ClockSampler:
 # workload
 # ---------------------------------------------------------------------------
 
-def build_workload(cfg):
-    import rchol_b200 as R
-    n, r, c, v, g = R.generate(cfg["kind"], cfg["dims"], wlo=cfg["wlo"], whi=cfg["whi"],
-                               log_weights=cfg["log_weights"], aniso_z=cfg.get("aniso_z", 1.0),
-                               excess_frac=cfg["excess_frac"], excess_lo=cfg["excess_lo"],
-                               excess_hi=cfg["excess_hi"], seed=cfg["seed"])
-    colptr, rowind, val = R.csc_from_triplets(n, r, c, v)
-    return dict(n=n, colptr=colptr, rowind=rowind, val=val, ground=g, triplets=(r, c, v))
+def build_workload(cfg, product=True):
+    """The configuration's matrix as host CSC.  product=False builds it with the
+    oracle's copy of the generator and preprocessing (oracle/gen_inputs.c,
+    oracle/rchol_oracle.c), so that the reference's CPU legs never load the
+    product library; both give bit-identical arrays (input_sha256 shows it)."""
+    gen = dict(wlo=cfg["wlo"], whi=cfg["whi"], log_weights=cfg["log_weights"], aniso_z=cfg.get("aniso_z", 1.0),
+               excess_frac=cfg["excess_frac"], excess_lo=cfg["excess_lo"], excess_hi=cfg["excess_hi"], seed=cfg["seed"])
+    if product:
+        import rchol_b200 as R
+        n, r, c, v, g = R.generate(cfg["kind"], cfg["dims"], **gen)
+        colptr, rowind, val = R.csc_from_triplets(n, r, c, v)
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as O
+        n, r, c, v, g = O.generate_grid(cfg["kind"], cfg["dims"], **gen)
+        colptr, rowind, val = O.triplets_to_csc(n, r, c, v)
+    h = hashlib.sha256()
+    for a in (colptr, rowind, val):
+        h.update(np.ascontiguousarray(a).tobytes())
+    ns = n - 1 if g else n
+    nnz_solve = int(colptr[-1]) - (int(np.diff(colptr)[-1]) * 2 - 1 if g else 0)
+    return dict(n=n, ns=ns, nnz_solve=nnz_solve, colptr=colptr, rowind=rowind, val=val, ground=g,
+                triplets=(r, c, v), sha=h.hexdigest()[:16])
+
+
+def workload_config(cfg, W):
+    """The `config` object both arms print (identical for the same input)."""
+    return {"workload": cfg["workload"], "n": W["ns"], "nnz_A": W["nnz_solve"], "tol": cfg["tol"], "rhs": 1,
+            "input_sha256": W["sha"]}
+
+
+def bench_rhs(ns, rank=0):
+    """The timed right-hand side: zero-mean N(0,1)."""
+    b = np.random.default_rng(1000 + rank).standard_normal(ns)
+    return b - b.mean()
 
 
 def algorithmic_bytes(n, nnz_a, nnz_l, lnnz_a, fills, k, sv):
@@ -249,11 +277,9 @@ def run_b200(args, cfg, rank, world, local):
         c = R.Context(device=local, seed=1, precision=prec, tol=cfg["tol"], stop_rule=R.STOP_RELRES)
         c.set_csc(n, W["colptr"], W["rowind"], W["val"], trim_ground=ground)
         ctx[form] = c
-    rng = np.random.default_rng(1000 + rank)
-    b = rng.standard_normal(ns)
-    b -= b.mean()
+    b = bench_rhs(ns, rank)
     b_dev = torch.as_tensor(b, device=dev)
-    x_dev = torch.zeros(ns, dtype=torch.float64, device=dev)
+    x_dev = {form: torch.zeros(ns, dtype=torch.float64, device=dev) for form in ctx}
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def step(form):
@@ -263,7 +289,7 @@ def run_b200(args, cfg, rank, world, local):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
         f = c.factor()
-        info = c.pcg_solve_device(f, 1, b_dev.data_ptr(), x_dev.data_ptr(), ns)
+        info = c.pcg_solve_device(f, 1, b_dev.data_ptr(), x_dev[form].data_ptr(), ns)
         e1.record()
         e1.synchronize()
         ms = e0.elapsed_time(e1)
@@ -319,9 +345,8 @@ def run_b200(args, cfg, rank, world, local):
     per_step = {"factor": fi32.ms_factor, "spmv_update": prof[0] * iters, "fwd_solve": prof[1] * iters,
                 "bwd_solve": prof[2] * iters}
     per_launch = {"factor": fi32.ms_factor, "spmv_update": prof[0], "fwd_solve": prof[1], "bwd_solve": prof[2]}
-    A_nnz = int(W["colptr"][-1])
     # the solve matrix is trimmed: nnz without the ground row/column
-    a_nnz_solve = A_nnz - (int(np.diff(W["colptr"])[-1]) * 2 - 1 if ground else 0)
+    a_nnz_solve = W["nnz_solve"]
     ab = algorithmic_bytes(ns, a_nnz_solve, fi32.nnz_strict, fi32.nnz_lower_a, fi32.fills, 1, 4)
     dom = max(per_step, key=per_step.get)
     peak, peak_src = measured_peaks()
@@ -371,9 +396,9 @@ def run_b200(args, cfg, rank, world, local):
         "metric": METRIC, "value": round(mixed_s, 6), "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(mixed_s * 1000.0, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 factor / f64 PCG", "data": "synthetic",
-        "config": {"workload": cfg["workload"], "n": ns, "nnz_A": a_nnz_solve, "tol": cfg["tol"], "rhs": 1,
-                   "parallelism": f"replicas x{args.gpus}", "l2": "inputs larger than L2 and a 256 MiB L2 flush "
-                                                               "between timed steps"},
+        "config": workload_config(cfg, W),
+        "parallelism": f"replicas x{args.gpus}",
+        "l2": "inputs larger than L2 and a 256 MiB L2 flush between timed steps",
         "fp64_s": round(fp64_s, 6), "speedup_mixed_vs_fp64": round(fp64_s / mixed_s, 3),
         "iterations": {"mixed": last["mixed"][2]["iterations"], "fp64": last["fp64"][2]["iterations"]},
         "relres_true": {"mixed": last["mixed"][2]["relres_true"], "fp64": last["fp64"][2]["relres_true"],
@@ -397,12 +422,10 @@ def run_b200(args, cfg, rank, world, local):
         "gpu_launches": int(launches),
         "clocks": clk,
     }
-    for c in ctx.values():
-        for form in last:
-            pass
+    out["_x"] = {form: x_dev[form].cpu().numpy() for form in x_dev}
     for form in last:
         last[form][0].free()
-    return out, W, last["fp64"][2]["iterations"]
+    return out, W, b
 
 
 def spmv_host(W, ns, x):
@@ -419,43 +442,67 @@ def spmv_host(W, ns, x):
 # CPU legs (reference factor + oracle PCG port)
 # ---------------------------------------------------------------------------
 
-def reference_cpu_step(W, mtx_path, threads, iters_hint, pcg_sample_iters, factor_cache):
-    """One bounded sample of the reference CPU implementation: a full run of
-    the reference CPU factor (its own printed factor time) and `pcg_sample_iters`
-    iterations of the FP64 CPU PCG on its factor, scaled to the iteration count
-    of the full solve."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle as O
-    n, ground = W["n"], W["ground"]
-    ns = n - 1 if ground else n
-    want = factor_cache.get("L") is None
-    out = O.run_reference(mtx_path, threads=threads, physics=ground, want_factor=want, timeout=1800)
-    if want:
-        rows, cols, vals, diag = out["rows"], out["cols"], out["vals"], out["diag"]
-        m = (rows != cols) & (rows < ns) & (cols < ns)
-        order = np.lexsort((rows[m], cols[m]))
-        r, c, v = rows[m][order], cols[m][order], vals[m][order]
-        cp = np.concatenate([[0], np.cumsum(np.bincount(c, minlength=ns))]).astype(np.int64)
-        acp, arow, aval = O.trim_last(n, W["colptr"], W["rowind"], W["val"]) if ground else \
-            (W["colptr"], W["rowind"], W["val"])
-        factor_cache["L"] = (cp, r.astype(np.int32), v, diag[:ns].copy())
-        factor_cache["A"] = (acp, arow, aval)
-    cp, r, v, d = factor_cache["L"]
-    acp, arow, aval = factor_cache["A"]
-    rng = np.random.default_rng(7)
-    b = rng.standard_normal(ns)
-    b -= b.mean()
-    if "iters" not in factor_cache:
-        if iters_hint is None:
-            _, info = O.pcg(ns, acp, arow, aval, cp, r, v, d, b, tol=1e-6, max_iter=1000, nthreads=threads)
-            factor_cache["iters"] = info["iterations"]
+class ReferenceCpu:
+    """The reference's own CPU implementation of the path on this host: the
+    reference CPU factor (cpu_implementation/driver_local.cpp, compiled from
+    its sources under oracle/_ref/, run as its own process on all host
+    threads; its printed "Factorization execution time") plus the CPU PCG the
+    reference runs on that factor (experiment/custom_cg.hpp:65-265), whose
+    MKL dependency is absent here, so the oracle's FP64 port stands in
+    (OpenMP SpMV and dot products, sequential triangular solves, as MKL's
+    unoptimised mkl_sparse_d_trsv).  Everything comes from oracle/: the
+    input is generated and written by oracle/gen_inputs.c."""
+
+    def __init__(self, W, threads, tmpdir):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as O
+        self.O, self.W, self.threads = O, W, threads
+        self.mtx = os.path.join(tmpdir, "input.mtx")
+        r, c, v = W["triplets"]
+        O.write_mtx_fast(self.mtx, W["n"], r, c, v)
+        ns = W["ns"]
+        if W["ground"]:
+            self.A = O.trim_last(W["n"], W["colptr"], W["rowind"], W["val"])
         else:
-            factor_cache["iters"] = iters_hint
-    t0 = time.perf_counter()
-    O.pcg(ns, acp, arow, aval, cp, r, v, d, b, tol=1e-300, max_iter=pcg_sample_iters, nthreads=threads)
-    per_iter = (time.perf_counter() - t0) / pcg_sample_iters
-    solve_s = per_iter * factor_cache["iters"]
-    return out["factor_time"] + solve_s, out["factor_time"], solve_s, factor_cache["iters"]
+            self.A = (W["colptr"], W["rowind"], W["val"])
+        self.L = None
+        self.nnz_L_trimmed = None
+
+    def factor(self, keep=False):
+        """One run of the reference factor; keep=True also reads its factor
+        files (l_sol.mtx, sol_diag.txt) for the PCG legs."""
+        O, W = self.O, self.W
+        out = O.run_reference(self.mtx, threads=self.threads, physics=W["ground"], want_factor=keep, timeout=1800)
+        if keep:
+            ns = W["ns"]
+            rows, cols, vals, diag = out["rows"], out["cols"], out["vals"], out["diag"]
+            m = (rows != cols) & (rows < ns) & (cols < ns)
+            order = np.lexsort((rows[m], cols[m]))
+            r, c, v = rows[m][order], cols[m][order], vals[m][order]
+            cp = np.concatenate([[0], np.cumsum(np.bincount(c, minlength=ns))]).astype(np.int64)
+            self.L = (cp, r.astype(np.int32), v, diag[:ns].copy())
+            self.nnz_L_trimmed = int(len(r) + ns)
+            self.factor_nnz = out["factor_nnz"]
+        return out["factor_time"]
+
+    def pcg(self, b, tol):
+        """The FP64 CPU PCG on the kept reference factor, to the true
+        relative residual `tol`; returns (x, info, seconds)."""
+        O = self.O
+        acp, arow, aval = self.A
+        cp, r, v, d = self.L
+        t0 = time.perf_counter()
+        x, info = O.pcg(self.W["ns"], acp, arow, aval, cp, r, v, d, b, tol=tol, max_iter=2000,
+                        nthreads=self.threads)
+        return x, info, time.perf_counter() - t0
+
+
+def err_vs(x, xstar, laplacian):
+    """||x - x*|| / ||x*|| (means removed for a singular Laplacian, whose
+    solutions are defined up to a constant)."""
+    if laplacian:
+        x, xstar = x - x.mean(), xstar - xstar.mean()
+    return float(np.linalg.norm(x - xstar) / np.linalg.norm(xstar))
 
 
 def run_reference_arm(args, cfg):
@@ -463,33 +510,73 @@ def run_reference_arm(args, cfg):
     import pyoracle as O
     if not os.path.exists(O.REF_BIN):
         return {"impl": "reference", "unavailable": "reference CPU factor not built (oracle/_ref/rchol_ref_cpu)"}
-    import rchol_b200 as R
-    W = build_workload(cfg)
+    W = build_workload(cfg, product=False)
     threads = os.cpu_count() or 1
+    b = bench_rhs(W["ns"])
     with tempfile.TemporaryDirectory() as td:
-        mtx = os.path.join(td, "input.mtx")
-        R.write_mtx(mtx, W["n"], *W["triplets"])
-        cache = {}
-        for _ in range(args.warmup):
-            reference_cpu_step(W, mtx, threads, None, 2, cache)
-        vals, facs, sols = [], [], []
+        ref = ReferenceCpu(W, threads, td)
+        # warm-up: reference factor runs (the first one's factor is kept for
+        # the PCG of every step, as the reference's solver reads it back)
+        ref.factor(keep=True)
+        for _ in range(max(0, args.warmup - 1)):
+            ref.factor()
+        vals, facs, sols, its = [], [], [], []
         for _ in range(args.steps):
-            tot, fac, sol, iters = reference_cpu_step(W, mtx, threads, None, 3, cache)
-            vals.append(tot)
+            fac = ref.factor()
+            x, info, sol = ref.pcg(b, cfg["tol"])
+            vals.append(fac + sol)
             facs.append(fac)
             sols.append(sol)
+            its.append(info["iterations"])
     v = statistics.mean(vals)
-    sample = (f"reference CPU factor (cpu_implementation/driver_local.cpp, unmodified) full run on {threads} threads "
-              f"+ 3 iterations of the FP64 CPU PCG port on the reference's factor (MKL absent), scaled to the "
-              f"{cache['iters']} iterations of its full solve")
+    sample = (f"each step: the reference CPU factor (cpu_implementation/driver_local.cpp, unmodified, "
+              f"{threads} threads, its printed factor time) + a full FP64 CPU PCG to true relres {cfg['tol']:g} "
+              f"on the reference's factor ({its[-1]} iterations; port of experiment/custom_cg.hpp, MKL absent)")
     return {"metric": METRIC, "value": round(v, 6), "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(v * 1000, 3), "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": cfg["workload"], "tol": cfg["tol"], "rhs": 1, "parallelism": "cpu"},
+            "config": workload_config(cfg, W), "parallelism": "cpu",
             "factor_s": round(statistics.mean(facs), 6), "pcg_s": round(statistics.mean(sols), 6),
+            "iterations": its[-1], "reference_factor_nnz": ref.factor_nnz,
+            "reference_nnz_L_trimmed": ref.nnz_L_trimmed,
             "cpu_baseline": {"value": round(v, 6), "unit": "s", "cores": threads, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": round(v, 6), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def cpu_baseline_and_oracle_error(out, W, b, cfg):
+    """The CPU baseline beside the GPU line (one step of the reference arm,
+    rank 0, N = 1), the reference factor's nnz on the same input, and each
+    GPU form's error against the FP64 oracle solution x*: PCG to 1e-12 with
+    the reference's own CPU factor.  Untimed for the GPU; ~1 min of CPU."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    xs = out.pop("_x", None)
+    if not os.path.exists(O.REF_BIN):
+        out["cpu_baseline"] = None
+        return
+    threads = os.cpu_count() or 1
+    Wo = build_workload(cfg, product=False)
+    assert Wo["sha"] == W["sha"], "oracle and product generators disagree"
+    with tempfile.TemporaryDirectory() as td:
+        ref = ReferenceCpu(Wo, threads, td)
+        ref.factor(keep=True)
+        fac = ref.factor()
+        _, info, sol = ref.pcg(b, cfg["tol"])
+        xstar, info12, _ = ref.pcg(b, 1e-12)
+    out["cpu_baseline"] = {"value": round(fac + sol, 6), "unit": "s", "cores": threads, "kind": "reference",
+                           "sample": f"one step of --impl reference: the reference CPU factor "
+                                     f"(cpu_implementation/driver_local.cpp) on {threads} threads ({fac:.3f} s) + a "
+                                     f"full FP64 CPU PCG port to relres {cfg['tol']:g} on its factor "
+                                     f"({info['iterations']} iterations, {sol:.3f} s)"}
+    out["reference_factor"] = {"nnz_L": ref.nnz_L_trimmed,
+                               "nnz_ratio_vs_ours": round(out["factor_stats"]["nnz_L"] / ref.nnz_L_trimmed, 4),
+                               "cpu_pcg_iterations": info["iterations"]}
+    if xs:
+        lap = not W["ground"]
+        out["err_vs_oracle"] = {form: err_vs(x, xstar, lap) for form, x in xs.items()}
+        out["err_vs_oracle"]["oracle"] = ("FP64 CPU PCG to true relres 1e-12 with the reference CPU factor "
+                                          f"({info12['iterations']} iterations, relres {info12['relres_true']:.2e})")
 
 
 def c4_systems():
@@ -686,23 +773,10 @@ def main():
         print(json.dumps(run_reference_arm(args, cfg)))
         return
     rank, world, local = dist_init(args.gpus)
-    out, W, iters64 = run_b200(args, cfg, rank, world, local)
+    out, W, b = run_b200(args, cfg, rank, world, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import pyoracle as O
-        if os.path.exists(O.REF_BIN):
-            import rchol_b200 as R
-            threads = os.cpu_count() or 1
-            with tempfile.TemporaryDirectory() as td:
-                mtx = os.path.join(td, "input.mtx")
-                R.write_mtx(mtx, W["n"], *W["triplets"])
-                tot, fac, sol, iters = reference_cpu_step(W, mtx, threads, iters64, 3, {})
-            out["cpu_baseline"] = {"value": round(tot, 6), "unit": "s", "cores": threads, "kind": "reference",
-                                   "sample": f"reference CPU factor (cpu_implementation/driver_local.cpp) full run on "
-                                             f"{threads} threads ({fac:.3f} s) + 3 iterations of the FP64 CPU PCG "
-                                             f"port on its factor scaled to {iters} iterations ({sol:.3f} s)"}
-        else:
-            out["cpu_baseline"] = None
+        cpu_baseline_and_oracle_error(out, W, b, cfg)
+    out.pop("_x", None)
     if rank == 0:
         print(json.dumps(out))
     if world > 1:

@@ -186,12 +186,18 @@ rchol_status rchol_precond_apply(rchol_ctx* ctx, const rchol_factor_t* f, int k,
  * stream).  The call returns after the stream has finished the apply.
  * Scratch is one fixed array in the library's device code, limited to
  * n * k <= 4194304 (2^22 doubles, 32 MiB, plus 4 KiB for scalars); larger
- * sizes return RCHOL_ERR_INVALID.  The first call on each device looks up
- * that array's address (this may load the library's device code), so make
- * it before any stream capture.  All calls on a device share the array:
- * calls that overlap on the GPU (other threads or streams) race on it and
- * must be serialised by the caller.  No counterpart in the reference, which
- * allocates its solver work vectors for each solve. */
+ * sizes return RCHOL_ERR_INVALID.  That array belongs to the library's
+ * device code, so every device that loads the library holds those 32 MiB
+ * until the process exits, whether or not this entry point is called.  Each
+ * call looks up the array's address in the current context; the first
+ * lookup on a device may load the library's device code, so make the first
+ * call before any stream capture.  All calls on a device share the array,
+ * and every solve or apply of one factor shares that factor's split-row
+ * partial sums: a call that overlaps on the GPU (other threads or streams)
+ * with another call, or with rchol_pcg_solve / rchol_precond_apply on the
+ * same factor, races with it, so the caller must serialise them.  No
+ * counterpart in the reference, which allocates its solver work vectors for
+ * each solve. */
 rchol_status rchol_precond_apply_noalloc(const rchol_factor_t* f, int k, const double* R, double* Z, int fp32,
                                          void* stream);
 /* Mean device time (ms) of the three PCG iteration kernels over `reps`
@@ -258,6 +264,11 @@ rchol_status rchol_generate(const char* kind, const long long* dims, int ndims, 
                             double excess_hi, int ordering, unsigned long long seed, int* n_out,
                             long long* nnz_out, int** rows, int** cols, double** vals, int* has_ground);
 void rchol_free_host(void* p);
+/* The reference right-hand side generate_zero_sum_vector(out, n, seed)
+ * (gpu_implementation/solver.hpp:43-61, experiment/custom_cg.hpp:45-63):
+ * n draws of std::mt19937(seed) through uniform_real_distribution<double>(0,1),
+ * minus their mean.  Host only; out[n] is caller-owned. */
+rchol_status rchol_zero_sum_vector(int n, unsigned int seed, double* out);
 /* Write 0-based triplets as a MatrixMarket coordinate/real/general file. */
 rchol_status rchol_write_mtx(const char* path, int n, long long nnz, const int* rows, const int* cols,
                              const double* vals);

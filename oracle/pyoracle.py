@@ -76,6 +76,14 @@ def lib():
                               _f64p, _f64p, C.c_double, C.c_int32, C.c_int, C.c_int,
                               C.POINTER(PcgInfo)]
         L.orc_pcg.restype = C.c_int
+        L.orc_generate_grid.argtypes = [C.c_char_p, _i64p, C.c_int, C.c_double, C.c_double, C.c_int, C.c_double,
+                                        C.c_double, C.c_double, C.c_double, C.c_uint64, C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_int64), C.POINTER(C.POINTER(C.c_int32)),
+                                        C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.POINTER(C.c_double)),
+                                        C.POINTER(C.c_int32)]
+        L.orc_free.argtypes = [C.c_void_p]
+        L.orc_free.restype = None
+        L.orc_write_mtx.argtypes = [C.c_char_p, C.c_int32, C.c_int64, _i32p, _i32p, _f64p]
         _lib = L
     return _lib
 
@@ -187,6 +195,37 @@ def pcg(n, arowptr, acolind, aval, lcolptr, lrow, lval, diag, b, tol=1e-6, max_i
     return x, dict(iterations=info.iterations, converged=bool(info.converged),
                    relres_true=info.relres_true, relres_rec=info.relres_rec,
                    precond_ratio=info.precond_ratio)
+
+
+def generate_grid(kind, dims, wlo=1.0, whi=1.0, log_weights=False, aniso_z=1.0, excess_frac=0.0, excess_lo=0.0,
+                  excess_hi=0.0, seed=0):
+    """The benchmark grid inputs (same triplets as the library's generator)
+    built by oracle/gen_inputs.c: (n, rows, cols, vals, has_ground)."""
+    L = lib()
+    d = np.ascontiguousarray(dims, np.int64)
+    n, nnz, g = C.c_int32(), C.c_int64(), C.c_int32()
+    rp, cp, vp = C.POINTER(C.c_int32)(), C.POINTER(C.c_int32)(), C.POINTER(C.c_double)()
+    rc = L.orc_generate_grid(kind.encode(), d, len(d), wlo, whi, int(log_weights), aniso_z, excess_frac, excess_lo,
+                             excess_hi, seed, C.byref(n), C.byref(nnz), C.byref(rp), C.byref(cp), C.byref(vp),
+                             C.byref(g))
+    if rc != 0:
+        raise ValueError(f"orc_generate_grid failed ({rc})")
+    m = nnz.value
+    try:
+        rows = np.ctypeslib.as_array(rp, (m,)).copy()
+        cols = np.ctypeslib.as_array(cp, (m,)).copy()
+        vals = np.ctypeslib.as_array(vp, (m,)).copy()
+    finally:
+        L.orc_free(C.cast(rp, C.c_void_p))
+        L.orc_free(C.cast(cp, C.c_void_p))
+        L.orc_free(C.cast(vp, C.c_void_p))
+    return n.value, rows, cols, vals, bool(g.value)
+
+
+def write_mtx_fast(path, n, rows, cols, vals):
+    """write_mtx in C (large inputs)."""
+    if lib().orc_write_mtx(path.encode(), n, len(rows), _i32(rows), _i32(cols), _f64(vals)) != 0:
+        raise OSError(f"could not write {path}")
 
 
 # ---------------------------------------------------------------------------

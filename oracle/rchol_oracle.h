@@ -152,6 +152,22 @@ int orc_pcg(int32_t n, const int32_t* arowptr, const int32_t* acolind, const dou
             const double* b, double* x, double tol, int32_t max_iter, int stop_rule,
             int nthreads, orc_pcg_info* info);
 
+/* ---- synthetic inputs without the product library (gen_inputs.c) ------ */
+
+/* The library's grid generator (rchol_generate with ordering 0) restated:
+ * kind "grid2d", "grid3d" or "grid3d27"; ascending-nnz order with a seeded
+ * tie-break; a ground vertex appended when any row has diagonal excess.
+ * The triplet arrays are malloc'ed (release with orc_free).  Returns 0, or
+ * a negative value for a bad kind or a failed allocation. */
+int orc_generate_grid(const char* kind, const int64_t* dims, int ndims, double wlo, double whi, int log_weights,
+                      double aniso_z, double excess_frac, double excess_lo, double excess_hi, uint64_t seed,
+                      int32_t* n_out, int64_t* nnz_out, int32_t** rows_out, int32_t** cols_out,
+                      double** vals_out, int32_t* has_ground_out);
+void orc_free(void* p);
+/* 1-based coordinate/real/general MatrixMarket file, entries in order. */
+int orc_write_mtx(const char* path, int32_t n, int64_t nnz, const int32_t* rows, const int32_t* cols,
+                  const double* vals);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,6 +35,9 @@
 #include <stdexcept>
 #include <string>
 #include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 namespace fast_matrix_market {
 
@@ -89,7 +92,20 @@ void read_matrix_market_triplet(std::istream& in, IT& nrows, IT& ncols,
                                 std::vector<IT>& rows, std::vector<IT>& cols,
                                 std::vector<VT>& vals,
                                 const read_options& opts = {}) {
-    std::string text((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+    // whole file in one read when the stream is seekable
+    std::string text;
+    in.seekg(0, std::ios::end);
+    const std::streamoff fsize = in.good() ? (std::streamoff)in.tellg() : (std::streamoff)-1;
+    if (fsize > 0) {
+        text.resize((size_t)fsize);
+        in.seekg(0, std::ios::beg);
+        in.read(&text[0], fsize);
+        text.resize((size_t)in.gcount());
+    } else {
+        in.clear();
+        in.seekg(0, std::ios::beg);
+        text.assign((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+    }
     const char* p = text.c_str();
     const char* end = p + text.size();
     // banner
@@ -123,14 +139,64 @@ void read_matrix_market_triplet(std::istream& in, IT& nrows, IT& ncols,
     rows.reserve((size_t)nz * (sym == general ? 1 : 2));
     cols.reserve(rows.capacity());
     vals.reserve(rows.capacity());
-    for (long long k = 0; k < nz; ++k) {
-        long long r = std::strtoll(p, &q, 10); p = q;
-        long long c = std::strtoll(p, &q, 10); p = q;
-        double v = 1.0;
-        if (!is_pattern) { v = std::strtod(p, &q); p = q; }
-        rows.push_back((IT)(r - 1));
-        cols.push_back((IT)(c - 1));
-        vals.push_back((VT)v);
+    rows.resize((size_t)nz);
+    cols.resize((size_t)nz);
+    vals.resize((size_t)nz);
+    // The body is split into line-aligned chunks parsed in parallel (the
+    // library parses in parallel too); each chunk first counts its entry
+    // lines, so entries keep their file order.
+    while (p < end && *p != '\n') ++p;  // rest of the size line
+    const char* body = p;
+    int nchunks = 1;
+#ifdef _OPENMP
+    nchunks = std::max(1, omp_get_max_threads());
+#endif
+    std::vector<const char*> cut((size_t)nchunks + 1, end);
+    cut[0] = body;
+    for (int t = 1; t < nchunks; ++t) {
+        const char* s = body + (end - body) * t / nchunks;
+        if (s < cut[(size_t)t - 1]) s = cut[(size_t)t - 1];
+        while (s < end && *s != '\n') ++s;
+        cut[(size_t)t] = s;
+    }
+    auto is_entry_line = [](const char* s, const char* e) {
+        while (s < e && (*s == ' ' || *s == '\t' || *s == '\r')) ++s;
+        return s < e && *s != '\n' && *s != '%';
+    };
+    std::vector<long long> count((size_t)nchunks + 1, 0);
+#pragma omp parallel for schedule(static, 1)
+    for (int t = 0; t < nchunks; ++t) {
+        long long c = 0;
+        for (const char* s = cut[(size_t)t]; s < cut[(size_t)t + 1];) {
+            const char* e = (const char*)std::memchr(s, '\n', (size_t)(cut[(size_t)t + 1] - s));
+            if (!e) e = cut[(size_t)t + 1];
+            if (is_entry_line(s, e)) ++c;
+            s = e + 1;
+        }
+        count[(size_t)t + 1] = c;
+    }
+    for (int t = 0; t < nchunks; ++t) count[(size_t)t + 1] += count[(size_t)t];
+    if (count[(size_t)nchunks] < nz) throw std::runtime_error("MatrixMarket file has fewer entries than its header");
+#pragma omp parallel for schedule(static, 1)
+    for (int t = 0; t < nchunks; ++t) {
+        long long k = count[(size_t)t];
+        char* qq = nullptr;
+        for (const char* s = cut[(size_t)t]; s < cut[(size_t)t + 1] && k < nz;) {
+            const char* e = (const char*)std::memchr(s, '\n', (size_t)(cut[(size_t)t + 1] - s));
+            if (!e) e = cut[(size_t)t + 1];
+            if (is_entry_line(s, e)) {
+                const char* z = s;
+                long long r = std::strtoll(z, &qq, 10); z = qq;
+                long long c = std::strtoll(z, &qq, 10); z = qq;
+                double v = 1.0;
+                if (!is_pattern) v = std::strtod(z, &qq);
+                rows[(size_t)k] = (IT)(r - 1);
+                cols[(size_t)k] = (IT)(c - 1);
+                vals[(size_t)k] = (VT)v;
+                ++k;
+            }
+            s = e + 1;
+        }
     }
     if (sym != general && opts.generalize_symmetry) {
         size_t base = rows.size();

@@ -526,13 +526,6 @@ __global__ void trim_scatter_kernel(int32_t nout, const int32_t* __restrict__ co
     }
 }
 
-int grid_for(int64_t work, int block) {
-    int64_t g = ceil_div(work, block);
-    if (g < 1) g = 1;
-    if (g > 148 * 32) g = 148 * 32;
-    return (int)g;
-}
-
 template <typename T>
 cudaError_t dmalloc(T** p, int64_t n) {
     return cudaMalloc((void**)p, sizeof(T) * (size_t)(n > 0 ? n : 1));
@@ -637,7 +630,7 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
     }
     // deterministic row order: warp sort for short rows, CTA sort for long ones
     const int sort_block = 256;
-    const int sort_grid = 148 * 4;
+    const int sort_grid = current_sm_count() * 4;
     RCHOL_TRY(cudaMemsetAsync(dsc, 0, sizeof(int32_t) * 4, s));  // long rows, max row, max level
     max_kernel<<<grid_for(nout, 256), 256, 0, s>>>(cnt, nout, dsc + 1);
     max_kernel<<<grid_for(nout, 256), 256, 0, s>>>(w.level, nout, dsc + 2);
@@ -651,7 +644,7 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
     int32_t* gkey = nullptr;
     double* gval = nullptr;
     int64_t gcap = 1;
-    const int lgrid = hs[0] > 0 ? std::min(hs[0], 148 * 2) : 1;
+    const int lgrid = hs[0] > 0 ? std::min(hs[0], current_sm_count() * 2) : 1;
     if (hs[0] > 0 && hs[1] > kBlockSortCap) {
         while (gcap < hs[1]) gcap <<= 1;
         RCHOL_TRY(sc.get(&gkey, (int64_t)lgrid * gcap));

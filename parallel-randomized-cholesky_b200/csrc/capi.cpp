@@ -1359,6 +1359,14 @@ extern "C" rchol_status rchol_csc_from_triplets(int n, long long nnz, const int*
     return RCHOL_OK;
 }
 
+extern "C" rchol_status rchol_zero_sum_vector(int n, unsigned int seed, double* out) {
+    if (n < 0 || (n > 0 && !out)) return RCHOL_ERR_INVALID;
+    std::vector<double> b;
+    zero_sum_rhs(b, (size_t)n, (unsigned long)seed);
+    if (n > 0) std::memcpy(out, b.data(), sizeof(double) * (size_t)n);
+    return RCHOL_OK;
+}
+
 extern "C" rchol_status rchol_read_mtx(const char* path, int* n, long long* nnz, int** rows, int** cols,
                                        double** vals) {
     if (!path || !n || !nnz || !rows || !cols || !vals) return RCHOL_ERR_INVALID;

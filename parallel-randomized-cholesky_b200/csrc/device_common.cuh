@@ -94,4 +94,27 @@ __host__ __device__ __forceinline__ double sample_uniform(uint64_t seed, int32_t
 
 __host__ __device__ __forceinline__ int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Streaming multiprocessors of the current device, queried once per device
+// ordinal (1 if the query fails: launches stay correct, only smaller).
+inline int current_sm_count() {
+    static int cached[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 1;
+    if (dev < 64 && cached[dev] > 0) return cached[dev];
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) return 1;
+    if (dev < 64) cached[dev] = sms;
+    return sms;
+}
+
+// Grid for a grid-stride loop over `work` items: enough blocks for one item
+// per thread, capped at `per_sm` blocks per SM of the current device.
+inline int grid_for(int64_t work, int block, int per_sm = 32) {
+    int64_t g = ceil_div(work, block);
+    const int64_t cap = (int64_t)current_sm_count() * per_sm;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
 }  // namespace rchol

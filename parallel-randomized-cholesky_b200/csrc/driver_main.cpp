@@ -18,7 +18,6 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <random>
 #include <string>
 #include <vector>
 
@@ -48,18 +47,6 @@ bool parse_extra(const char* a, rchol_opts& o, int& k) {
     else if (key == "timeout") o.timeout_s = std::atof(v.c_str());
     else return false;
     return true;
-}
-
-void zero_sum(std::vector<double>& b, size_t n, unsigned long seed) {
-    std::mt19937 gen(seed);
-    std::uniform_real_distribution<double> dist(0.0, 1.0);
-    double s = 0.0;
-    b.resize(n);
-    for (size_t i = 0; i < n; ++i) {
-        b[i] = dist(gen);
-        s += b[i];
-    }
-    for (size_t i = 0; i < n; ++i) b[i] -= s / (double)n;
 }
 
 int die(rchol_ctx* ctx, rchol_status s, const char* what) {
@@ -147,11 +134,9 @@ int main(int argc, char** argv) {
     if (solve) {
         const int ns = fi.n;
         if (k < 1) k = 1;
-        std::vector<double> b((size_t)ns * k), x((size_t)ns * k, 0.0), col;
-        for (int c = 0; c < k; ++c) {
-            zero_sum(col, (size_t)ns, (unsigned long)c);
-            std::copy(col.begin(), col.end(), b.begin() + (size_t)c * ns);
-        }
+        std::vector<double> b((size_t)ns * k), x((size_t)ns * k, 0.0);
+        // column c: the reference right-hand side generate_zero_sum_vector(seed c)
+        for (int c = 0; c < k; ++c) rchol_zero_sum_vector(ns, (unsigned)c, b.data() + (size_t)c * ns);
         rchol_solve_info si;
         s = rchol_pcg_solve(ctx, f, k, b.data(), x.data(), ns, 0, &si);
         if (s != RCHOL_OK && s != RCHOL_ERR_NOT_CONVERGED) return die(ctx, s, "solve");

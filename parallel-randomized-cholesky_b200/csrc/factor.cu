@@ -1075,13 +1075,6 @@ __global__ void init_queue_kernel(int32_t n, const int32_t* __restrict__ dep, in
     }
 }
 
-int grid_for(int64_t work, int block) {
-    int64_t g = ceil_div(work, block);
-    if (g < 1) g = 1;
-    if (g > 148 * 32) g = 148 * 32;
-    return (int)g;
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------------------

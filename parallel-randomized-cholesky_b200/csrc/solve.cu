@@ -20,7 +20,6 @@
 #include <cstdio>
 #include <algorithm>
 #include <cstring>
-#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -1105,6 +1104,18 @@ struct Kernels {
     static void* bwd() { return (void*)bwd_kernel<K, TV>; }
 };
 
+// The part-task counters of split rows (pcount_*) return to zero when a row
+// completes.  A pass abandoned on a timeout leaves some of them part-way, so
+// every solve and every preconditioner apply clears them first (a memset of
+// one int per split row; no allocation).
+cudaError_t clear_split_counters(const DevFactor& F, cudaStream_t s) {
+    if (F.nsplit_f > 0 && F.pcount_f)
+        RCHOL_TRY(cudaMemsetAsync(F.pcount_f, 0, sizeof(int32_t) * (size_t)F.nsplit_f, s));
+    if (F.nsplit_b > 0 && F.pcount_b)
+        RCHOL_TRY(cudaMemsetAsync(F.pcount_b, 0, sizeof(int32_t) * (size_t)F.nsplit_b, s));
+    return cudaSuccess;
+}
+
 int resident_blocks(const void* fn, int device) {
     int per_sm = 0, sms = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0);
@@ -1367,6 +1378,7 @@ cudaError_t pcg_solve(PcgSolver* s, const double* dB, double* dX, SolveResult* r
     if (s->cfg.use_graph && (e = build_graph(s, dB, dX)) != cudaSuccess) return e;
     e = cudaEventRecord(s->ev0, s->stream);
     if (e != cudaSuccess) return e;
+    if ((e = clear_split_counters(s->F, s->stream)) != cudaSuccess) return e;
     SolveArgs a = s->args(dB, dX);
     if ((e = s->launch(s->k_init, s->grid_vec, a)) != cudaSuccess) return e;
     if ((e = s->launch_start(dB, dX)) != cudaSuccess) return e;
@@ -1467,6 +1479,7 @@ cudaError_t pcg_profile(PcgSolver* s, const double* dB, double* dX, int reps, fl
     s->cfg.max_iter = 1 << 30;
     SolveArgs a = s->args(dB, dX);
     cudaError_t e;
+    if ((e = clear_split_counters(s->F, s->stream)) != cudaSuccess) return e;
     if ((e = s->launch(s->k_init, s->grid_vec, a)) != cudaSuccess) return e;
     if ((e = s->launch_start(dB, dX)) != cudaSuccess) return e;
     cudaEvent_t ev[4];
@@ -1911,6 +1924,7 @@ cudaError_t batch_solve(BatchSolver* s, const double* dB, double* dX, BatchResul
         s->gx = dX;
     }
     cudaEventRecord(b->ev0, b->stream);
+    if ((e = clear_split_counters(b->F, b->stream)) != cudaSuccess) return e;
     BatchArgs a = s->args(dB, dX);
     if ((e = s->launch(s->k_init, s->grid, &a)) != cudaSuccess) return e;
     {  // start: z = M r, rz per pair
@@ -1994,21 +2008,21 @@ __global__ void rm_to_cm_kernel(const double* __restrict__ rm, double* cm, int l
 
 cudaError_t cm_to_rm(const double* cm, int ld, double* rm, int32_t n, int k, cudaStream_t s) {
     int64_t total = (int64_t)n * k;
-    int grid = (int)std::min<int64_t>(std::max<int64_t>(ceil_div(total, kBlock), 1), 148 * 16);
+    int grid = grid_for(total, kBlock, 16);
     cm_to_rm_kernel<<<grid, kBlock, 0, s>>>(cm, ld, rm, n, k);
     return cudaGetLastError();
 }
 
 cudaError_t rm_to_cm(const double* rm, double* cm, int ld, int32_t n, int k, cudaStream_t s) {
     int64_t total = (int64_t)n * k;
-    int grid = (int)std::min<int64_t>(std::max<int64_t>(ceil_div(total, kBlock), 1), 148 * 16);
+    int grid = grid_for(total, kBlock, 16);
     rm_to_cm_kernel<<<grid, kBlock, 0, s>>>(rm, cm, ld, n, k);
     return cudaGetLastError();
 }
 
 cudaError_t spmv_f64(const DevCsc& A, const double* x, double* y, int k, cudaStream_t s) {
     int64_t total = (int64_t)A.n * k;
-    int grid = (int)std::min<int64_t>(std::max<int64_t>(ceil_div(total, kBlock), 1), 148 * 16);
+    int grid = grid_for(total, kBlock, 16);
     spmv_plain_kernel<<<grid, kBlock, 0, s>>>(A.n, A.colptr, A.rowind, A.val, x, y, k);
     return cudaGetLastError();
 }
@@ -2019,7 +2033,12 @@ static cudaError_t precond_apply_t(const DevFactor& F, const double* r, double* 
     PcgScalars* sc = nullptr;
     cudaError_t e = cudaMalloc(&sc, sizeof(PcgScalars));
     if (e != cudaSuccess) return e;
-    cudaMemsetAsync(sc, 0, sizeof(PcgScalars), s);
+    e = cudaMemsetAsync(sc, 0, sizeof(PcgScalars), s);
+    if (e == cudaSuccess) e = clear_split_counters(F, s);
+    if (e != cudaSuccess) {
+        cudaFree(sc);
+        return e;
+    }
     SolveArgs a;
     memset(&a, 0, sizeof(a));
     a.n = F.n;
@@ -2056,7 +2075,7 @@ static cudaError_t precond_apply_t(const DevFactor& F, const double* r, double* 
     a.reduce = 0;
     a.timeout_ns = (unsigned long long)(timeout_s * 1e9);
     const int64_t total = (int64_t)F.n * K;
-    fill_pending_kernel<<<148 * 8, kBlock, 0, s>>>(y, total);
+    fill_pending_kernel<<<grid_for(total, kBlock, 8), kBlock, 0, s>>>(y, total);
     if (K == 1) {
         int gf = resident_blocks((void*)fwd_pack_kernel<TV>, device);
         int gb = resident_blocks((void*)bwd_pack_kernel<TV>, device);
@@ -2102,31 +2121,28 @@ cudaError_t precond_apply(const DevFactor& F, const double* r, double* z, double
 // n x k forward-solve vector y) taken from one statically sized module
 // array instead of cudaMalloc.  All calls on a device share that array and
 // leave their contents in it; two calls whose kernels overlap on the GPU
-// race on it.
+// race on it.  They also share the factor's split-row partial sums and
+// counters (psum_*, pcount_*) with every other solve or apply of the same
+// factor, so calls must be serialised against those as well.  The array is
+// part of this module's device code: every device that loads the library
+// holds its 32 MiB + 4 KiB until the process exits, whether or not this
+// entry point is ever called.
 
 constexpr int kNoAllocHeadDoubles = 512;  // 4 KiB: the PcgScalars block
 static_assert(sizeof(PcgScalars) <= kNoAllocHeadDoubles * sizeof(double), "scalar block does not fit");
-constexpr int kNoAllocMaxDevices = 64;
-
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocHeadDoubles + kNoAllocMaxElems];
 
 namespace {
 
-std::mutex g_noalloc_mu;
-double* g_noalloc_base[kNoAllocMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on `device` (which must be current),
-// looked up once per device; the lookup may load this module onto the device.
-cudaError_t noalloc_scratch(int device, double** out) {
-    if (device < 0 || device >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> guard(g_noalloc_mu);
-    if (!g_noalloc_base[device]) {
-        double* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_noalloc_base[device] = p;
-    }
-    *out = g_noalloc_base[device];
+// Device address of g_noalloc_scratch in the current context.  It is looked
+// up on every call (cheap once the module is loaded), so a context that was
+// torn down and recreated, e.g. after cudaDeviceReset, gets its new address;
+// the first lookup in a context may load this module onto the device.
+cudaError_t noalloc_scratch(double** out) {
+    double* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    *out = p;
     return cudaSuccess;
 }
 
@@ -2137,6 +2153,7 @@ cudaError_t precond_apply_noalloc_t(const DevFactor& F, const double* r, double*
     double* y = scratch + kNoAllocHeadDoubles;
     // the status word and counters must start at zero; y starts "pending"
     cudaError_t e = cudaMemsetAsync(sc, 0, sizeof(PcgScalars), s);
+    if (e == cudaSuccess) e = clear_split_counters(F, s);
     if (e != cudaSuccess) return e;
     SolveArgs a;
     memset(&a, 0, sizeof(a));
@@ -2173,7 +2190,7 @@ cudaError_t precond_apply_noalloc_t(const DevFactor& F, const double* r, double*
     a.update = 0;
     a.reduce = 0;
     a.timeout_ns = (unsigned long long)(timeout_s * 1e9);
-    fill_pending_kernel<<<148 * 8, kBlock, 0, s>>>(y, (int64_t)F.n * K);
+    fill_pending_kernel<<<grid_for((int64_t)F.n * K, kBlock, 8), kBlock, 0, s>>>(y, (int64_t)F.n * K);
     if (K == 1) {
         fwd_pack_kernel<TV><<<resident_blocks((void*)fwd_pack_kernel<TV>, device), kBlock, 0, s>>>(a);
         bwd_pack_kernel<TV><<<resident_blocks((void*)bwd_pack_kernel<TV>, device), kBlock, 0, s>>>(a);
@@ -2198,7 +2215,7 @@ cudaError_t precond_apply_noalloc(const DevFactor& F, const double* r, double* z
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) return e;
     double* scratch = nullptr;
-    e = noalloc_scratch(device, &scratch);
+    e = noalloc_scratch(&scratch);
     if (e != cudaSuccess) return e;
 #define RCHOL_PAN(KK)                                                                                        \
     case KK:                                                                                                 \

@@ -26,15 +26,15 @@ STOP_RELRES, STOP_PRECOND, STOP_ABS_R2 = 0, 1, 2
 SPMV_AUTO, SPMV_CSR = 0, 1
 
 # every symbol include/rchol.h declares
-EXPORTS = [
+EXPORTS = sorted([
     "rchol_opts_default", "rchol_create", "rchol_destroy", "rchol_set_opts", "rchol_status_string",
     "rchol_last_error", "rchol_load_mtx", "rchol_set_triplets", "rchol_set_csc", "rchol_csc_from_triplets",
     "rchol_read_mtx", "rchol_matrix_info", "rchol_matrix_copy_to_host", "rchol_factor", "rchol_factor_get_info",
     "rchol_factor_copy_to_host", "rchol_factor_write", "rchol_factor_read", "rchol_factor_from_csr_upper",
     "rchol_factor_free", "rchol_pcg_solve", "rchol_precond_apply", "rchol_precond_apply_noalloc", "rchol_profile_solve", "rchol_spmv", "rchol_factorization_driver",
     "rchol_prepare_and_solve", "rchol_generate", "rchol_free_host", "rchol_write_mtx", "rchol_batch_set",
-    "rchol_batch_solve",
-]
+    "rchol_batch_solve", "rchol_zero_sum_vector",
+])
 
 
 class RcholError(RuntimeError):
@@ -132,6 +132,7 @@ def lib():
         L.rchol_free_host.argtypes = [vp]
         L.rchol_free_host.restype = None
         L.rchol_write_mtx.argtypes = [C.c_char_p, C.c_int, C.c_longlong, vp, vp, vp]
+        L.rchol_zero_sum_vector.argtypes = [C.c_int, C.c_uint, vp]
         L.rchol_batch_set.argtypes = [vp, C.c_int, C.POINTER(System), C.POINTER(C.c_longlong)]
         L.rchol_batch_solve.argtypes = [vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, C.POINTER(SolveInfo),
                                         C.POINTER(SolveInfo)]
@@ -217,6 +218,14 @@ def read_mtx(path):
            np.ctypeslib.as_array(v, shape=(m,)).copy())
     for p in (r, c, v):
         L.rchol_free_host(C.cast(p, C.c_void_p))
+    return out
+
+
+def zero_sum_vector(n, seed=0):
+    """The reference right-hand side generate_zero_sum_vector(n, seed)
+    (gpu_implementation/solver.hpp:43-61), host only."""
+    out = np.zeros(n, np.float64)
+    _check(lib().rchol_zero_sum_vector(int(n), int(seed), _ptr(out)))
     return out
 
 

@@ -202,3 +202,32 @@ def test_invalid_inputs_report_status():
             ctx.set_triplets(n, r, c, v)
     finally:
         ctx.close()
+
+
+def test_factor_timeout_is_reported_then_recovers():
+    """A wait limit far below the elimination's queue waits: the factor
+    kernel gives up with RCHOL_ERR_TIMEOUT (bounded device waits, no hang),
+    and the next factorization with the normal limit is bit-exact."""
+    n, r, c, v, g = grid_laplacian((40, 40, 40), seed=9, excess_frac=0.05)
+    P = OracleProblem(n, r, c, v, trim=g)
+    orc = P.factor(seed=5)
+    ctx = R.Context(seed=5)
+    try:
+        ctx.set_triplets(n, r, c, v, trim_ground=g)
+        ctx.set_opts(timeout_s=1e-7)
+        timeouts = 0
+        for _ in range(3):
+            try:
+                ctx.factor().free()
+            except R.RcholError as e:
+                assert e.status == 5
+                timeouts += 1
+        assert timeouts > 0
+        ctx.set_opts(timeout_s=30.0)
+        f = ctx.factor()
+        cp, ri, val, d = f.to_host()
+        assert np.array_equal(cp, orc["colptr"]) and np.array_equal(ri, orc["rowind"])
+        assert np.array_equal(val, orc["val"]) and np.array_equal(d, orc["diag"])
+        f.free()
+    finally:
+        ctx.close()

@@ -198,6 +198,46 @@ def test_split_rows_match_oracle(graph):
         ctx.close()
 
 
+def test_split_counters_recover_after_timeout():
+    """A wait limit far below an apply's duration abandons the passes with
+    some split rows' part counters part-way; the next apply with a normal
+    limit must still match the oracle (the counters are cleared per call)."""
+    n, r, c, v, g = R.generate("chunglu", [20000, 150000, 2, 5000], wlo=1.0, whi=10.0, seed=7)
+    P = OracleProblem(n, r, c, v, trim=g)
+    orc = P.factor(seed=12)
+    assert np.bincount(orc["rowind"], minlength=P.ns).max() > 1024  # split rows exist
+    ctx = R.Context(seed=12, precision=R.PREC_FP64, tol=1e-8)
+    try:
+        ctx.set_triplets(n, r, c, v, trim_ground=g)
+        f = ctx.factor()
+        rr = zero_sum_normal(P.ns, 22)
+        ref = O.precond_apply(P.ns, orc["colptr"], orc["rowind"], orc["val"], orc["diag"], rr)
+        ctx.set_opts(timeout_s=1e-7)
+        timeouts = 0
+        for _ in range(4):
+            try:
+                ctx.precond_apply(f, rr)
+            except R.RcholError as e:
+                assert e.status == 5
+                timeouts += 1
+            try:
+                ctx.pcg_solve(f, rr)
+            except R.RcholError as e:
+                assert e.status == 5
+                timeouts += 1
+        assert timeouts > 0
+        ctx.set_opts(timeout_s=30.0)
+        for fp32 in (False, True):
+            z = ctx.precond_apply(f, rr, fp32=fp32)
+            tol = 2e-5 if fp32 else 1e-12
+            np.testing.assert_allclose(z, ref, rtol=tol, atol=tol * np.abs(ref).max())
+        x, info = ctx.pcg_solve(f, rr)
+        assert info["converged"]
+        f.free()
+    finally:
+        ctx.close()
+
+
 def test_laplacian_without_ground():
     n, r, c, v, g = grid_laplacian((64, 64), seed=31)
     P = OracleProblem(n, r, c, v)

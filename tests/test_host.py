@@ -178,3 +178,33 @@ def test_cli_usage_errors_without_gpu():
     for name in ["driver", "driver_physics", "driver_local"]:
         p = subprocess.run([R.driver_binary(name)], capture_output=True, text=True)
         assert p.returncode == 1 and "argument count not correct" in p.stdout
+
+
+@pytest.mark.parametrize("kind,dims,kw", [
+    ("grid3d", [14, 13, 12], dict(wlo=1e-3, whi=1e3, log_weights=True, excess_frac=0.05, excess_lo=0.0,
+                                  excess_hi=1e-2, seed=2)),
+    ("grid2d", [33, 17], dict(seed=0)),
+    ("grid3d27", [9, 8, 7], dict(wlo=0.1, whi=10.0, log_weights=True, aniso_z=100.0, excess_frac=1.0,
+                                 excess_lo=1e-4, excess_hi=1e-4, seed=5)),
+])
+def test_oracle_input_generator_matches_library(kind, dims, kw):
+    """The CPU legs of bench.py build their input with oracle/gen_inputs.c
+    (never loading the product library); it must give the library
+    generator's triplets bit for bit."""
+    a = R.generate(kind, dims, **kw)
+    b = O.generate_grid(kind, dims, **kw)
+    assert a[0] == b[0] and a[4] == b[4]
+    for x, y in zip(a[1:4], b[1:4]):
+        assert np.array_equal(x, y)
+
+
+def test_bench_arms_share_the_input():
+    """Both bench arms print the same config, including the input checksum."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench", os.path.join(ROOT, "bench.py"))
+    B = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(B)
+    cfg = dict(B.CONFIGS["c2"], dims=[12, 12, 12])
+    Wp = B.build_workload(cfg, product=True)
+    Wo = B.build_workload(cfg, product=False)
+    assert B.workload_config(cfg, Wp) == B.workload_config(cfg, Wo)

@@ -56,6 +56,9 @@ def test_zero_sum_vector_matches_reference(name, n, seed):
     ref = np.loadtxt(os.path.join(GOLDEN, name))
     got = O.zero_sum_vector(n, seed)
     assert np.array_equal(got, ref)  # bit-exact (17 significant digits round-trip)
+    # the library's copy (used by the CLI drivers) is the same generator
+    import rchol_b200 as R
+    assert np.array_equal(R.zero_sum_vector(n, seed), ref)
 
 
 def _golden_cases():

@@ -2,7 +2,8 @@
 against the allocating one (rchol_precond_apply) on the same factor.
 
 Both run the same sweeps over the same factor, so they agree to 1e-12
-relative (FP64 and FP32 factor copies alike).  Two calls in a row check that
+relative (FP64 and FP32 factor copies alike); the results are also checked
+against the oracle's CPU apply on the host copy of the factor.  Two calls in a row check that
 the shared scratch is reset between calls, and device free memory must not
 move across a call.  This file is collected last so that it also runs after
 every other GPU test in the same process.
@@ -10,6 +11,7 @@ every other GPU test in the same process.
 import numpy as np
 import pytest
 
+import pyoracle as O
 import rchol_b200 as R
 
 pytestmark = pytest.mark.gpu
@@ -49,6 +51,15 @@ def test_noalloc_matches_precond_apply(setup, k, fp32):
     for z, ref in zip(Zd, refs):
         got = z.cpu().numpy()
         np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+    # and directly against the oracle's L^-T D^+ L^-1 on the same factor
+    # (FP64 sweeps: 1e-12; the FP32 factor copy: 2e-5, as the other tests)
+    cp, ri, lv, d = f.to_host()
+    tol = 2e-5 if fp32 else 1e-12
+    for z, Rh in zip(Zd, Rs):
+        got = z.cpu().numpy()
+        for c in range(k):
+            ref = O.precond_apply(ns, cp, ri, lv, d, Rh[:, c])
+            np.testing.assert_allclose(got[:, c], ref, rtol=tol, atol=tol * np.abs(ref).max())
 
 
 def test_noalloc_rejects_oversize_and_bad_k():
