@@ -52,10 +52,14 @@ struct rchol_ctx {
     double* dB = nullptr;
     double* dX = nullptr;
     size_t stage_elems = 0;
+    // factors made by this context and not yet freed: rchol_destroy detaches
+    // them, so that a factor freed after its context does not touch it
+    std::vector<rchol_factor_t*> live;
 };
 
 struct rchol_factor {
-    rchol_ctx* ctx = nullptr;
+    rchol_ctx* ctx = nullptr;  // null once the context is destroyed
+    int device = 0;
     DevFactor F;
     rchol_factor_info info;
 };
@@ -304,6 +308,7 @@ extern "C" rchol_status rchol_create(rchol_ctx** out, const rchol_opts* opts) {
 extern "C" void rchol_destroy(rchol_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
+    for (rchol_factor_t* f : ctx->live) f->ctx = nullptr;
     drop_solver(ctx);
     drop_sell(ctx);
     free_work(ctx->w);
@@ -554,6 +559,8 @@ extern "C" rchol_status rchol_factor(rchol_ctx* ctx, rchol_factor_t** out) {
     }
     rchol_factor_t* f = new rchol_factor_t();
     f->ctx = ctx;
+    f->device = ctx->device;
+    ctx->live.push_back(f);
     f->F = ctx->spare;  // reuse the buffers of the last released factor
     ctx->spare = DevFactor();
     cudaError_t e = rchol::assemble_factor(w, ctx->trim, o.precision == RCHOL_PREC_FP32_FACTOR, o.sched_epl,
@@ -614,7 +621,7 @@ extern "C" rchol_status rchol_factor_copy_to_host(const rchol_factor_t* f, long 
                                                   double* val, double* diag) {
     if (!f) return RCHOL_ERR_INVALID;
     rchol_ctx* ctx = f->ctx;
-    cudaSetDevice(ctx->device);
+    cudaSetDevice(f->device);
     const DevFactor& F = f->F;
     if (colptr) CK(cudaMemcpy(colptr, F.lc_ptr, sizeof(int64_t) * ((size_t)F.n + 1), cudaMemcpyDeviceToHost), "copy");
     if (rowind) CK(cudaMemcpy(rowind, F.lc_idx, sizeof(int32_t) * (size_t)F.nnz, cudaMemcpyDeviceToHost), "copy");
@@ -659,6 +666,8 @@ rchol_status factor_from_host_csc(rchol_ctx* ctx, int32_t n, const std::vector<i
         }
     rchol_factor_t* f = new rchol_factor_t();
     f->ctx = ctx;
+    f->device = ctx->device;
+    ctx->live.push_back(f);
     DevFactor& F = f->F;
     F.n = n;
     F.nnz = nnz;
@@ -802,8 +811,9 @@ extern "C" rchol_status rchol_factor_from_csr_upper(rchol_ctx* ctx, int n, const
 extern "C" void rchol_factor_free(rchol_factor_t* f) {
     if (!f) return;
     rchol_ctx* ctx = f->ctx;
+    cudaSetDevice(f->device);
     if (ctx) {
-        cudaSetDevice(ctx->device);
+        ctx->live.erase(std::remove(ctx->live.begin(), ctx->live.end(), f), ctx->live.end());
         // the PCG solver stays for the next factor (rchol::pcg_rebind)
         if (ctx->solver_f == f) ctx->solver_f = nullptr;
         if (ctx->bsolver_f == f) drop_solver(ctx);
@@ -998,7 +1008,7 @@ extern "C" rchol_status rchol_precond_apply_noalloc(const rchol_factor_t* f, int
                     "precond_apply_noalloc: n * k = " + std::to_string((long long)f->F.n * k) +
                         " exceeds the allocation-free limit of " + std::to_string(rchol::kNoAllocMaxElems) +
                         " elements");
-    if (ctx) cudaSetDevice(ctx->device);
+    cudaSetDevice(f->device);
     int status = 0;
     CK(rchol::precond_apply_noalloc(f->F, R, Z, k, fp32 != 0, &status, ctx ? ctx->o.timeout_s : 30.0,
                                     (cudaStream_t)stream),

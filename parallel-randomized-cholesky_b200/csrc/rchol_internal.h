@@ -16,8 +16,7 @@ namespace rchol {
 struct Scratch {
     char* base = nullptr;
     size_t cap = 0, used = 0;
-    void* overflow[64] = {};
-    int noverflow = 0;
+    std::vector<void*> overflow;
     size_t overflow_bytes = 0;  // requests the arena could not serve since the last reset
     cudaError_t reserve(size_t bytes) {
         if (bytes <= cap) return cudaSuccess;
@@ -33,8 +32,8 @@ struct Scratch {
     void reset() {
         const size_t peak = used + overflow_bytes;
         used = 0;
-        for (int i = 0; i < noverflow; ++i) cudaFree(overflow[i]);
-        noverflow = 0;
+        for (void* p : overflow) cudaFree(p);
+        overflow.clear();
         if (overflow_bytes) {
             overflow_bytes = 0;
             reserve(peak + (peak >> 3));
@@ -48,10 +47,9 @@ struct Scratch {
             used += bytes;
             return cudaSuccess;
         }
-        if (noverflow == 64) return cudaErrorMemoryAllocation;
         cudaError_t e = cudaMalloc((void**)p, bytes);
         if (e == cudaSuccess) {
-            overflow[noverflow++] = *p;
+            overflow.push_back(*p);
             overflow_bytes += bytes;
         }
         return e;

@@ -231,3 +231,19 @@ def test_factor_timeout_is_reported_then_recovers():
         f.free()
     finally:
         ctx.close()
+
+
+def test_factor_outlives_its_context():
+    """A factor freed after its context (as on an error path that skips the
+    factor's release) is detached by rchol_destroy: its host copy still
+    works and freeing it does not touch the destroyed context."""
+    n, r, c, v, g = grid_laplacian((20, 20), seed=5)
+    P = OracleProblem(n, r, c, v, trim=g)
+    orc = P.factor(seed=6)
+    ctx = R.Context(seed=6)
+    ctx.set_triplets(n, r, c, v, trim_ground=g)
+    f = ctx.factor()
+    ctx.close()
+    cp, ri, val, d = f.to_host()
+    assert np.array_equal(ri, orc["rowind"]) and np.array_equal(val, orc["val"])
+    f.free()
