@@ -11,6 +11,7 @@ sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs through the C-ABI library")
+    config.addinivalue_line("markers", "slow: takes minutes (benchmark-size inputs)")
 
 
 @pytest.fixture(scope="session")

@@ -73,28 +73,20 @@ class OracleProblem:
         f = O.factor(self.n, self.lcp, self.lrow, self.lval, self.dep, mode=mode, seed=seed)
         return trim_factor(f, self.n) if self.trim else f
 
-    def pcg(self, f, b, tol=1e-6, max_iter=1000, stop_rule=O.STOP_RELRES):
+    def pcg(self, f, b, tol=1e-6, max_iter=1000, stop_rule=O.STOP_RELRES, nthreads=1):
         return O.pcg(self.ns, self.acp, self.arow, self.aval, f["colptr"], f["rowind"], f["val"], f["diag"], b,
-                     tol=tol, max_iter=max_iter, stop_rule=stop_rule)
+                     tol=tol, max_iter=max_iter, stop_rule=stop_rule, nthreads=nthreads)
 
 
 def trim_factor(f, n):
     """Drop the last vertex (ground) from an oracle factor."""
     cp, ri, v = f["colptr"], f["rowind"], f["val"]
-    keep_cols = n - 1
-    new_cp = [0]
-    rows, vals = [], []
-    for j in range(keep_cols):
-        s, e = cp[j], cp[j + 1]
-        r = ri[s:e]
-        m = r < n - 1
-        rows.append(r[m])
-        vals.append(v[s:e][m])
-        new_cp.append(new_cp[-1] + int(m.sum()))
+    cols = np.repeat(np.arange(n), np.diff(cp))
+    keep = (ri < n - 1) & (cols < n - 1)
     out = dict(f)
-    out["colptr"] = np.array(new_cp, np.int64)
-    out["rowind"] = np.concatenate(rows).astype(np.int32) if rows else np.zeros(0, np.int32)
-    out["val"] = np.concatenate(vals) if vals else np.zeros(0)
+    out["colptr"] = np.concatenate([[0], np.cumsum(np.bincount(cols[keep], minlength=n - 1))]).astype(np.int64)
+    out["rowind"] = ri[keep].astype(np.int32)
+    out["val"] = v[keep].copy()
     out["diag"] = f["diag"][:n - 1].copy()
     return out
 

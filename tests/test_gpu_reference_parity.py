@@ -23,12 +23,16 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.skipif(not os.path.exists(O.REF_BIN), reason="reference CPU factor not built (oracle/_ref)")
-@pytest.mark.parametrize("config", ["grid2d_256_unit", "grid3d_32_sddm"])
+@pytest.mark.parametrize("config", ["grid2d_256_unit", "grid3d_32_sddm",
+                                    pytest.param("grid3d_128_sddm", marks=pytest.mark.slow)])
 def test_statistical_parity_with_reference(config):
+    """grid3d_128_sddm is the benchmark's headline input itself (128^3 SDDM,
+    2,097,152 unknowns); it takes a few minutes of host time."""
     if config == "grid2d_256_unit":
         n, r, c, v, g = R.generate("grid2d", [256, 256], seed=0)
     else:
-        n, r, c, v, g = R.generate("grid3d", [32, 32, 32], wlo=1e-3, whi=1e3, log_weights=True, excess_frac=0.05,
+        side = 128 if config == "grid3d_128_sddm" else 32
+        n, r, c, v, g = R.generate("grid3d", [side] * 3, wlo=1e-3, whi=1e3, log_weights=True, excess_frac=0.05,
                                    excess_lo=0.0, excess_hi=1e-2, seed=2)
     P = OracleProblem(n, r, c, v, trim=g)
     threads = str(max(1, min(os.cpu_count() or 1, 16)))
@@ -45,7 +49,7 @@ def test_statistical_parity_with_reference(config):
                 from helpers import trim_factor
                 f = trim_factor(f, n)
             ref_nnz.append(len(f["rowind"]))
-            _, info = P.pcg(f, b, tol=1e-6)
+            _, info = P.pcg(f, b, tol=1e-6, nthreads=int(threads))
             assert info["converged"]
             ref_its.append(info["iterations"])
     gpu_nnz, gpu_its = [], []
