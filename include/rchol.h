@@ -132,6 +132,26 @@ rchol_status rchol_load_mtx(rchol_ctx* ctx, const char* path, int trim_ground);
 /* Same preprocessing from 0-based host triplets. */
 rchol_status rchol_set_triplets(rchol_ctx* ctx, int n, long long nnz, const int* rows, const int* cols,
                                 const double* vals, int trim_ground);
+/* An SDDM (or a Laplacian) as the reference's physics preprocessing takes
+ * it -- physics_produce, cpu_implementation/write_graph.jl:98-183, run there
+ * offline in Julia -- converted and ordered on the device:
+ *   signs normalised (off-diagonal -|v|, diagonal |v|; a diagonal of
+ *   sum |off| per column appended when the input has none);
+ *   ordering RCHOL_ORDER_NNZ_SORT: a seeded random permutation, then a
+ *   stable sort by column nnz (write_graph.jl:112-128); RCHOL_ORDER_RANDOM:
+ *   the seeded permutation alone; RCHOL_ORDER_GIVEN: the input order;
+ *   ground vertex (write_graph.jl:153-163): when the entries sum to more
+ *   than 1e-9, vertex n is appended with entries -c_j for every column sum
+ *   c_j > 0 and diagonal sum c_j, and the context trims it after factoring
+ *   (*has_ground = 1); a sum below -1e-9 returns RCHOL_ERR_NUMERIC.
+ * rows/cols/vals: nnz 0-based triplets (both triangles), host (on_device =
+ * 0) or device (1).  perm (host, n entries, may be NULL) receives the
+ * position of each input vertex in the context's matrix: right-hand sides
+ * and solutions of the input's numbering map through it. */
+enum { RCHOL_ORDER_GIVEN = 0, RCHOL_ORDER_NNZ_SORT = 1, RCHOL_ORDER_RANDOM = 2 };
+rchol_status rchol_set_sddm(rchol_ctx* ctx, int n, long long nnz, const int* rows, const int* cols,
+                            const double* vals, int on_device, int ordering, unsigned long long order_seed,
+                            int* perm, int* has_ground);
 /* A preprocessed matrix in CSC (== CSR, symmetric, diagonal included), host
  * (on_device = 0) or device (on_device = 1) arrays; copied into the context. */
 rchol_status rchol_set_csc(rchol_ctx* ctx, int n, const int* colptr, const int* rowind, const double* val,

@@ -222,6 +222,105 @@ def generate_grid(kind, dims, wlo=1.0, whi=1.0, log_weights=False, aniso_z=1.0, 
     return n.value, rows, cols, vals, bool(g.value)
 
 
+_M64 = (1 << 64) - 1
+
+
+def _mix64(x):
+    """splitmix64 finaliser on numpy uint64 arrays (wrapping arithmetic)."""
+    x = (x + np.uint64(0x9E3779B97F4A7C15)) & np.uint64(_M64)
+    x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return x ^ (x >> np.uint64(31))
+
+
+def order_keys(n, seed):
+    """The 64-bit ordering key of every vertex: splitmix64 of (seed,
+    stream 4, vertex), the tie-break of the ascending-nnz order."""
+    with np.errstate(over="ignore"):
+        base = _mix64(_mix64(np.array([seed], np.uint64)) ^ np.uint64((4 * 0xD1B54A32D192ED03) & _M64))
+        return _mix64(base ^ np.arange(n, dtype=np.uint64))
+
+
+def sddm_to_laplacian(n, rows, cols, vals, ordering=1, seed=0):
+    """Restatement of the physics preprocessing (cpu_implementation/
+    write_graph.jl:98-183) as rchol_set_sddm performs it: sign
+    normalisation (and a diagonal of sum |off| per column when the input has
+    none), the ordering (0 given, 1 ascending column nnz after the seeded
+    permutation, 2 the seeded permutation), and the ground vertex appended
+    when the entries sum to more than 1e-9.  Column sums are added in row
+    order, the ground diagonal in column order.  Returns
+    (N, colptr, rowind, val, perm, has_ground).  Small inputs only."""
+    rows = np.asarray(rows, np.int64)
+    cols = np.asarray(cols, np.int64)
+    vals = np.asarray(vals, np.float64)
+    v = np.where(rows == cols, np.abs(vals), -np.abs(vals))
+    append_diag = not np.any(rows == cols)
+    cnt = np.bincount(cols, minlength=n)
+    ident = np.arange(n)
+    if ordering == 0:
+        order = ident
+    else:
+        key = order_keys(n, seed)
+        order = np.lexsort((ident, key, cnt)) if ordering == 1 else np.lexsort((ident, key))
+    pos = np.empty(n, np.int64)
+    pos[order] = ident
+    pr, pc = pos[rows], pos[cols]
+    if append_diag:
+        pr = np.concatenate([pr, pos])
+        pc = np.concatenate([pc, pos])
+        v = np.concatenate([v, np.zeros(n)])
+    e = np.lexsort((np.arange(len(pr)), pr, pc))
+    ri, cc, val = pr[e], pc[e], v[e].copy()
+    cp = np.concatenate([[0], np.cumsum(np.bincount(cc, minlength=n))])
+    if append_diag:
+        for j in range(n):
+            s_ = 0.0
+            d = -1
+            for p in range(cp[j], cp[j + 1]):
+                if ri[p] == j:
+                    d = p
+                else:
+                    s_ += abs(val[p])
+            if d >= 0:
+                val[d] = s_
+    csum = np.zeros(n)
+    pos_c = np.zeros(n, bool)
+    for j in range(n):
+        s_ = 0.0
+        a_ = 0.0
+        for p in range(cp[j], cp[j + 1]):
+            s_ += val[p]
+            a_ += abs(val[p])
+        csum[j] = s_
+        # a column sum within the rounding bound of its own sum counts as zero
+        pos_c[j] = s_ > float(cp[j + 1] - cp[j]) * 2.0 ** -52 * a_
+    total = float(np.sum(csum))
+    if total < -1e-9:
+        raise ValueError("not diagonally dominant")
+    if not total > 1e-9:
+        return n, cp.astype(np.int32), ri.astype(np.int32), val, pos.astype(np.int32), False
+    g = np.nonzero(pos_c)[0]
+    gd = 0.0
+    for j in g:
+        gd += csum[j]
+    ncp = [0]
+    nri, nval = [], []
+    for j in range(n):
+        nri.append(ri[cp[j]:cp[j + 1]])
+        nval.append(val[cp[j]:cp[j + 1]])
+        if pos_c[j]:
+            nri.append(np.array([n]))
+            nval.append(np.array([-csum[j]]))
+        ncp.append(ncp[-1] + (cp[j + 1] - cp[j]) + (1 if pos_c[j] else 0))
+    nri.append(g)
+    nval.append(-csum[g])
+    nri.append(np.array([n]))
+    nval.append(np.array([gd]))
+    ncp.append(ncp[-1] + len(g) + 1)
+    return (n + 1, np.array(ncp, np.int32), np.concatenate(nri).astype(np.int32), np.concatenate(nval),
+            pos.astype(np.int32), True)
+
+
 def write_mtx_fast(path, n, rows, cols, vals):
     """write_mtx in C (large inputs)."""
     if lib().orc_write_mtx(path.encode(), n, len(rows), _i32(rows), _i32(cols), _f64(vals)) != 0:

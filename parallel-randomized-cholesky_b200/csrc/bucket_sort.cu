@@ -185,6 +185,11 @@ cudaError_t stable_key_order_carried(const int32_t* key, int32_t n, int32_t nkey
 
 cudaError_t stable_key_order(const int32_t* key, int32_t n, int32_t nkeys, int32_t* order, Scratch& sc,
                              cudaStream_t s) {
+    return stable_key_order_from(key, nullptr, n, nkeys, order, sc, s);
+}
+
+cudaError_t stable_key_order_from(const int32_t* key, const int32_t* in0, int32_t n, int32_t nkeys, int32_t* order,
+                                  Scratch& sc, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     int bits = 0;
     while (bits < 31 && (1ll << bits) < (int64_t)nkeys) ++bits;
@@ -197,8 +202,14 @@ cudaError_t stable_key_order(const int32_t* key, int32_t n, int32_t nkeys, int32
     RCHOL_TRY(sc.get(&offs, nh + 1));
     RCHOL_TRY(sc.get((char**)&tmp, (int64_t)scan_tmp_bytes(nh)));
     if (passes > 1) RCHOL_TRY(sc.get(&buf, n));
-    // ping-pong so that the last pass writes `order`
-    const int32_t* in = nullptr;
+    // ping-pong so that the last pass writes `order` (which may alias in0)
+    if (in0 && in0 == order) {
+        int32_t* copy = nullptr;
+        RCHOL_TRY(sc.get(&copy, n));
+        RCHOL_TRY(cudaMemcpyAsync(copy, in0, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+        in0 = copy;
+    }
+    const int32_t* in = in0;
     for (int p = 0; p < passes; ++p) {
         int32_t* out = ((passes - 1 - p) % 2 == 0) ? order : buf;
         radix_hist_kernel<<<ntiles, kSortThreads, 0, s>>>(key, in, n, 8 * p, ntiles, hist);

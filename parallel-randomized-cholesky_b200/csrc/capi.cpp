@@ -448,6 +448,53 @@ extern "C" rchol_status rchol_set_triplets(rchol_ctx* ctx, int n, long long nnz,
     return install_host_csc(ctx, h, trim_ground);
 }
 
+extern "C" rchol_status rchol_set_sddm(rchol_ctx* ctx, int n, long long nnz, const int* rows, const int* cols,
+                                       const double* vals, int on_device, int ordering, unsigned long long order_seed,
+                                       int* perm, int* has_ground) {
+    if (!ctx || n <= 0 || nnz < 0 || (nnz > 0 && (!rows || !cols || !vals)))
+        return fail(ctx, RCHOL_ERR_INVALID, "bad triplet arguments");
+    if (ordering != RCHOL_ORDER_GIVEN && ordering != RCHOL_ORDER_NNZ_SORT && ordering != RCHOL_ORDER_RANDOM)
+        return fail(ctx, RCHOL_ERR_INVALID, "ordering must be RCHOL_ORDER_GIVEN, _NNZ_SORT or _RANDOM");
+    if (nnz + 2 * (long long)n + 2 >= (long long)INT32_MAX)
+        return fail(ctx, RCHOL_ERR_INVALID, "matrix too large for int32 indices");
+    cudaSetDevice(ctx->device);
+    if (!on_device) {
+        for (long long k = 0; k < nnz; ++k)
+            if (!std::isfinite(vals[k])) return fail(ctx, RCHOL_ERR_NUMERIC, "non-finite matrix entry");
+    }
+    struct Release {
+        rchol::Scratch& sc;
+        ~Release() { sc.reset(); }
+    } release{ctx->scratch};
+    const int32_t* drows = rows;
+    const int32_t* dcols = cols;
+    const double* dvals = vals;
+    if (!on_device) {
+        int32_t *r = nullptr, *c = nullptr;
+        double* v = nullptr;
+        CK(ctx->scratch.get(&r, nnz), "alloc triplets");
+        CK(ctx->scratch.get(&c, nnz), "alloc triplets");
+        CK(ctx->scratch.get(&v, nnz), "alloc triplets");
+        if (nnz > 0) {
+            CK(cudaMemcpyAsync(r, rows, sizeof(int32_t) * (size_t)nnz, cudaMemcpyHostToDevice, ctx->stream), "upload");
+            CK(cudaMemcpyAsync(c, cols, sizeof(int32_t) * (size_t)nnz, cudaMemcpyHostToDevice, ctx->stream), "upload");
+            CK(cudaMemcpyAsync(v, vals, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice, ctx->stream), "upload");
+        }
+        drows = r;
+        dcols = c;
+        dvals = v;
+    }
+    rchol::SddmResult res;
+    CK(rchol::sddm_to_laplacian(n, nnz, drows, dcols, dvals, ordering, order_seed, ctx->scratch, ctx->stream, res),
+       "sddm conversion");
+    if (res.status == rchol::SddmResult::kBadIndex) return fail(ctx, RCHOL_ERR_INVALID, "triplet index out of range");
+    if (res.status == rchol::SddmResult::kNotDominant)
+        return fail(ctx, RCHOL_ERR_NUMERIC, "not diagonally dominant: the entries sum to " + std::to_string(res.total));
+    if (perm) CK(cudaMemcpy(perm, res.perm, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost), "copy permutation");
+    if (has_ground) *has_ground = res.ground ? 1 : 0;
+    return rchol_set_csc(ctx, res.n, res.colptr, res.rowind, res.val, 1, res.ground ? 1 : 0);
+}
+
 extern "C" rchol_status rchol_load_mtx(rchol_ctx* ctx, const char* path, int trim_ground) {
     if (!ctx || !path) return fail(ctx, RCHOL_ERR_INVALID, "null path");
     rchol::Triplets t;

@@ -287,10 +287,38 @@ cudaError_t max_i32(const int32_t* v, int64_t n, int32_t* out, cudaStream_t s);
 // equal keys keep ascending index order (bucket_sort.cu).
 cudaError_t stable_key_order(const int32_t* key, int32_t n, int32_t nkeys, int32_t* order, Scratch& sc,
                              cudaStream_t s);
+// The same, stably re-sorting the items in the order `in` (a permutation of
+// 0..n-1; null = identity) by key: chained calls sort by several keys, the
+// last call's key being the most significant.  `order` may alias `in`.
+cudaError_t stable_key_order_from(const int32_t* key, const int32_t* in, int32_t n, int32_t nkeys, int32_t* order,
+                                  Scratch& sc, cudaStream_t s);
 // The same order with the keys moved along with the items in every pass
 // (sequential key reads; two extra key buffers of scratch): for large n.
 cudaError_t stable_key_order_carried(const int32_t* key, int32_t n, int32_t nkeys, int32_t* order, Scratch& sc,
                                      cudaStream_t s);
+
+// ---- SDDM -> ordered Laplacian (ordering.cu) ------------------------------
+constexpr int kOrderGiven = 0, kOrderNnzSort = 1, kOrderRandom = 2;
+// A converted matrix: CSC (rows ascending per column, duplicates kept) in
+// the scratch arena, and the position of each input vertex.
+struct SddmResult {
+    enum { kOk = 0, kBadIndex = 1, kNotDominant = 2 };
+    int status = kOk;
+    int32_t n = 0;              // input n, plus one with a ground vertex
+    int64_t nnz = 0;
+    bool ground = false;
+    double total = 0.0;         // sum of every entry (before the ground vertex)
+    int32_t* colptr = nullptr;  // device, scratch
+    int32_t* rowind = nullptr;
+    double* val = nullptr;
+    int32_t* perm = nullptr;    // device [input n]: new index of input vertex i
+};
+// Device triplets (0-based, both triangles) of an SDDM or Laplacian: signs
+// normalised, ordered (kOrder*; `seed` keys the random permutation), and a
+// ground vertex appended when the entries sum to more than 1e-9
+// (write_graph.jl:98-183).  Synchronises `s`.
+cudaError_t sddm_to_laplacian(int32_t n, int64_t nnz, const int32_t* rows, const int32_t* cols, const double* vals,
+                              int ordering, uint64_t seed, Scratch& sc, cudaStream_t s, SddmResult& res);
 
 // ---- scans (scan.cu) -------------------------------------------------------
 // out[0] = 0, out[i+1] = sum(in[0..i]); out has n+1 entries.  Uses `tmp`

@@ -23,6 +23,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "i/o error", 3: "CUDA error", 4: "c
           5: "timeout", 6: "not converged", 7: "no CUDA device", 8: "numeric", 9: "no matrix"}
 PREC_FP64, PREC_FP32_FACTOR = 0, 1
 STOP_RELRES, STOP_PRECOND, STOP_ABS_R2 = 0, 1, 2
+ORDER_GIVEN, ORDER_NNZ_SORT, ORDER_RANDOM = 0, 1, 2
 SPMV_AUTO, SPMV_CSR = 0, 1
 
 # every symbol include/rchol.h declares
@@ -33,7 +34,7 @@ EXPORTS = sorted([
     "rchol_factor_copy_to_host", "rchol_factor_write", "rchol_factor_read", "rchol_factor_from_csr_upper",
     "rchol_factor_free", "rchol_pcg_solve", "rchol_precond_apply", "rchol_precond_apply_noalloc", "rchol_profile_solve", "rchol_spmv", "rchol_factorization_driver",
     "rchol_prepare_and_solve", "rchol_generate", "rchol_free_host", "rchol_write_mtx", "rchol_batch_set",
-    "rchol_batch_solve", "rchol_zero_sum_vector",
+    "rchol_batch_solve", "rchol_zero_sum_vector", "rchol_set_sddm",
 ])
 
 
@@ -133,6 +134,8 @@ def lib():
         L.rchol_free_host.restype = None
         L.rchol_write_mtx.argtypes = [C.c_char_p, C.c_int, C.c_longlong, vp, vp, vp]
         L.rchol_zero_sum_vector.argtypes = [C.c_int, C.c_uint, vp]
+        L.rchol_set_sddm.argtypes = [vp, C.c_int, C.c_longlong, vp, vp, vp, C.c_int, C.c_int, C.c_ulonglong, vp,
+                                     i32p]
         L.rchol_batch_set.argtypes = [vp, C.c_int, C.POINTER(System), C.POINTER(C.c_longlong)]
         L.rchol_batch_solve.argtypes = [vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, C.POINTER(SolveInfo),
                                         C.POINTER(SolveInfo)]
@@ -309,6 +312,19 @@ class Context:
         vals = np.ascontiguousarray(vals, np.float64)
         _check(lib().rchol_set_triplets(self.h, n, len(rows), _ptr(rows), _ptr(cols), _ptr(vals),
                                         int(trim_ground)), self.h)
+
+    def set_sddm(self, n, rows, cols, vals, ordering=ORDER_NNZ_SORT, order_seed=0):
+        """An SDDM or Laplacian converted and ordered on the device
+        (rchol_set_sddm).  Returns (perm, has_ground): perm[i] = position of
+        input vertex i in the context's matrix."""
+        rows = np.ascontiguousarray(rows, np.int32)
+        cols = np.ascontiguousarray(cols, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        perm = np.zeros(n, np.int32)
+        g = C.c_int(0)
+        _check(lib().rchol_set_sddm(self.h, n, len(rows), _ptr(rows), _ptr(cols), _ptr(vals), 0, int(ordering),
+                                    int(order_seed), _ptr(perm), C.byref(g)), self.h)
+        return perm, bool(g.value)
 
     def set_csc(self, n, colptr, rowind, val, trim_ground=False, on_device=False):
         if on_device:

@@ -208,3 +208,29 @@ def test_bench_arms_share_the_input():
     Wp = B.build_workload(cfg, product=True)
     Wo = B.build_workload(cfg, product=False)
     assert B.workload_config(cfg, Wp) == B.workload_config(cfg, Wo)
+
+
+@pytest.mark.parametrize("kind,dims,kw", [
+    ("grid3d", [9, 8, 7], dict(wlo=1e-3, whi=1e3, log_weights=True, excess_frac=0.05, excess_lo=0.0, excess_hi=1e-2,
+                               seed=2)),
+    ("grid3d27", [6, 7, 5], dict(wlo=0.1, whi=10.0, log_weights=True, aniso_z=100.0, excess_frac=1.0,
+                                 excess_lo=1e-4, excess_hi=1e-4, seed=5)),
+    ("grid2d", [15, 13], dict(seed=5)),
+])
+def test_sddm_conversion_oracle_matches_generator(kind, dims, kw):
+    """The oracle's restatement of the physics preprocessing (write_graph.jl:
+    98-183), applied to the natural-order SDDM, gives the generator's ordered
+    Laplacian: same order, same pattern, ground values within rounding (the
+    generator knows each excess, the conversion recovers it as a column sum)."""
+    nN, rN, cN, vN, gN = R.generate(kind, dims, ordering=2, **kw)
+    n0, r0, c0, v0, g0 = R.generate(kind, dims, ordering=0, **kw)
+    if gN:  # strip the natural-order ground vertex: back to the SDDM
+        m = (rN < nN - 1) & (cN < nN - 1)
+        rN, cN, vN, n = rN[m], cN[m], vN[m], nN - 1
+    else:
+        n = nN
+    N, cp, ri, val, perm, g = O.sddm_to_laplacian(n, rN, cN, vN, 1, kw["seed"])
+    cp0, ri0, val0 = O.triplets_to_csc(n0, r0, c0, v0)
+    assert N == n0 and g == g0
+    assert np.array_equal(cp, cp0) and np.array_equal(ri, ri0)
+    np.testing.assert_allclose(val, val0, rtol=1e-10, atol=0)
