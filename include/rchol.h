@@ -164,6 +164,20 @@ rchol_status rchol_csc_from_triplets(int n, long long nnz, const int* rows, cons
 /* Host-only MatrixMarket read (0-based triplets, symmetric files generalised);
  * arrays are malloc'ed, release them with rchol_free_host. */
 rchol_status rchol_read_mtx(const char* path, int* n, long long* nnz, int** rows, int** cols, double** vals);
+/* Binary matrix cache: a preprocessed CSC with its trim flag, read back with
+ * one read per array instead of a text parse (the reference reads text
+ * MatrixMarket only, gpu_implementation/pre_process.hpp:322-356).  Layout:
+ * "RCHOLCSC", uint32 version 1, int32 trim flag, int64 n, int64 nnz, int32
+ * colptr[n+1], int32 rowind[nnz], float64 val[nnz], host byte order.
+ * rchol_write_bin / rchol_read_bin are host-only (read_bin's arrays are
+ * malloc'ed: release them with rchol_free_host); rchol_save_bin writes the
+ * context's matrix and rchol_load_bin installs a file as rchol_set_csc does. */
+rchol_status rchol_write_bin(const char* path, int n, const int* colptr, const int* rowind, const double* val,
+                             int trim_ground);
+rchol_status rchol_read_bin(const char* path, int* n, long long* nnz, int** colptr, int** rowind, double** val,
+                            int* trim_ground);
+rchol_status rchol_save_bin(const rchol_ctx* ctx, const char* path);
+rchol_status rchol_load_bin(rchol_ctx* ctx, const char* path);
 /* n and nnz of the loaded matrix (before trimming). */
 rchol_status rchol_matrix_info(const rchol_ctx* ctx, int* n, long long* nnz);
 /* Copy the preprocessed CSC back to the host (sizes from rchol_matrix_info). */

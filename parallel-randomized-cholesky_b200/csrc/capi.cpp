@@ -495,6 +495,64 @@ extern "C" rchol_status rchol_set_sddm(rchol_ctx* ctx, int n, long long nnz, con
     return rchol_set_csc(ctx, res.n, res.colptr, res.rowind, res.val, 1, res.ground ? 1 : 0);
 }
 
+extern "C" rchol_status rchol_write_bin(const char* path, int n, const int* colptr, const int* rowind,
+                                        const double* val, int trim_ground) {
+    if (!path || n <= 0 || !colptr || !rowind || !val) return RCHOL_ERR_INVALID;
+    std::string err;
+    return rchol::write_csc_bin(path, n, colptr, rowind, val, trim_ground, err) ? RCHOL_OK : RCHOL_ERR_IO;
+}
+
+extern "C" rchol_status rchol_read_bin(const char* path, int* n, long long* nnz, int** colptr, int** rowind,
+                                       double** val, int* trim_ground) {
+    if (!path || !n || !nnz || !colptr || !rowind || !val) return RCHOL_ERR_INVALID;
+    rchol::HostCsc h;
+    int trim = 0;
+    std::string err;
+    if (!rchol::read_csc_bin(path, h, trim, err)) return RCHOL_ERR_IO;
+    const size_t nz = h.rowind.size();
+    *colptr = (int*)std::malloc(sizeof(int) * ((size_t)h.n + 1));
+    *rowind = (int*)std::malloc(sizeof(int) * std::max<size_t>(nz, 1));
+    *val = (double*)std::malloc(sizeof(double) * std::max<size_t>(nz, 1));
+    if (!*colptr || !*rowind || !*val) {
+        std::free(*colptr);
+        std::free(*rowind);
+        std::free(*val);
+        return RCHOL_ERR_CAPACITY;
+    }
+    std::memcpy(*colptr, h.colptr.data(), sizeof(int) * ((size_t)h.n + 1));
+    std::memcpy(*rowind, h.rowind.data(), sizeof(int) * nz);
+    std::memcpy(*val, h.val.data(), sizeof(double) * nz);
+    *n = h.n;
+    *nnz = (long long)nz;
+    if (trim_ground) *trim_ground = trim;
+    return RCHOL_OK;
+}
+
+extern "C" rchol_status rchol_load_bin(rchol_ctx* ctx, const char* path) {
+    if (!ctx || !path) return fail(ctx, RCHOL_ERR_INVALID, "null path");
+    rchol::HostCsc h;
+    int trim = 0;
+    std::string err;
+    if (!rchol::read_csc_bin(path, h, trim, err)) return fail(ctx, RCHOL_ERR_IO, err);
+    return install_host_csc(ctx, h, trim);
+}
+
+extern "C" rchol_status rchol_save_bin(const rchol_ctx* ctx, const char* path) {
+    if (!ctx || !path) return RCHOL_ERR_INVALID;
+    if (!ctx->have) return RCHOL_ERR_NO_MATRIX;
+    cudaSetDevice(ctx->device);
+    std::vector<int32_t> cp((size_t)ctx->A.n + 1), ri((size_t)ctx->A.nnz);
+    std::vector<double> v((size_t)ctx->A.nnz);
+    if (cudaMemcpy(cp.data(), ctx->A.colptr, sizeof(int32_t) * cp.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(ri.data(), ctx->A.rowind, sizeof(int32_t) * ri.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(v.data(), ctx->A.val, sizeof(double) * v.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return RCHOL_ERR_CUDA;
+    std::string err;
+    return rchol::write_csc_bin(path, ctx->A.n, cp.data(), ri.data(), v.data(), ctx->trim ? 1 : 0, err)
+               ? RCHOL_OK
+               : RCHOL_ERR_IO;
+}
+
 extern "C" rchol_status rchol_load_mtx(rchol_ctx* ctx, const char* path, int trim_ground) {
     if (!ctx || !path) return fail(ctx, RCHOL_ERR_INVALID, "null path");
     rchol::Triplets t;

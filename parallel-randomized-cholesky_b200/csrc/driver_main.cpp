@@ -45,6 +45,7 @@ bool parse_extra(const char* a, rchol_opts& o, int& k) {
     else if (key == "warps") o.warps_per_block = std::atoi(v.c_str());
     else if (key == "unroll") o.unroll = std::atoi(v.c_str());
     else if (key == "timeout") o.timeout_s = std::atof(v.c_str());
+    else if (key == "sddm" || key == "order_seed") return true;  // read by main
     else return false;
     return true;
 }
@@ -105,11 +106,40 @@ int main(int argc, char** argv) {
     }
     const int solve = mode < 2 ? std::atoi(pos[2]) : 1;
     const int trim = mode == 1 ? 1 : (mode == 2 ? (pos.size() > 3) : 0);
+    // --sddm=nnz|random|given: the input is an SDDM (or Laplacian) in its own
+    // order, converted and ordered on the device as write_graph.jl does
+    // offline; a .rchb input is the binary matrix cache
+    int sddm = -1;
+    unsigned long long order_seed = 0;
+    for (int i = 1; i < argc; ++i) {
+        if (std::strncmp(argv[i], "--sddm=", 7) == 0) {
+            const std::string m = argv[i] + 7;
+            sddm = m == "random" ? RCHOL_ORDER_RANDOM : (m == "given" ? RCHOL_ORDER_GIVEN : RCHOL_ORDER_NNZ_SORT);
+        } else if (std::strncmp(argv[i], "--order_seed=", 13) == 0) {
+            order_seed = std::strtoull(argv[i] + 13, nullptr, 10);
+        }
+    }
     rchol_ctx* ctx = nullptr;
     rchol_status s = rchol_create(&ctx, &o);
     if (s != RCHOL_OK) return die(nullptr, s, "create");
     std::printf("problem: %s\n", path);
-    s = rchol_load_mtx(ctx, path, trim);
+    const size_t plen = std::strlen(path);
+    if (plen > 5 && std::strcmp(path + plen - 5, ".rchb") == 0) {
+        s = rchol_load_bin(ctx, path);
+    } else if (sddm >= 0) {
+        int n0 = 0, has_ground = 0;
+        long long nz0 = 0;
+        int *rr = nullptr, *cc = nullptr;
+        double* vv = nullptr;
+        s = rchol_read_mtx(path, &n0, &nz0, &rr, &cc, &vv);
+        if (s == RCHOL_OK) s = rchol_set_sddm(ctx, n0, nz0, rr, cc, vv, 0, sddm, order_seed, nullptr, &has_ground);
+        rchol_free_host(rr);
+        rchol_free_host(cc);
+        rchol_free_host(vv);
+        if (s == RCHOL_OK) std::printf("converted on the device: %s ground vertex\n", has_ground ? "with" : "no");
+    } else {
+        s = rchol_load_mtx(ctx, path, trim);
+    }
     if (s != RCHOL_OK) return die(ctx, s, "load");
     int n = 0;
     long long nnz = 0;

@@ -2,6 +2,7 @@
 #include "host_io.h"
 
 #include <algorithm>
+#include <climits>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
@@ -10,6 +11,8 @@
 #include <fstream>
 #include <numeric>
 #include <sstream>
+
+#include <omp.h>
 
 namespace rchol {
 
@@ -102,34 +105,88 @@ bool read_mtx(const std::string& path, Triplets& t, std::string& err) {
         return false;
     }
     t.n = (int32_t)nr;
+    size_t reserve = (size_t)nz * (sym ? 2 : 1);
     t.rows.clear();
     t.cols.clear();
     t.vals.clear();
-    size_t reserve = (size_t)nz * (sym ? 2 : 1);
     t.rows.reserve(reserve);
     t.cols.reserve(reserve);
     t.vals.reserve(reserve);
-    for (long long k = 0; k < nz; ++k) {
-        long long r = std::strtoll(p, &q, 10);
-        if (q == p) {
-            err = path + ": truncated entry list";
-            return false;
+    t.rows.resize((size_t)nz);
+    t.cols.resize((size_t)nz);
+    t.vals.resize((size_t)nz);
+    // The entry lines are parsed in parallel: the body is cut into
+    // line-aligned chunks, each chunk counts its entry lines, and a prefix
+    // sum gives every chunk its first entry, so the entries keep file order.
+    while (p < end && *p != '\n') ++p;  // rest of the size line
+    const char* body = p;
+    const int nchunks = std::max(1, std::min(omp_get_max_threads() * 4, (int)((end - body) / 65536) + 1));
+    std::vector<const char*> cut((size_t)nchunks + 1, end);
+    cut[0] = body;
+    for (int c = 1; c < nchunks; ++c) {
+        const char* q0 = body + (end - body) * c / nchunks;
+        if (q0 < cut[(size_t)c - 1]) q0 = cut[(size_t)c - 1];
+        while (q0 < end && *q0 != '\n') ++q0;
+        cut[(size_t)c] = q0;
+    }
+    auto entry_line = [](const char* a, const char* b) {
+        while (a < b && (*a == ' ' || *a == '\t' || *a == '\r' || *a == '\n')) ++a;
+        return a < b && *a != '%';
+    };
+    std::vector<long long> first((size_t)nchunks + 1, 0);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int c = 0; c < nchunks; ++c) {
+        long long cnt = 0;
+        for (const char* a = cut[(size_t)c]; a < cut[(size_t)c + 1];) {
+            const char* e = (const char*)std::memchr(a, '\n', (size_t)(cut[(size_t)c + 1] - a));
+            if (!e) e = cut[(size_t)c + 1];
+            if (entry_line(a, e)) ++cnt;
+            a = e + 1;
         }
-        p = q;
-        long long c = std::strtoll(p, &q, 10);
-        p = q;
-        double v = 1.0;
-        if (!pattern) {
-            v = std::strtod(p, &q);
-            p = q;
+        first[(size_t)c + 1] = cnt;
+    }
+    for (int c = 0; c < nchunks; ++c) first[(size_t)c + 1] += first[(size_t)c];
+    if (first[(size_t)nchunks] < nz) {
+        err = path + ": truncated entry list";
+        return false;
+    }
+    int bad = 0;  // 1: malformed entry, 2: index out of range
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : bad)
+    for (int c = 0; c < nchunks; ++c) {
+        long long k = first[(size_t)c];
+        char* qq = nullptr;
+        for (const char* a = cut[(size_t)c]; a < cut[(size_t)c + 1] && k < nz;) {
+            const char* e = (const char*)std::memchr(a, '\n', (size_t)(cut[(size_t)c + 1] - a));
+            if (!e) e = cut[(size_t)c + 1];
+            if (entry_line(a, e)) {
+                const char* z = a;
+                long long r = std::strtoll(z, &qq, 10);
+                if (qq == z) bad |= 1;
+                z = qq;
+                long long cc = std::strtoll(z, &qq, 10);
+                if (qq == z) bad |= 1;
+                z = qq;
+                double v = 1.0;
+                if (!pattern) {
+                    v = std::strtod(z, &qq);
+                    if (qq == z) bad |= 1;
+                }
+                if (r < 1 || r > nr || cc < 1 || cc > nc) bad |= 2;
+                t.rows[(size_t)k] = (int32_t)(r - 1);
+                t.cols[(size_t)k] = (int32_t)(cc - 1);
+                t.vals[(size_t)k] = v;
+                ++k;
+            }
+            a = e + 1;
         }
-        if (r < 1 || r > nr || c < 1 || c > nc) {
-            err = path + ": index out of range";
-            return false;
-        }
-        t.rows.push_back((int32_t)(r - 1));
-        t.cols.push_back((int32_t)(c - 1));
-        t.vals.push_back(v);
+    }
+    if (bad & 1) {
+        err = path + ": truncated entry list";
+        return false;
+    }
+    if (bad & 2) {
+        err = path + ": index out of range";
+        return false;
     }
     if (sym) {
         size_t base = t.rows.size();
@@ -233,6 +290,75 @@ bool triplets_to_csc(const Triplets& t, HostCsc& out, std::string& err) {
     return true;
 }
 
+namespace {
+constexpr char kBinMagic[8] = {'R', 'C', 'H', 'O', 'L', 'C', 'S', 'C'};
+}
+
+bool write_csc_bin(const std::string& path, int32_t n, const int32_t* colptr, const int32_t* rowind,
+                   const double* val, int trim, std::string& err) {
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) {
+        err = "cannot write " + path + ": " + std::strerror(errno);
+        return false;
+    }
+    const uint32_t version = 1;
+    const int32_t tr = trim ? 1 : 0;
+    const int64_t n64 = n, nnz = colptr[n];
+    bool ok = std::fwrite(kBinMagic, 1, 8, f) == 8 && std::fwrite(&version, 4, 1, f) == 1 &&
+              std::fwrite(&tr, 4, 1, f) == 1 && std::fwrite(&n64, 8, 1, f) == 1 && std::fwrite(&nnz, 8, 1, f) == 1;
+    ok = ok && std::fwrite(colptr, 4, (size_t)n + 1, f) == (size_t)n + 1;
+    ok = ok && std::fwrite(rowind, 4, (size_t)nnz, f) == (size_t)nnz;
+    ok = ok && std::fwrite(val, 8, (size_t)nnz, f) == (size_t)nnz;
+    if (std::fclose(f) != 0 || !ok) {
+        err = "write failed on " + path;
+        return false;
+    }
+    return true;
+}
+
+bool read_csc_bin(const std::string& path, HostCsc& out, int& trim, std::string& err) {
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) {
+        err = "cannot open " + path + ": " + std::strerror(errno);
+        return false;
+    }
+    char magic[8];
+    uint32_t version = 0;
+    int32_t tr = 0;
+    int64_t n = 0, nnz = 0;
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kBinMagic, 8) == 0 &&
+              std::fread(&version, 4, 1, f) == 1 && version == 1 && std::fread(&tr, 4, 1, f) == 1 &&
+              std::fread(&n, 8, 1, f) == 1 && std::fread(&nnz, 8, 1, f) == 1 && n > 0 && n <= INT32_MAX &&
+              nnz >= 0 && nnz <= INT32_MAX;
+    if (!ok) {
+        std::fclose(f);
+        err = path + ": not a binary matrix file of version 1";
+        return false;
+    }
+    out.n = (int32_t)n;
+    out.colptr.resize((size_t)n + 1);
+    out.rowind.resize((size_t)nnz);
+    out.val.resize((size_t)nnz);
+    ok = std::fread(out.colptr.data(), 4, (size_t)n + 1, f) == (size_t)n + 1 &&
+         std::fread(out.rowind.data(), 4, (size_t)nnz, f) == (size_t)nnz &&
+         std::fread(out.val.data(), 8, (size_t)nnz, f) == (size_t)nnz;
+    std::fclose(f);
+    if (!ok) {
+        err = "short read on " + path;
+        return false;
+    }
+    // structure checks: monotone pointers ending at nnz, indices in range
+    if (out.colptr[0] != 0 || out.colptr[(size_t)n] != nnz) ok = false;
+    for (int64_t j = 0; j < n && ok; ++j) ok = out.colptr[(size_t)j] <= out.colptr[(size_t)j + 1];
+    for (int64_t k = 0; k < nnz && ok; ++k) ok = out.rowind[(size_t)k] >= 0 && out.rowind[(size_t)k] < n;
+    if (!ok) {
+        err = path + ": corrupt matrix structure";
+        return false;
+    }
+    trim = tr;
+    return true;
+}
+
 bool write_factor_files(const std::string& prefix, int32_t n, const std::vector<int64_t>& colptr,
                         const std::vector<int32_t>& rowind, const std::vector<double>& val,
                         const std::vector<double>& diag, std::string& err) {
@@ -244,24 +370,34 @@ bool write_factor_files(const std::string& prefix, int32_t n, const std::vector<
     }
     const long long nnz = (long long)colptr[(size_t)n] + n;
     std::fprintf(f, "%%%%MatrixMarket matrix coordinate real general\n%d %d %lld\n", n, n, nnz);
-    std::vector<char> buf;
-    buf.reserve(1 << 22);
-    char line[96];
-    auto put = [&](long long r, long long c, double v) {
-        int len = std::snprintf(line, sizeof(line), "%lld %lld %.16g\n", r, c, v);
-        buf.insert(buf.end(), line, line + len);
-        if (buf.size() > (1u << 22) - 128) {
-            std::fwrite(buf.data(), 1, buf.size(), f);
-            buf.clear();
+    // columns are formatted in parallel, a block of columns per buffer, and
+    // the buffers written in column order
+    const int32_t block = 16384;
+    const int32_t nblocks = (n + block - 1) / block;
+    bool ok = true;
+    for (int32_t b0 = 0; b0 < nblocks && ok; b0 += 64) {
+        const int32_t b1 = std::min(nblocks, b0 + 64);
+        std::vector<std::string> out((size_t)(b1 - b0));
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int32_t b = b0; b < b1; ++b) {
+            std::string& o = out[(size_t)(b - b0)];
+            char line[96];
+            const int32_t j0 = b * block, j1 = std::min(n, j0 + block);
+            o.reserve((size_t)(colptr[(size_t)j1] - colptr[(size_t)j0] + (j1 - j0)) * 36);
+            for (int32_t j = j0; j < j1; ++j) {
+                int len = std::snprintf(line, sizeof(line), "%d %d 1\n", j + 1, j + 1);  // unit diagonal first
+                o.append(line, (size_t)len);
+                for (int64_t p = colptr[(size_t)j]; p < colptr[(size_t)j + 1]; ++p) {
+                    len = std::snprintf(line, sizeof(line), "%d %d %.16g\n", rowind[(size_t)p] + 1, j + 1,
+                                        val[(size_t)p]);
+                    o.append(line, (size_t)len);
+                }
+            }
         }
-    };
-    for (int32_t j = 0; j < n; ++j) {
-        put(j + 1, j + 1, 1.0);  // unit diagonal first: rows ascending
-        for (int64_t p = colptr[(size_t)j]; p < colptr[(size_t)j + 1]; ++p)
-            put((long long)rowind[(size_t)p] + 1, j + 1, val[(size_t)p]);
+        for (const std::string& o : out)
+            if (std::fwrite(o.data(), 1, o.size(), f) != o.size()) ok = false;
     }
-    std::fwrite(buf.data(), 1, buf.size(), f);
-    if (std::fclose(f) != 0) {
+    if (std::fclose(f) != 0 || !ok) {
         err = "write failed on " + lpath;
         return false;
     }

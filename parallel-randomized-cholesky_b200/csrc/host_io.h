@@ -28,6 +28,14 @@ bool read_mtx(const std::string& path, Triplets& t, std::string& err);
 bool write_mtx(const std::string& path, int32_t n, int64_t nnz, const int32_t* rows, const int32_t* cols,
                const double* vals, std::string& err);
 
+// Binary matrix cache (a preprocessed CSC, read with one fread per array):
+// magic "RCHOLCSC", uint32 version 1, int32 trim flag, int64 n, int64 nnz,
+// then colptr (int32, n+1), rowind (int32, nnz), val (float64, nnz), in the
+// host's byte order (little-endian on the supported hosts).
+bool write_csc_bin(const std::string& path, int32_t n, const int32_t* colptr, const int32_t* rowind,
+                   const double* val, int trim, std::string& err);
+bool read_csc_bin(const std::string& path, HostCsc& out, int& trim, std::string& err);
+
 // sparse_matrix_processor preprocessing (pre_process.hpp:189-306, 338-356):
 // off-diagonals -> -|v|, diagonal -> |v|, diagonal appended as the column
 // sum of |off-diagonals| when the input has none, CSC sorted by (col,row),

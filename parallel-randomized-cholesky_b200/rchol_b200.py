@@ -34,7 +34,8 @@ EXPORTS = sorted([
     "rchol_factor_copy_to_host", "rchol_factor_write", "rchol_factor_read", "rchol_factor_from_csr_upper",
     "rchol_factor_free", "rchol_pcg_solve", "rchol_precond_apply", "rchol_precond_apply_noalloc", "rchol_profile_solve", "rchol_spmv", "rchol_factorization_driver",
     "rchol_prepare_and_solve", "rchol_generate", "rchol_free_host", "rchol_write_mtx", "rchol_batch_set",
-    "rchol_batch_solve", "rchol_zero_sum_vector", "rchol_set_sddm",
+    "rchol_batch_solve", "rchol_zero_sum_vector", "rchol_set_sddm", "rchol_write_bin", "rchol_read_bin",
+    "rchol_save_bin", "rchol_load_bin",
 ])
 
 
@@ -134,6 +135,11 @@ def lib():
         L.rchol_free_host.restype = None
         L.rchol_write_mtx.argtypes = [C.c_char_p, C.c_int, C.c_longlong, vp, vp, vp]
         L.rchol_zero_sum_vector.argtypes = [C.c_int, C.c_uint, vp]
+        L.rchol_write_bin.argtypes = [C.c_char_p, C.c_int, vp, vp, vp, C.c_int]
+        L.rchol_read_bin.argtypes = [C.c_char_p, i32p, i64p, C.POINTER(i32p), C.POINTER(i32p), C.POINTER(f64p),
+                                     i32p]
+        L.rchol_save_bin.argtypes = [vp, C.c_char_p]
+        L.rchol_load_bin.argtypes = [vp, C.c_char_p]
         L.rchol_set_sddm.argtypes = [vp, C.c_int, C.c_longlong, vp, vp, vp, C.c_int, C.c_int, C.c_ulonglong, vp,
                                      i32p]
         L.rchol_batch_set.argtypes = [vp, C.c_int, C.POINTER(System), C.POINTER(C.c_longlong)]
@@ -221,6 +227,31 @@ def read_mtx(path):
            np.ctypeslib.as_array(v, shape=(m,)).copy())
     for p in (r, c, v):
         L.rchol_free_host(C.cast(p, C.c_void_p))
+    return out
+
+
+def write_bin(path, n, colptr, rowind, val, trim_ground=False):
+    """Binary matrix cache of a preprocessed CSC (rchol_write_bin)."""
+    colptr = np.ascontiguousarray(colptr, np.int32)
+    rowind = np.ascontiguousarray(rowind, np.int32)
+    val = np.ascontiguousarray(val, np.float64)
+    _check(lib().rchol_write_bin(path.encode(), n, _ptr(colptr), _ptr(rowind), _ptr(val), int(trim_ground)))
+
+
+def read_bin(path):
+    """(n, colptr, rowind, val, trim_ground) of a binary matrix cache."""
+    L = lib()
+    n, nnz, tr = C.c_int(), C.c_longlong(), C.c_int()
+    cp, ri, v = C.POINTER(C.c_int)(), C.POINTER(C.c_int)(), C.POINTER(C.c_double)()
+    _check(L.rchol_read_bin(path.encode(), C.byref(n), C.byref(nnz), C.byref(cp), C.byref(ri), C.byref(v),
+                            C.byref(tr)))
+    try:
+        out = (n.value, np.ctypeslib.as_array(cp, (n.value + 1,)).copy(),
+               np.ctypeslib.as_array(ri, (max(nnz.value, 1),))[:nnz.value].copy(),
+               np.ctypeslib.as_array(v, (max(nnz.value, 1),))[:nnz.value].copy(), bool(tr.value))
+    finally:
+        for p in (cp, ri, v):
+            L.rchol_free_host(C.cast(p, C.c_void_p))
     return out
 
 
@@ -325,6 +356,12 @@ class Context:
         _check(lib().rchol_set_sddm(self.h, n, len(rows), _ptr(rows), _ptr(cols), _ptr(vals), 0, int(ordering),
                                     int(order_seed), _ptr(perm), C.byref(g)), self.h)
         return perm, bool(g.value)
+
+    def load_bin(self, path):
+        _check(lib().rchol_load_bin(self.h, path.encode()), self.h)
+
+    def save_bin(self, path):
+        _check(lib().rchol_save_bin(self.h, path.encode()), self.h)
 
     def set_csc(self, n, colptr, rowind, val, trim_ground=False, on_device=False):
         if on_device:

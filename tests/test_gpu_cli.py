@@ -66,3 +66,26 @@ def test_factorization_driver_entry_point():
     L = R.lib()
     st = L.rchol_factorization_driver(os.path.join(GOLDEN, "grid12_unit.mtx").encode(), 128, 1, 1e-7, 0)
     assert st == 0
+
+
+def test_driver_physics_converts_sddm_and_reads_binary_cache(tmp_path):
+    """--sddm=nnz: a natural-order SDDM file is converted and ordered on the
+    device (the reference's offline write_graph.jl step); a .rchb binary
+    cache of the same matrix runs as the converted file does."""
+    nN, r, c, v, g = R.generate("grid3d", [12, 11, 10], wlo=1e-3, whi=1e3, log_weights=True, excess_frac=0.05,
+                                excess_lo=0.0, excess_hi=1e-2, ordering=2, seed=2)
+    m = (r < nN - 1) & (c < nN - 1)  # the SDDM without its ground vertex
+    path = str(tmp_path / "sddm.mtx")
+    R.write_mtx(path, nN - 1, r[m], c[m], v[m])
+    out = _run([R.driver_binary("driver"), path, "512", "1", "1e-7", "--sddm=nnz", "--order_seed=2"])
+    assert "converted on the device: with ground vertex" in out
+    res = float(re.search(r"residual: ([0-9.e+-]+)", out).group(1))
+    assert res <= 1e-7
+    n0, r0, c0, v0, g0 = R.generate("grid3d", [12, 11, 10], wlo=1e-3, whi=1e3, log_weights=True, excess_frac=0.05,
+                                    excess_lo=0.0, excess_hi=1e-2, seed=2)
+    cp, ri, val = R.csc_from_triplets(n0, r0, c0, v0)
+    bpath = str(tmp_path / "c.rchb")
+    R.write_bin(bpath, n0, cp, ri, val, trim_ground=True)
+    out2 = _run([R.driver_binary("driver"), bpath, "512", "1", "1e-7"])
+    assert float(re.search(r"residual: ([0-9.e+-]+)", out2).group(1)) <= 1e-7
+    assert re.search(r"number of nodes: (\d+)", out2).group(1) == str(n0)

@@ -234,3 +234,40 @@ def test_sddm_conversion_oracle_matches_generator(kind, dims, kw):
     assert N == n0 and g == g0
     assert np.array_equal(cp, cp0) and np.array_equal(ri, ri0)
     np.testing.assert_allclose(val, val0, rtol=1e-10, atol=0)
+
+
+def test_parallel_mtx_reader_keeps_file_order(tmp_path):
+    """The chunked parallel MatrixMarket parse returns the entries in file
+    order (blank and comment lines in the body skipped), as the sequential
+    reader of the test oracle does."""
+    n, r, c, v, g = R.generate("grid3d", [30, 29, 28], wlo=1e-3, whi=1e3, log_weights=True, excess_frac=0.05,
+                               excess_lo=0.0, excess_hi=1e-2, seed=2)
+    path = str(tmp_path / "a.mtx")
+    O.write_mtx(path, n, r, c, v)
+    n2, r2, c2, v2 = R.read_mtx(path)
+    assert n2 == n and np.array_equal(r2, r) and np.array_equal(c2, c) and np.array_equal(v2, v)
+    # a symmetric file with comments and a blank line is generalised
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real symmetric\n% comment\n3 3 4\n1 1 2.5\n\n2 1 -1\n3 2 -0.5\n"
+                "3 3 4\n")
+    n3, r3, c3, v3 = R.read_mtx(path)
+    assert n3 == 3 and list(r3) == [0, 1, 2, 2, 0, 1] and list(c3) == [0, 0, 1, 2, 1, 2]
+    assert list(v3) == [2.5, -1.0, -0.5, 4.0, -1.0, -0.5]
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n3 3 3\n1 1 1\n2 2 1\n")
+    with pytest.raises(R.RcholError):
+        R.read_mtx(path)
+
+
+def test_binary_matrix_cache_roundtrip(tmp_path):
+    n, r, c, v, g = R.generate("grid2d", [40, 33], wlo=1e-2, whi=1e2, log_weights=True, seed=8)
+    cp, ri, val = R.csc_from_triplets(n, r, c, v)
+    path = str(tmp_path / "a.rchb")
+    R.write_bin(path, n, cp, ri, val, trim_ground=True)
+    n2, cp2, ri2, val2, tr = R.read_bin(path)
+    assert n2 == n and tr and np.array_equal(cp2, cp) and np.array_equal(ri2, ri) and np.array_equal(val2, val)
+    with open(path, "r+b") as f:  # corrupt an index: rejected, not trusted
+        f.seek(32 + 4 * (n + 1))
+        f.write(np.array([n + 7], np.int32).tobytes())
+    with pytest.raises(R.RcholError):
+        R.read_bin(path)
