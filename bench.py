@@ -597,22 +597,60 @@ def c4_systems():
     return out
 
 
-def run_c4(args):
+def shard_systems(costs, world):
+    """Systems of a batch partitioned over `world` ranks by cost (Σnnz):
+    longest first, each to the least-loaded rank (ties to the lower rank).
+    Returns one ascending list of system indices per rank."""
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for s in sorted(range(len(costs)), key=lambda q: (-costs[q], q)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(s)
+        load[r] += costs[s]
+    return [sorted(p) for p in parts]
+
+
+def gather_per_system(local, world, nsys):
+    """Rank 0 collects every rank's {system: (iterations, relres)} and checks
+    that each system was solved exactly once (all ranks take part)."""
+    if world <= 1:
+        merged = dict(local)
+    else:
+        import torch.distributed as dist
+        got = [None] * world
+        dist.all_gather_object(got, local)
+        merged = {}
+        for part in got:
+            for sysid, v in part.items():
+                assert sysid not in merged, f"system {sysid} solved twice"
+                merged[sysid] = v
+    assert sorted(merged) == list(range(nsys)), "systems missing from the gather"
+    return merged
+
+
+def run_c4(args, rank=0, world=1):
     """Batched uneven systems: one block-diagonal factor launch + one batched
     PCG (8 RHS per system, FP32 factor / FP64 PCG, tol 1e-6) against looping
-    the single-system path over the same systems (factor + 8-RHS solve each)."""
+    the single-system path over the same systems (factor + 8-RHS solve each).
+    With N ranks the systems are sharded by Σnnz (no exchange while solving);
+    the per-system results are gathered to rank 0 and the time is the max
+    over ranks."""
     import torch
     import rchol_b200 as R
     k = 8
-    systems = c4_systems()
-    ntot = sum(s[0] for s in systems)
+    systems_all = c4_systems()
+    costs = [int(s[1][-1]) for s in systems_all]
+    mine = shard_systems(costs, world)[rank]
+    systems = [systems_all[q] for q in mine]
+    ntot = sum(s[0] for s in systems_all)
     rng = np.random.default_rng(44)
-    Bs = []
-    for n, *_ in systems:
+    Bs_all = []
+    for n, *_ in systems_all:
         B = rng.standard_normal((n, k))
-        Bs.append(B - B.mean(axis=0))
+        Bs_all.append(B - B.mean(axis=0))
+    Bs = [Bs_all[q] for q in mine]
     Bstack = np.concatenate(Bs, axis=0)
-    ctx = R.Context(seed=1, precision=R.PREC_FP32_FACTOR, tol=1e-6)
+    ctx = R.Context(device=torch.cuda.current_device(), seed=1, precision=R.PREC_FP32_FACTOR, tol=1e-6)
     ctx.set_opts(max_iter=2000)
     off = ctx.batch_set(systems)
 
@@ -624,7 +662,7 @@ def run_c4(args):
 
     singles = []
     for n, cp, ri, val in systems:
-        c = R.Context(seed=1, precision=R.PREC_FP32_FACTOR, tol=1e-6)
+        c = R.Context(device=torch.cuda.current_device(), seed=1, precision=R.PREC_FP32_FACTOR, tol=1e-6)
         c.set_opts(max_iter=2000)
         c.set_csc(n, cp, ri, val)
         singles.append(c)
@@ -643,29 +681,39 @@ def run_c4(args):
         looped()
     tb, tl = [], []
     for _ in range(args.steps):
+        barrier(world)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         tot, per = batched()
         torch.cuda.synchronize()
         tb.append(time.perf_counter() - t0)
+        barrier(world)
         t0 = time.perf_counter()
         its = looped()
         torch.cuda.synchronize()
         tl.append(time.perf_counter() - t0)
-    solves = len(systems) * k
-    vb = solves / statistics.mean(tb)
-    vl = solves / statistics.mean(tl)
-    print(json.dumps({"metric": "batched solves/s: 64 uneven Laplacians x 8 RHS, factor + PCG to 1e-6",
-                      "value": round(vb, 2), "unit": "solves/s", "higher_is_better": True, "steps": args.steps,
-                      "warmup": args.warmup, "n_gpus": 1, "dtype": "f32 factor / f64 PCG", "data": "synthetic",
-                      "config": {"workload": "64 systems: 32 2D grids sides U{32..1024}, 32 3D grids sides "
-                                             "U{10..100} (seed 4), log-uniform conductances [1e-2,1e2]",
-                                 "unknowns": int(ntot), "rhs_per_system": k},
-                      "looped_single_system_solves_per_s": round(vl, 2),
-                      "speedup_vs_looped": round(vb / vl, 3),
-                      "batched_s": round(statistics.mean(tb), 4), "looped_s": round(statistics.mean(tl), 4),
-                      "max_iterations": tot["iterations"], "max_relres": tot["relres_true"],
-                      "looped_max_iterations": max(its), "wall_clock_timing": True}))
+    merged = gather_per_system({sysid: (int(p["iterations"]), float(p["relres_true"])) for sysid, p in zip(mine, per)},
+                               world, len(systems_all))
+    solves = len(systems_all) * k
+    t_b = max_over_ranks(statistics.mean(tb), world)
+    t_l = max_over_ranks(statistics.mean(tl), world)
+    vb = solves / t_b
+    vl = solves / t_l
+    if rank == 0:
+        print(json.dumps({"metric": "batched solves/s: 64 uneven Laplacians x 8 RHS, factor + PCG to 1e-6",
+                          "value": round(vb, 2), "unit": "solves/s", "higher_is_better": True, "steps": args.steps,
+                          "warmup": args.warmup, "n_gpus": world, "dtype": "f32 factor / f64 PCG",
+                          "data": "synthetic",
+                          "config": {"workload": "64 systems: 32 2D grids sides U{32..1024}, 32 3D grids sides "
+                                                 "U{10..100} (seed 4), log-uniform conductances [1e-2,1e2]",
+                                     "unknowns": int(ntot), "rhs_per_system": k},
+                          "parallelism": f"systems sharded by nnz over {world} rank(s)",
+                          "looped_single_system_solves_per_s": round(vl, 2),
+                          "speedup_vs_looped": round(vb / vl, 3),
+                          "batched_s": round(t_b, 4), "looped_s": round(t_l, 4),
+                          "max_iterations": max(v[0] for v in merged.values()),
+                          "max_relres": max(v[1] for v in merged.values()),
+                          "looped_max_iterations": max(its) if its else 0, "wall_clock_timing": True}))
     for c in singles:
         c.close()
     ctx.close()
@@ -755,8 +803,11 @@ def profile_run(args, cfg):
 def main():
     args = parse()
     if args.config == "c4":
-        dist_init(1)
-        run_c4(args)
+        rank, world, local = dist_init(args.gpus)
+        run_c4(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     if args.profile_run:
         profile_run(args, CONFIGS[args.config] if args.config in CONFIGS else SECONDARY[args.config])
