@@ -71,6 +71,11 @@ typedef struct rchol_opts {
     int exact_bwd_levels;     /* order the backward solve by its true DAG levels (default 1) */
     int spmv_layout;          /* one-RHS PCG SpMV: RCHOL_SPMV_AUTO (sliced-ELL copy of A
                                  when its padding is at most 25%, else CSR) or RCHOL_SPMV_CSR */
+    int tail_vertices;        /* the last tail_vertices vertices are eliminated one at a time by a
+                                 whole 1024-thread CTA each, after the rest (hubs and dense cores of
+                                 power-law graphs); 0 = none; rchol_autotune picks it */
+    int rhs_block;            /* multi-RHS PCG: solve k right-hand sides in blocks of this width
+                                 (1, 2, 4, 8, 16, 32; 0 = all k at once); rchol_autotune picks it */
 } rchol_opts;
 
 typedef struct rchol_factor_info {
@@ -98,6 +103,7 @@ typedef struct rchol_factor_info {
     const int* lr_idx;
     const double* lr_val;
     const double* diag;       /* D [n] */
+    int tail_vertices;        /* vertices eliminated by the cooperative tail pass */
 } rchol_factor_info;
 
 typedef struct rchol_solve_info {
@@ -234,6 +240,31 @@ rchol_status rchol_precond_apply(rchol_ctx* ctx, const rchol_factor_t* f, int k,
  * each solve. */
 rchol_status rchol_precond_apply_noalloc(const rchol_factor_t* f, int k, const double* R, double* Z, int fp32,
                                          void* stream);
+/* ---- autotuner ---------------------------------------------------------
+ * Picks, for the loaded matrix on this GPU, the options the reference fixes
+ * by hand (WARPS_PER_SQUAD, gpu_implementation/auxilliary.hpp:10-19):
+ *   tail_vertices  the last vertices eliminated by one whole CTA each (the
+ *                  longest suffix in which 3/4 of the vertices gather >= 1024
+ *                  entries), kept only when a timed factorization is faster;
+ *   bucket_cap     the power of two covering 95% of the vertices' gathers,
+ *                  kept only when faster;
+ *   rhs_block      the block width (<= max_rhs) of least iteration time per
+ *                  right-hand side.
+ * One profiling factorization plus at most three timed trials; the choices
+ * are written into the context's options and cached per process for the
+ * same matrix fingerprint (n, nnz, trim, column-length histogram), GPU,
+ * precision and max_rhs (from_cache = 1 on a hit). */
+typedef struct rchol_tune_result {
+    int tail_vertices;
+    int bucket_cap;
+    int rhs_block;
+    int from_cache;
+    int max_gather;          /* largest gathered neighbour list of the profile */
+    float ms_factor_default; /* factor time with the options on entry, no tail */
+    float ms_factor_tuned;   /* factor time with the chosen options */
+    float per_rhs_ms[6];     /* iteration time per right-hand side, k = 1, 2, 4, 8, 16, 32 */
+} rchol_tune_result;
+rchol_status rchol_autotune(rchol_ctx* ctx, int max_rhs, rchol_tune_result* out);
 /* Mean device time (ms) of the three PCG iteration kernels over `reps`
  * iterations on this factor with k right-hand sides: ms_out[0] SpMV +
  * vector update, ms_out[1] forward solve, ms_out[2] backward solve. */

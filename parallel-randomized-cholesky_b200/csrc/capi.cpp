@@ -1,6 +1,8 @@
 // C-ABI implementation (include/rchol.h): context, matrix upload, factor
 // orchestration with capacity retries, PCG, the reference drop-ins.
 #include <algorithm>
+#include <mutex>
+#include <map>
 #include <chrono>
 #include <climits>
 #include <cmath>
@@ -55,6 +57,8 @@ struct rchol_ctx {
     // factors made by this context and not yet freed: rchol_destroy detaches
     // them, so that a factor freed after its context does not touch it
     std::vector<rchol_factor_t*> live;
+    // the autotuner's record of each vertex's gathered entries (device, n)
+    int32_t* gsize = nullptr;
 };
 
 struct rchol_factor {
@@ -263,6 +267,8 @@ extern "C" rchol_status rchol_opts_default(rchol_opts* o) {
     o->sched_epl = 0;
     o->exact_bwd_levels = 1;
     o->spmv_layout = RCHOL_SPMV_AUTO;
+    o->tail_vertices = 0;
+    o->rhs_block = 0;
     return RCHOL_OK;
 }
 
@@ -280,6 +286,10 @@ static rchol_status check_opts(const rchol_opts* o, std::string& why) {
     else if (o->poll_ns < 0 || o->poll_ns > 100000) why = "poll_ns must be 0..100000";
     else if (o->sched_epl < 0 || o->sched_epl > 64) why = "sched_epl must be 0 (automatic) or 1..64";
     else if (o->spmv_layout != RCHOL_SPMV_AUTO && o->spmv_layout != RCHOL_SPMV_CSR) why = "spmv_layout";
+    else if (o->tail_vertices < 0) why = "tail_vertices must be >= 0";
+    else if (o->rhs_block != 0 && o->rhs_block != 1 && o->rhs_block != 2 && o->rhs_block != 4 && o->rhs_block != 8 &&
+             o->rhs_block != 16 && o->rhs_block != 32)
+        why = "rhs_block must be 0 or 1, 2, 4, 8, 16, 32";
     else return RCHOL_OK;
     return RCHOL_ERR_INVALID;
 }
@@ -318,6 +328,7 @@ extern "C" void rchol_destroy(rchol_ctx* ctx) {
     free_csc(ctx->A);
     cudaFree(ctx->dB);
     cudaFree(ctx->dX);
+    cudaFree(ctx->gsize);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -635,6 +646,8 @@ extern "C" rchol_status rchol_factor(rchol_ctx* ctx, rchol_factor_t** out) {
         fl.smem_slab = o.slab_entries;
         fl.seed = o.seed;
         fl.timeout_s = o.timeout_s;
+        fl.tail = std::min<int32_t>(std::max(0, o.tail_vertices), ctx->A.n);
+        fl.gsize = ctx->gsize;
         CK(rchol::launch_factor(w, fl, ctx->stream), "factor launch");
         CK(cudaEventRecord(ev[2], ctx->stream), "record");
         CK(cudaMemcpyAsync(counters, w.counters, sizeof(counters), cudaMemcpyDeviceToHost, ctx->stream), "counters");
@@ -711,6 +724,8 @@ extern "C" rchol_status rchol_factor(rchol_ctx* ctx, rchol_factor_t** out) {
     info.lr_val = f->F.lr_val;
     info.diag = f->F.diag;
     info.fills = (long long)c64[1];
+    info.tail_vertices = std::min<int32_t>(std::max(0, o.tail_vertices), ctx->A.n);
+    if (info.tail_vertices > 0) ++info.kernel_launches;
     f->info = info;
     *out = f;
     return RCHOL_OK;
@@ -1039,8 +1054,44 @@ rchol_status stage_out(rchol_ctx* ctx, const double* src, double* X, int ldb, in
 
 }  // namespace
 
+static rchol_status pcg_solve_block(rchol_ctx* ctx, const rchol_factor_t* f, int k, const double* B, double* X,
+                                    int ldb, int on_device, rchol_solve_info* info);
+
 extern "C" rchol_status rchol_pcg_solve(rchol_ctx* ctx, const rchol_factor_t* f, int k, const double* B, double* X,
                                         int ldb, int on_device, rchol_solve_info* info) {
+    const int blk = ctx ? ctx->o.rhs_block : 0;
+    if (!ctx || !f || !B || !X || blk <= 0 || k <= blk) return pcg_solve_block(ctx, f, k, B, X, ldb, on_device, info);
+    if (!valid_k(k)) return fail(ctx, RCHOL_ERR_INVALID, "k must be 1, 2, 4, 8, 16 or 32");
+    // k right-hand sides in blocks of rhs_block columns (column-major: block
+    // j starts at column j * blk), each its own PCG; the statistics merge
+    rchol_solve_info tot;
+    std::memset(&tot, 0, sizeof(tot));
+    tot.converged = 1;
+    rchol_status worst = RCHOL_OK;
+    for (int c0 = 0; c0 < k; c0 += blk) {
+        rchol_solve_info bi;
+        std::memset(&bi, 0, sizeof(bi));
+        const rchol_status s = pcg_solve_block(ctx, f, blk, B + (size_t)c0 * ldb, X + (size_t)c0 * ldb, ldb,
+                                               on_device, &bi);
+        if (s != RCHOL_OK && s != RCHOL_ERR_NOT_CONVERGED) return s;
+        if (s != RCHOL_OK) worst = s;
+        tot.iterations = std::max(tot.iterations, bi.iterations);
+        tot.converged = tot.converged && bi.converged;
+        tot.device_status = tot.device_status ? tot.device_status : bi.device_status;
+        tot.relres_true = std::max(tot.relres_true, bi.relres_true);
+        tot.relres_rec = std::max(tot.relres_rec, bi.relres_rec);
+        tot.precond_ratio = std::max(tot.precond_ratio, bi.precond_ratio);
+        tot.ms_total += bi.ms_total;
+        tot.ms_iterations += bi.ms_iterations;
+        tot.kernel_launches += bi.kernel_launches;
+        tot.graph_launches += bi.graph_launches;
+    }
+    if (info) *info = tot;
+    return worst == RCHOL_OK ? RCHOL_OK : fail(ctx, worst, "pcg did not reach the tolerance");
+}
+
+static rchol_status pcg_solve_block(rchol_ctx* ctx, const rchol_factor_t* f, int k, const double* B, double* X,
+                                    int ldb, int on_device, rchol_solve_info* info) {
     if (!ctx || !f || !B || !X) return fail(ctx, RCHOL_ERR_INVALID, "null argument");
     if (!ctx->have) return fail(ctx, RCHOL_ERR_NO_MATRIX, "no matrix loaded");
     if (!valid_k(k)) return fail(ctx, RCHOL_ERR_INVALID, "k must be 1, 2, 4, 8, 16 or 32");
@@ -1119,6 +1170,156 @@ extern "C" rchol_status rchol_precond_apply_noalloc(const rchol_factor_t* f, int
                                     (cudaStream_t)stream),
        "precond apply (no alloc)");
     if (status != 0) return fail(ctx, RCHOL_ERR_TIMEOUT, "precond apply: a device wait timed out");
+    return RCHOL_OK;
+}
+
+// ---- autotuner ----------------------------------------------------------------
+// Picks, for the loaded matrix on this GPU: the tail of vertices eliminated
+// by the cooperative CTA pass (tail_vertices), the first fill-chunk size per
+// column (bucket_cap) and the right-hand-side block width of multi-RHS
+// solves (rhs_block).  One factorization records every vertex's gathered
+// entries; the candidates come from that profile and each is kept only when
+// a timed trial beats the options it started from.  Results are cached per
+// process, keyed by the matrix fingerprint (n, nnz, trim, a hash of the
+// column-length histogram), the GPU, the precision and max_rhs.
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::string, rchol_tune_result> g_tune_cache;
+
+// Factor once with `o` and return its factor time (ms), or < 0 on failure.
+float timed_factor(rchol_ctx* ctx, const rchol_opts& o, rchol_status* st) {
+    *st = rchol_set_opts(ctx, &o);
+    if (*st != RCHOL_OK) return -1.0f;
+    rchol_factor_t* f = nullptr;
+    *st = rchol_factor(ctx, &f);
+    if (*st != RCHOL_OK) return -1.0f;
+    const float ms = f->info.ms_factor;
+    rchol_factor_free(f);
+    return ms;
+}
+}  // namespace
+
+extern "C" rchol_status rchol_autotune(rchol_ctx* ctx, int max_rhs, rchol_tune_result* out) {
+    if (!ctx || !out) return fail(ctx, RCHOL_ERR_INVALID, "null argument");
+    if (!ctx->have) return fail(ctx, RCHOL_ERR_NO_MATRIX, "no matrix loaded");
+    if (max_rhs < 1 || max_rhs > 32) return fail(ctx, RCHOL_ERR_INVALID, "max_rhs must be 1..32");
+    cudaSetDevice(ctx->device);
+    std::memset(out, 0, sizeof(*out));
+    const int32_t n = ctx->A.n;
+    // fingerprint
+    std::vector<int32_t> cp((size_t)n + 1);
+    CK(cudaMemcpy(cp.data(), ctx->A.colptr, sizeof(int32_t) * cp.size(), cudaMemcpyDeviceToHost), "copy colptr");
+    std::map<int32_t, int64_t> hist;
+    for (int32_t j = 0; j < n; ++j) hist[cp[(size_t)j + 1] - cp[(size_t)j]]++;
+    uint64_t h = 1469598103934665603ull;
+    for (auto& kv : hist) {
+        h = (h ^ (uint64_t)(uint32_t)kv.first) * 1099511628211ull;
+        h = (h ^ (uint64_t)kv.second) * 1099511628211ull;
+    }
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, ctx->device), "device properties");
+    const std::string key = std::to_string(n) + "/" + std::to_string(ctx->A.nnz) + "/" + std::to_string(ctx->trim) +
+                            "/" + std::to_string(h) + "/" + prop.name + "/" + std::to_string(ctx->o.precision) + "/" +
+                            std::to_string(max_rhs);
+    rchol_opts base = ctx->o;
+    {
+        std::lock_guard<std::mutex> guard(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            *out = it->second;
+            out->from_cache = 1;
+            rchol_opts o = base;
+            o.tail_vertices = out->tail_vertices;
+            o.bucket_cap = out->bucket_cap;
+            o.rhs_block = out->rhs_block;
+            return rchol_set_opts(ctx, &o);
+        }
+    }
+    // 1. profile: every vertex's gathered entries, no cooperative tail
+    rchol_opts o = base;
+    o.tail_vertices = 0;
+    rchol_status st = rchol_set_opts(ctx, &o);
+    if (st != RCHOL_OK) return st;
+    CK(cudaMalloc(&ctx->gsize, sizeof(int32_t) * (size_t)n), "alloc gather record");
+    CK(cudaMemset(ctx->gsize, 0, sizeof(int32_t) * (size_t)n), "clear gather record");
+    rchol_factor_t* f0 = nullptr;
+    st = rchol_factor(ctx, &f0);
+    std::vector<int32_t> g((size_t)n);
+    if (st == RCHOL_OK) {
+        out->ms_factor_default = f0->info.ms_factor;
+        out->max_gather = f0->info.max_gather;
+        if (cudaMemcpy(g.data(), ctx->gsize, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
+            st = RCHOL_ERR_CUDA;
+        rchol_factor_free(f0);
+    }
+    cudaFree(ctx->gsize);
+    ctx->gsize = nullptr;
+    if (st != RCHOL_OK) return st;
+    float best = out->ms_factor_default;
+    // 2. tail: the longest suffix in which at least 3/4 of the vertices
+    // gather >= 1024 entries (at least 64 vertices long)
+    int32_t tail = 0, big = 0;
+    for (int32_t L = 1; L <= n; ++L) {
+        big += g[(size_t)(n - L)] >= 1024;
+        if (4 * big >= 3 * L) tail = L;
+    }
+    if (tail < 64) tail = 0;
+    if (tail > 0) {
+        o.tail_vertices = tail;
+        const float ms = timed_factor(ctx, o, &st);
+        if (st != RCHOL_OK) return st;
+        if (ms < best) best = ms;
+        else o.tail_vertices = 0;
+    }
+    // 3. bucket capacity: the power of two covering 95% of the gathers
+    std::vector<int32_t> sorted(g);
+    std::sort(sorted.begin(), sorted.end());
+    const int32_t p95 = sorted.empty() ? 0 : sorted[(size_t)((sorted.size() - 1) * 95 / 100)];
+    int cap = 8;
+    while (cap < p95 && cap < 64) cap <<= 1;
+    if (cap != o.bucket_cap) {
+        rchol_opts t = o;
+        t.bucket_cap = cap;
+        const float ms = timed_factor(ctx, t, &st);
+        if (st != RCHOL_OK) return st;
+        if (ms < best) {
+            best = ms;
+            o = t;
+        }
+    }
+    out->ms_factor_tuned = best;
+    // 4. right-hand-side block: the width with the least iteration time per RHS
+    o.rhs_block = 0;
+    if (max_rhs > 1) {
+        st = rchol_set_opts(ctx, &o);
+        if (st != RCHOL_OK) return st;
+        rchol_factor_t* f = nullptr;
+        st = rchol_factor(ctx, &f);
+        if (st != RCHOL_OK) return st;
+        float best_rhs = 0.0f;
+        int kbest = 1;
+        for (int q = 0, kk = 1; kk <= max_rhs && q < 6; ++q, kk <<= 1) {
+            float ms3[3] = {0, 0, 0};
+            st = rchol_profile_solve(ctx, f, kk, 3, ms3);
+            if (st != RCHOL_OK) break;
+            out->per_rhs_ms[q] = (ms3[0] + ms3[1] + ms3[2]) / (float)kk;
+            if (kk == 1 || out->per_rhs_ms[q] < best_rhs) {
+                best_rhs = out->per_rhs_ms[q];
+                kbest = kk;
+            }
+        }
+        rchol_factor_free(f);
+        if (st != RCHOL_OK) return st;
+        o.rhs_block = kbest;
+    }
+    out->tail_vertices = o.tail_vertices;
+    out->bucket_cap = o.bucket_cap;
+    out->rhs_block = o.rhs_block;
+    st = rchol_set_opts(ctx, &o);
+    if (st != RCHOL_OK) return st;
+    std::lock_guard<std::mutex> guard(g_tune_mu);
+    g_tune_cache[key] = *out;
     return RCHOL_OK;
 }
 

@@ -325,6 +325,8 @@ struct FactorArgs {
     int smem_slab;
     int smem_region;  // bytes of shared memory per warp (slab, or radix histogram + CDF index)
     unsigned long long timeout_ns;
+    int32_t tail;     // vertices >= tail are left to factor_tail_kernel (n: none)
+    int32_t* gsize;   // gathered entries of each vertex (null: not recorded)
 };
 
 __device__ __forceinline__ bool aborted(const FactorArgs& a) { return ld_relaxed(a.counters + kAbort) != 0; }
@@ -632,6 +634,7 @@ __device__ bool eliminate(const FactorArgs& a, int32_t k, Slab sm, unsigned char
         return true;
     }
     if (total > max_gather) max_gather = total;
+    if (a.gsize && lane == 0) a.gsize[k] = total;
     if (no == 0 && nf <= a.c0 && total <= kWarp)  // every entry is in the bucket
         return eliminate_small(a, k, total, brow_l, bval_l, lvl, lane, pool_cur, pool_end, fills, next);
     if (total <= a.smem_slab)
@@ -905,7 +908,7 @@ __global__ void __launch_bounds__(256, 3) factor_kernel(FactorArgs a) {
                 while ((k = ld_acquire(a.queue + idx)) < 0) {
                     if ((++spins & 63u) == 0) {
                         const int done = ld_relaxed(a.counters + kDone);
-                        if (done >= a.n || aborted(a)) break;
+                        if (done >= a.tail || aborted(a)) break;
                         const unsigned long long now = global_timer_ns();
                         if (done != seen) {
                             seen = done;
@@ -920,6 +923,7 @@ __global__ void __launch_bounds__(256, 3) factor_kernel(FactorArgs a) {
             k = __shfl_sync(kFull, k, 0);
             if (k < 0) break;
         }
+        if (k >= a.tail) continue;  // left to the cooperative tail pass
         __threadfence();
         if (!eliminate(a, k, sm, wsm, warp_global, lane, pool_cur, pool_end, fills, next, max_gather)) break;
         ++done_local;
@@ -929,6 +933,354 @@ __global__ void __launch_bounds__(256, 3) factor_kernel(FactorArgs a) {
     if (lane == 0 && max_gather) atomicMax(a.counters + kMaxGather, max_gather);
     if (lane == 0 && fills) atomicAdd(a.pool_cursor + 1, (unsigned long long)fills);
 }
+
+// ---- cooperative elimination of the tail -----------------------------------
+// The last vertices of a power-law graph (hubs and the dense core) depend
+// on one another in a chain and gather thousands of entries each; a warp
+// per vertex leaves the rest of the GPU idle while it sorts.  Vertices
+// >= tail are therefore eliminated after factor_kernel by one CTA of
+// kTailThreads threads, in index order (every dependency of a vertex has a
+// smaller index, so each column is final when its turn comes).  The steps
+// and their rounding are those of eliminate_slab<true> -- the same radix
+// orders, duplicate runs added in sorted order, 32-wide Kogge-Stone chunks
+// with the carry chained in chunk order, the same sampling search -- so the
+// factor is bit-identical to the warp path's (and the oracle's).
+
+constexpr int kTailThreads = 1024;
+constexpr int kTailWarps = kTailThreads / kWarp;
+
+// One stable CTA pass of (row, val[, aux]) by digit d: warp w takes a
+// contiguous tile (a multiple of 32 entries), counts, and scatters it in
+// order through digit-major, warp-minor offsets.  Returns false when one
+// digit holds all n entries (nothing would move; nothing is written).
+template <bool VR, bool AUX>
+__device__ bool tail_radix_pass(const int32_t* row, const double* val, const long long* aux, int32_t* orow,
+                                double* oval, long long* oaux, int n, int d, int* hist, int* tot) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int tile = ((n + kTailWarps - 1) / kTailWarps + 31) & ~31;
+    const int t0 = min(n, w * tile), t1 = min(n, t0 + tile);
+    int* h = hist + w * 256;
+    for (int i = lane; i < 256; i += kWarp) h[i] = 0;
+    __syncwarp();
+    for (int base = t0; base < t1; base += kRadixRounds * kWarp) {
+        int dig[kRadixRounds];
+#pragma unroll
+        for (int q = 0; q < kRadixRounds; ++q) {
+            const int i = base + q * kWarp + lane;
+            dig[q] = i < t1 ? (VR ? vr_digit(row[i], val[i], d) : rv_digit(row[i], val[i], d)) : -1;
+        }
+#pragma unroll
+        for (int q = 0; q < kRadixRounds; ++q)
+            if (dig[q] >= 0) atomicAdd(&h[dig[q]], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < 256) {
+        int c = 0;
+        for (int q = 0; q < kTailWarps; ++q) c += hist[q * 256 + threadIdx.x];
+        tot[threadIdx.x] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0, one = 0;
+        for (int g = 0; g < 256; ++g) {
+            const int c = tot[g];
+            one |= c == n;
+            tot[g] = run;
+            run += c;
+        }
+        tot[256] = one;
+    }
+    __syncthreads();
+    const bool skip = tot[256] != 0;
+    if (!skip && threadIdx.x < 256) {
+        int run = tot[threadIdx.x];
+        for (int q = 0; q < kTailWarps; ++q) {
+            const int c = hist[q * 256 + threadIdx.x];
+            hist[q * 256 + threadIdx.x] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    if (skip) return false;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int base = t0; base < t1; base += kRadixRounds * kWarp) {
+        int32_t r[kRadixRounds];
+        double v[kRadixRounds];
+        long long x[kRadixRounds];
+#pragma unroll
+        for (int q = 0; q < kRadixRounds; ++q) {
+            const int i = base + q * kWarp + lane;
+            r[q] = 0;
+            v[q] = 0.0;
+            x[q] = 0;
+            if (i < t1) {
+                r[q] = row[i];
+                v[q] = val[i];
+                if (AUX) x[q] = aux[i];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kRadixRounds; ++q) {
+            const bool valid = base + q * kWarp + lane < t1;
+            const int dig = valid ? (VR ? vr_digit(r[q], v[q], d) : rv_digit(r[q], v[q], d)) : 256;
+            const unsigned peers = __match_any_sync(kFull, dig);
+            const int rank = __popc(peers & lt);
+            const int at = valid ? h[dig] + rank : 0;
+            __syncwarp();
+            if (valid && rank == 0) h[dig] += __popc(peers);
+            __syncwarp();
+            if (valid) {
+                orow[at] = r[q];
+                oval[at] = v[q];
+                if (AUX) oaux[at] = x[q];
+            }
+        }
+    }
+    __syncthreads();
+    return true;
+}
+
+template <bool VR, bool AUX>
+__device__ void tail_radix_sort(int32_t* r_out, double* v_out, long long* x_out, int32_t* r_tmp, double* v_tmp,
+                                long long* x_tmp, int n, int dlo, int dhi, int* hist, int* tot) {
+    int32_t *r0 = r_out, *r1 = r_tmp;
+    double *v0 = v_out, *v1 = v_tmp;
+    long long *x0 = x_out, *x1 = x_tmp;
+    for (int d = dlo; d < dhi; ++d) {
+        if (!tail_radix_pass<VR, AUX>(r0, v0, x0, r1, v1, x1, n, d, hist, tot)) continue;
+        int32_t* tr = r0;
+        r0 = r1;
+        r1 = tr;
+        double* tv = v0;
+        v0 = v1;
+        v1 = tv;
+        long long* tx = x0;
+        x0 = x1;
+        x1 = tx;
+    }
+    if (r0 != r_out) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            r_out[i] = r0[i];
+            v_out[i] = v0[i];
+            if (AUX) x_out[i] = x0[i];
+        }
+        __syncthreads();
+    }
+}
+
+// Exclusive count of the flagged entries before each warp's tile, for an
+// order-preserving compaction (warp w holds the tile as in the radix passes).
+__device__ __forceinline__ int tail_tile_offset(int count, int* scan) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) scan[w] = count;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int q = 0; q < kTailWarps; ++q) {
+            const int c = scan[q];
+            scan[q] = run;
+            run += c;
+        }
+        scan[kTailWarps] = run;
+    }
+    __syncthreads();
+    return scan[w];
+}
+
+__global__ void __launch_bounds__(kTailThreads, 1) factor_tail_kernel(FactorArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    int* hist = reinterpret_cast<int*>(smem);      // [kTailWarps][256]
+    int* tot = hist + kTailWarps * 256;            // [257]
+    int* scan = tot + 260;                         // [kTailWarps + 1]
+    __shared__ long long sh_base;
+    __shared__ int sh_stop;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    long long fills = 0;
+    int max_gather = 0, done = 0;
+    if (threadIdx.x == 0) sh_stop = 0;
+    __syncthreads();
+    Slab s = make_global_slab(a.hscratch, (int)a.hscratch_entries);
+    for (int32_t k = a.tail; k < a.n; ++k) {
+        if (aborted(a)) break;
+        const int nf = ld_relaxed(a.fcnt + k);
+        const int oc0 = a.lcolptr[k];
+        const int ocnt = a.lcolptr[k + 1] - oc0;
+        const int o0 = oc0 + min(ocnt, a.c0);
+        const int no = ocnt - min(ocnt, a.c0);
+        const int total = nf + no;
+        if (a.gsize && threadIdx.x == 0) a.gsize[k] = total;
+        ++done;
+        if (total == 0) {
+            if (threadIdx.x == 0) {
+                a.diag[k] = 0.0;
+                a.pcnt[k] = 0;
+                a.pstart[k] = 0;
+            }
+            continue;
+        }
+        if (total > max_gather) max_gather = total;
+        if ((int64_t)total > a.hscratch_entries) {
+            if (threadIdx.x == 0) fail(a, kDevCapacity);
+            break;
+        }
+        // ---- gather: bucket, overflow chunks, originals
+        const int n0 = min(nf, a.c0);
+        for (int t = threadIdx.x; t < n0; t += blockDim.x) {
+            const size_t o = (size_t)k * (size_t)a.c0 + (size_t)t;
+            s.a_row[t] = __ldcg(a.brow + o);
+            s.a_val[t] = __ldcg(a.bval + o);
+        }
+        int rem = nf - n0, pos = n0;
+        int chunk = rem > 0 ? ld_relaxed(a.chead + k) : -1;
+        bool bad = false;
+        for (int lvl = 0; rem > 0; ++lvl) {
+            if (chunk < 0 || chunk > a.nchunks - (1 << lvl)) {
+                bad = true;
+                break;
+            }
+            const int cnt = min(rem, kChunk << lvl);
+            for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+                s.a_row[pos + t] = __ldcg(a.crow + (size_t)chunk * kChunk + t);
+                s.a_val[pos + t] = __ldcg(a.cval + (size_t)chunk * kChunk + t);
+            }
+            pos += cnt;
+            rem -= cnt;
+            if (rem > 0) chunk = ld_relaxed(a.cnext + chunk);
+        }
+        if (bad) {
+            if (threadIdx.x == 0) fail(a, kDevBadInput);
+            break;
+        }
+        for (int t = threadIdx.x; t < no; t += blockDim.x) {
+            s.a_row[nf + t] = a.lrow[o0 + t];
+            s.a_val[nf + t] = a.lval[o0 + t];
+        }
+        __syncthreads();
+        // ---- sort by (row, value bits); merge duplicate rows in that order
+        tail_radix_sort<false, false>(s.a_row, s.a_val, nullptr, s.t_row, s.t_val, nullptr, total, 0, 12, hist, tot);
+        const int tile = ((total + kTailWarps - 1) / kTailWarps + 31) & ~31;
+        const int t0 = min(total, w * tile), t1 = min(total, t0 + tile);
+        int heads = 0;
+        for (int base = t0; base < t1; base += kWarp) {
+            const int i = base + lane;
+            const bool head = i < t1 && (i == 0 || s.a_row[i - 1] != s.a_row[i]);
+            heads += __popc(__ballot_sync(kFull, head));
+        }
+        int m0 = tail_tile_offset(heads, scan);
+        const int m = scan[kTailWarps];
+        for (int base = t0; base < t1; base += kWarp) {
+            const int i = base + lane;
+            const bool valid = i < t1;
+            const int32_t ri = valid ? s.a_row[i] : INT_MAX;
+            const bool head = valid && (i == 0 || s.a_row[i - 1] != ri);
+            const unsigned bal = __ballot_sync(kFull, head);
+            if (head) {
+                const int rank = m0 + __popc(bal & lt);
+                double acc = s.a_val[i];
+                int cnt = 1;
+                for (int j = i + 1; j < total && s.a_row[j] == ri; ++j) {
+                    acc = __dadd_rn(acc, s.a_val[j]);
+                    ++cnt;
+                }
+                s.b_val[rank] = acc;
+                s.b_row[rank] = ri;
+                s.b_aux[rank] = ((long long)cnt << 32) | (long long)rank;
+            }
+            m0 += __popc(bal);
+        }
+        __syncthreads();
+        // ---- sort by value (input in row order: the value bytes suffice)
+        tail_radix_sort<true, true>(s.b_row, s.b_val, s.b_aux, s.t_row, s.t_val, s.t_aux, m, 4, 12, hist, tot);
+        // ---- prefix sums: 32-wide Kogge-Stone chunks (warp c % 32 takes
+        // chunk c), the chunk totals in t_val; then the carries chained in
+        // chunk order by one thread, as the warp path carries them
+        const int nchunk = (m + kWarp - 1) / kWarp;
+        for (int c = w; c < nchunk; c += kTailWarps) {
+            const int i = c * kWarp + lane;
+            double v = i < m ? s.b_val[i] : 0.0;
+#pragma unroll
+            for (int off = 1; off < kWarp; off <<= 1) {
+                const double t = __shfl_up_sync(kFull, v, off);
+                if (lane >= off) v = __dadd_rn(v, t);
+            }
+            if (i < m) s.a_val[i] = v;
+            if (lane == kWarp - 1) s.t_val[c] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            // t_val[c] becomes the carry into chunk c (c >= 1)
+            double carry = s.t_val[0];
+            for (int c = 1; c < nchunk; ++c) {
+                const double tc = s.t_val[c];
+                s.t_val[c] = carry;
+                carry = __dadd_rn(carry, tc);
+            }
+        }
+        __syncthreads();
+        for (int i = kWarp + threadIdx.x; i < m; i += blockDim.x) s.a_val[i] = __dadd_rn(s.t_val[i / kWarp], s.a_val[i]);
+        __syncthreads();
+        const double S = s.a_val[m - 1];
+        // ---- L column k into the pool (row order), D_k
+        if (threadIdx.x == 0) {
+            const unsigned long long got = atomicAdd(a.pool_cursor, (unsigned long long)m);
+            sh_base = (long long)got;
+            if ((int64_t)got + m > a.pool_cap) {
+                fail(a, kDevCapacity);
+                sh_stop = 1;
+            } else {
+                a.diag[k] = S;
+                a.pstart[k] = (int64_t)got;
+                a.pcnt[k] = m;
+            }
+        }
+        __syncthreads();
+        if (sh_stop) break;
+        const int64_t pbase = sh_base;
+        fills += m - 1;
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            const int p = (int)(s.b_aux[i] & 0xffffffffll);
+            a.prow[pbase + p] = s.b_row[i];
+            a.pval[pbase + p] = __ddiv_rn(s.b_val[i], S);
+        }
+        // ---- clique sampling (the same search predicate as the warp path)
+        const double* C = s.a_val;
+        bool ok = true;
+        for (int i = threadIdx.x; i < m - 1; i += blockDim.x) {
+            const double ci = C[i];
+            const double rem_i = __dsub_rn(S, ci);
+            const double target = __dmul_rn(sample_uniform(a.seed, k, i), rem_i);
+            int lo = i + 1, hi = m;
+            while (lo < hi) {
+                const int mid = lo + ((hi - lo) >> 1);
+                if (__dsub_rn(C[mid], ci) < target) lo = mid + 1;
+                else hi = mid;
+            }
+            const int j = lo < m ? lo : m - 1;
+            const int32_t r_i = s.b_row[i], r_j = s.b_row[j];
+            const int32_t grow = r_i > r_j ? r_i : r_j;
+            const int32_t gcol = r_i > r_j ? r_j : r_i;
+            const double gval = __ddiv_rn(__dmul_rn(s.b_val[i], rem_i), S);
+            if (!append_fill(a, gcol, grow, gval)) ok = false;
+        }
+        // rows of L column k are one level below k (the solve schedules)
+        const int lk = ld_relaxed(a.level + k) + 1;
+        for (int i = threadIdx.x; i < m; i += blockDim.x) atomicMax(a.level + s.b_row[i], lk);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) fail(a, kDevCapacity);
+            break;
+        }
+        __threadfence();
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(a.counters + kDone, done);
+        atomicMax(a.counters + kMaxGather, max_gather);
+        atomicAdd(a.pool_cursor + 1, (unsigned long long)fills);
+    }
+}
+
+size_t tail_smem_bytes() { return sizeof(int) * ((size_t)kTailWarps * 256 + 260 + kTailWarps + 1); }
 
 // ---- setup kernels --------------------------------------------------------
 
@@ -1166,11 +1518,21 @@ cudaError_t launch_factor(FactorWork& w, const FactorLaunch& cfg, cudaStream_t s
     a.smem_slab = cfg.smem_slab;
     a.smem_region = smem_region_bytes(cfg.smem_slab);
     a.timeout_ns = (unsigned long long)(cfg.timeout_s * 1e9);
+    a.tail = cfg.tail > 0 && cfg.tail < w.n ? w.n - cfg.tail : w.n;
+    a.gsize = cfg.gsize;
     size_t smem = factor_smem_bytes(cfg.block, cfg.smem_slab);
     cudaError_t e = cudaFuncSetAttribute(factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     factor_kernel<<<cfg.grid, cfg.block, smem, s>>>(a);
-    return cudaGetLastError();
+    RCHOL_TRY(cudaGetLastError());
+    if (a.tail < w.n) {
+        // the tail, one CTA, in index order, after the rest is eliminated
+        const size_t tsmem = tail_smem_bytes();
+        RCHOL_TRY(cudaFuncSetAttribute(factor_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
+        factor_tail_kernel<<<1, kTailThreads, tsmem, s>>>(a);
+        RCHOL_TRY(cudaGetLastError());
+    }
+    return cudaSuccess;
 }
 
 }  // namespace rchol

@@ -248,6 +248,8 @@ struct FactorLaunch {
     int smem_slab = 256;      // entries per warp slab in shared memory
     uint64_t seed = 1;
     double timeout_s = 20.0;
+    int32_t tail = 0;         // the last `tail` vertices are eliminated by one cooperative CTA (0: none)
+    int32_t* gsize = nullptr; // device [n]: gathered entries of each vertex (null: not recorded)
 };
 
 // ---- setup / factor / assembly (factor.cu) --------------------------------

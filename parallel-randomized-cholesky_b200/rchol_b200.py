@@ -35,7 +35,7 @@ EXPORTS = sorted([
     "rchol_factor_free", "rchol_pcg_solve", "rchol_precond_apply", "rchol_precond_apply_noalloc", "rchol_profile_solve", "rchol_spmv", "rchol_factorization_driver",
     "rchol_prepare_and_solve", "rchol_generate", "rchol_free_host", "rchol_write_mtx", "rchol_batch_set",
     "rchol_batch_solve", "rchol_zero_sum_vector", "rchol_set_sddm", "rchol_write_bin", "rchol_read_bin",
-    "rchol_save_bin", "rchol_load_bin",
+    "rchol_save_bin", "rchol_load_bin", "rchol_autotune",
 ])
 
 
@@ -51,7 +51,8 @@ class Opts(C.Structure):
                 ("pool_mult", C.c_double), ("max_iter", C.c_int), ("tol", C.c_double), ("stop_rule", C.c_int),
                 ("unroll", C.c_int), ("use_graph", C.c_int), ("device", C.c_int), ("timeout_s", C.c_double),
                 ("verbose", C.c_int), ("poll_ns", C.c_int),
-                ("sched_epl", C.c_int), ("exact_bwd_levels", C.c_int), ("spmv_layout", C.c_int)]
+                ("sched_epl", C.c_int), ("exact_bwd_levels", C.c_int), ("spmv_layout", C.c_int),
+                ("tail_vertices", C.c_int), ("rhs_block", C.c_int)]
 
 
 class FactorInfo(C.Structure):
@@ -62,7 +63,14 @@ class FactorInfo(C.Structure):
                 ("ms_assemble", C.c_float), ("attempts", C.c_int),
                 ("solve_depth", C.c_int), ("kernel_launches", C.c_int),
                 ("lc_ptr", C.c_void_p), ("lc_idx", C.c_void_p), ("lc_val", C.c_void_p),
-                ("lr_ptr", C.c_void_p), ("lr_idx", C.c_void_p), ("lr_val", C.c_void_p), ("diag", C.c_void_p)]
+                ("lr_ptr", C.c_void_p), ("lr_idx", C.c_void_p), ("lr_val", C.c_void_p), ("diag", C.c_void_p),
+                ("tail_vertices", C.c_int)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("tail_vertices", C.c_int), ("bucket_cap", C.c_int), ("rhs_block", C.c_int),
+                ("from_cache", C.c_int), ("max_gather", C.c_int), ("ms_factor_default", C.c_float),
+                ("ms_factor_tuned", C.c_float), ("per_rhs_ms", C.c_float * 6)]
 
 
 class System(C.Structure):
@@ -140,6 +148,7 @@ def lib():
                                      i32p]
         L.rchol_save_bin.argtypes = [vp, C.c_char_p]
         L.rchol_load_bin.argtypes = [vp, C.c_char_p]
+        L.rchol_autotune.argtypes = [vp, C.c_int, C.POINTER(TuneResult)]
         L.rchol_set_sddm.argtypes = [vp, C.c_int, C.c_longlong, vp, vp, vp, C.c_int, C.c_int, C.c_ulonglong, vp,
                                      i32p]
         L.rchol_batch_set.argtypes = [vp, C.c_int, C.POINTER(System), C.POINTER(C.c_longlong)]
@@ -356,6 +365,17 @@ class Context:
         _check(lib().rchol_set_sddm(self.h, n, len(rows), _ptr(rows), _ptr(cols), _ptr(vals), 0, int(ordering),
                                     int(order_seed), _ptr(perm), C.byref(g)), self.h)
         return perm, bool(g.value)
+
+    def autotune(self, max_rhs=1):
+        """rchol_autotune: the chosen options (also set on the context)."""
+        r = TuneResult()
+        _check(lib().rchol_autotune(self.h, int(max_rhs), C.byref(r)), self.h)
+        d = {k: getattr(r, k) for k, _ in r._fields_ if k != "per_rhs_ms"}
+        d["per_rhs_ms"] = list(r.per_rhs_ms)
+        # the context now runs with the tuned options; keep this copy in step
+        for k in ("tail_vertices", "bucket_cap", "rhs_block"):
+            setattr(self.opts, k, d[k])
+        return d
 
     def load_bin(self, path):
         _check(lib().rchol_load_bin(self.h, path.encode()), self.h)

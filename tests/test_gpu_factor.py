@@ -10,7 +10,7 @@ import pytest
 
 import pyoracle as O
 import rchol_b200 as R
-from helpers import OracleProblem, grid_laplacian
+from helpers import OracleProblem, grid_laplacian, zero_sum_normal
 
 pytestmark = pytest.mark.gpu
 
@@ -247,3 +247,60 @@ def test_factor_outlives_its_context():
     cp, ri, val, d = f.to_host()
     assert np.array_equal(ri, orc["rowind"]) and np.array_equal(val, orc["val"])
     f.free()
+
+
+@pytest.mark.parametrize("case,tail", [("powerlaw", 400), ("powerlaw", 6000), ("cube_sddm", 10 ** 9)])
+def test_cooperative_tail_is_bit_exact(case, tail):
+    """The last `tail` vertices eliminated one at a time by a whole CTA
+    (CTA radix sorts, chained Kogge-Stone carries) give the oracle's factor
+    bit for bit, including a tail that covers every vertex."""
+    if case == "powerlaw":
+        n, r, c, v, g = R.generate("chunglu", [6000, 30000, 2, 1500], wlo=1.0, whi=10.0, seed=7)
+    else:
+        n, r, c, v, g = grid_laplacian((11, 10, 9), seed=3, excess_frac=0.05, wlo=1e-3, whi=1e3)
+    P = OracleProblem(n, r, c, v, trim=g)
+    orc = P.factor(seed=21)
+    ctx = R.Context(seed=21, tail_vertices=min(tail, n))
+    try:
+        ctx.set_triplets(n, r, c, v, trim_ground=g)
+        f = ctx.factor()
+        assert f.info().tail_vertices == min(tail, n)
+        cp, ri, val, d = f.to_host()
+        assert np.array_equal(cp, orc["colptr"]) and np.array_equal(ri, orc["rowind"])
+        assert np.array_equal(val, orc["val"]) and np.array_equal(d, orc["diag"])
+        b = zero_sum_normal(P.ns, 4)
+        x, info = ctx.pcg_solve(f, b)
+        assert info["converged"]
+        f.free()
+    finally:
+        ctx.close()
+
+
+def test_autotune_choices_are_used_and_cached():
+    """rchol_autotune profiles the gathers, keeps only choices that time
+    faster, writes them into the context's options (the next factorization
+    reports the chosen tail) and serves a second call from its cache."""
+    n, r, c, v, g = R.generate("chunglu", [20000, 150000, 2, 5000], wlo=1.0, whi=10.0, seed=7)
+    ctx = R.Context(seed=3, precision=R.PREC_FP32_FACTOR)
+    try:
+        ctx.set_triplets(n, r, c, v, trim_ground=g)
+        t1 = ctx.autotune(max_rhs=32)
+        assert not t1["from_cache"] and t1["max_gather"] > 1024
+        assert t1["rhs_block"] in (1, 2, 4, 8, 16, 32) and t1["bucket_cap"] in (8, 16, 32, 64)
+        assert t1["ms_factor_tuned"] <= t1["ms_factor_default"]
+        assert all(x > 0 for x in t1["per_rhs_ms"])
+        assert ctx.opts.tail_vertices == t1["tail_vertices"] and ctx.opts.rhs_block == t1["rhs_block"]
+        f = ctx.factor()
+        assert f.info().tail_vertices == t1["tail_vertices"]
+        f.free()
+        t2 = ctx.autotune(max_rhs=32)
+        assert t2["from_cache"] and t2["tail_vertices"] == t1["tail_vertices"]
+        # a k-RHS solve runs in blocks of the chosen width and still converges
+        B = np.random.default_rng(2).standard_normal((n - (1 if g else 0), 32))
+        B -= B.mean(axis=0)
+        f = ctx.factor()
+        X, info = ctx.pcg_solve(f, B)
+        assert info["converged"]
+        f.free()
+    finally:
+        ctx.close()
