@@ -71,6 +71,7 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--config", default="c2", choices=sorted(CONFIGS) + ["c4"] + sorted(SECONDARY))
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-autotune", action="store_true", help="secondary configs: keep the default options")
     p.add_argument("--profile-run", action="store_true",
                    help="one factorization + one PCG solve of the config (mixed form), for profilers")
     p.add_argument("--size", type=int, default=0, help="grid side override for --profile-run (small ncu cases)")
@@ -741,6 +742,13 @@ def run_secondary(args, cfg, name):
         ctx = R.Context(seed=1, precision=prec, tol=cfg["tol"], stop_rule=R.STOP_RELRES)
         ctx.set_opts(max_iter=1000)
         ctx.set_csc(n, W["colptr"], W["rowind"], W["val"], trim_ground=ground)
+        if not args.no_autotune:
+            # the library's autotuner (tail, bucket capacity, RHS block),
+            # untimed, once per form: its choices hold for the timed runs
+            t0 = time.perf_counter()
+            tune = ctx.autotune(max_rhs=max(cfg["rhs"]))
+            tune["tune_s"] = round(time.perf_counter() - t0, 2)
+            out.setdefault("autotune", {})[form] = tune
         for k in cfg["rhs"]:
             B = np.random.default_rng(3000 + k).standard_normal((ns, k))
             B -= B.mean(axis=0)

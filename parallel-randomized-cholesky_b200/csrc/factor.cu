@@ -327,6 +327,7 @@ struct FactorArgs {
     unsigned long long timeout_ns;
     int32_t tail;     // vertices >= tail are left to factor_tail_kernel (n: none)
     int32_t* gsize;   // gathered entries of each vertex (null: not recorded)
+    int32_t tail_cdf_cap;  // prefix sums the tail kernel keeps in shared memory
 };
 
 __device__ __forceinline__ bool aborted(const FactorArgs& a) { return ld_relaxed(a.counters + kAbort) != 0; }
@@ -948,6 +949,12 @@ __global__ void __launch_bounds__(256, 3) factor_kernel(FactorArgs a) {
 
 constexpr int kTailThreads = 1024;
 constexpr int kTailWarps = kTailThreads / kWarp;
+// shared memory of the tail kernel: per-warp digit histograms, 256 totals
+// (+ a flag), warp offsets, padded to an even word count; then a copy of up
+// to kTailCdfCap prefix sums for the sampling searches
+constexpr int kTailIntWords = kTailWarps * 256 + 260 + 36;
+constexpr int kTailCdfCap = 20480;
+static_assert(kTailIntWords % 2 == 0, "the prefix-sum copy must be 8-byte aligned");
 
 // One stable CTA pass of (row, val[, aux]) by digit d: warp w takes a
 // contiguous tile (a multiple of 32 entries), counts, and scatters it in
@@ -980,15 +987,29 @@ __device__ bool tail_radix_pass(const int32_t* row, const double* val, const lon
         tot[threadIdx.x] = c;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int run = 0, one = 0;
-        for (int g = 0; g < 256; ++g) {
-            const int c = tot[g];
-            one |= c == n;
-            tot[g] = run;
-            run += c;
+    if (w == 0) {
+        // exclusive scan of the 256 totals: 8 digits per lane, then the lanes
+        int c[8], sum = 0, one = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            c[q] = tot[8 * lane + q];
+            sum += c[q];
+            one |= c[q] == n;
         }
-        tot[256] = one;
+        int incl = sum;
+#pragma unroll
+        for (int o = 1; o < kWarp; o <<= 1) {
+            const int t = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += t;
+        }
+        int run = incl - sum;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            tot[8 * lane + q] = run;
+            run += c[q];
+        }
+        one = __any_sync(kFull, one != 0) ? 1 : 0;
+        if (lane == 0) tot[256] = one;
     }
     __syncthreads();
     const bool skip = tot[256] != 0;
@@ -1208,13 +1229,19 @@ __global__ void __launch_bounds__(kTailThreads, 1) factor_tail_kernel(FactorArgs
             if (lane == kWarp - 1) s.t_val[c] = v;
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            // t_val[c] becomes the carry into chunk c (c >= 1)
-            double carry = s.t_val[0];
-            for (int c = 1; c < nchunk; ++c) {
-                const double tc = s.t_val[c];
-                s.t_val[c] = carry;
-                carry = __dadd_rn(carry, tc);
+        if (w == 0) {
+            // t_val[c] becomes the carry into chunk c (c >= 1): one lane adds
+            // the totals in chunk order, 32 at a time read into registers
+            double carry = 0.0;
+            for (int c0 = 0; c0 < nchunk; c0 += kWarp) {
+                const double tl = c0 + lane < nchunk ? s.t_val[c0 + lane] : 0.0;
+                double cin = 0.0;
+                for (int q = 0; q < kWarp && c0 + q < nchunk; ++q) {
+                    const double tq = __shfl_sync(kFull, tl, q);
+                    if (lane == q) cin = carry;  // carry into chunk c0 + q
+                    carry = (c0 + q == 0) ? tq : __dadd_rn(carry, tq);
+                }
+                if (c0 + lane < nchunk) s.t_val[c0 + lane] = cin;
             }
         }
         __syncthreads();
@@ -1243,8 +1270,15 @@ __global__ void __launch_bounds__(kTailThreads, 1) factor_tail_kernel(FactorArgs
             a.prow[pbase + p] = s.b_row[i];
             a.pval[pbase + p] = __ddiv_rn(s.b_val[i], S);
         }
-        // ---- clique sampling (the same search predicate as the warp path)
+        // ---- clique sampling (the same search predicate as the warp path),
+        // searching a shared-memory copy of the prefix sums when it fits
         const double* C = s.a_val;
+        if (m <= a.tail_cdf_cap) {
+            double* cs = reinterpret_cast<double*>(smem + sizeof(int) * kTailIntWords);
+            for (int i = threadIdx.x; i < m; i += blockDim.x) cs[i] = s.a_val[i];
+            __syncthreads();
+            C = cs;
+        }
         bool ok = true;
         for (int i = threadIdx.x; i < m - 1; i += blockDim.x) {
             const double ci = C[i];
@@ -1280,7 +1314,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) factor_tail_kernel(FactorArgs
     }
 }
 
-size_t tail_smem_bytes() { return sizeof(int) * ((size_t)kTailWarps * 256 + 260 + kTailWarps + 1); }
+size_t tail_smem_bytes() { return sizeof(int) * (size_t)kTailIntWords + sizeof(double) * (size_t)kTailCdfCap; }
 
 // ---- setup kernels --------------------------------------------------------
 
@@ -1519,6 +1553,7 @@ cudaError_t launch_factor(FactorWork& w, const FactorLaunch& cfg, cudaStream_t s
     a.smem_region = smem_region_bytes(cfg.smem_slab);
     a.timeout_ns = (unsigned long long)(cfg.timeout_s * 1e9);
     a.tail = cfg.tail > 0 && cfg.tail < w.n ? w.n - cfg.tail : w.n;
+    a.tail_cdf_cap = kTailCdfCap;
     a.gsize = cfg.gsize;
     size_t smem = factor_smem_bytes(cfg.block, cfg.smem_slab);
     cudaError_t e = cudaFuncSetAttribute(factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
