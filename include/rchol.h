@@ -146,6 +146,7 @@ rchol_status rchol_set_triplets(rchol_ctx* ctx, int n, long long nnz, const int*
  *   ordering RCHOL_ORDER_NNZ_SORT: a seeded random permutation, then a
  *   stable sort by column nnz (write_graph.jl:112-128); RCHOL_ORDER_RANDOM:
  *   the seeded permutation alone; RCHOL_ORDER_GIVEN: the input order;
+ *   RCHOL_ORDER_RCM / RCHOL_ORDER_ND: computed on the host (see below);
  *   ground vertex (write_graph.jl:153-163): when the entries sum to more
  *   than 1e-9, vertex n is appended with entries -c_j for every column sum
  *   c_j > 0 and diagonal sum c_j, and the context trims it after factoring
@@ -154,7 +155,23 @@ rchol_status rchol_set_triplets(rchol_ctx* ctx, int n, long long nnz, const int*
  * 0) or device (1).  perm (host, n entries, may be NULL) receives the
  * position of each input vertex in the context's matrix: right-hand sides
  * and solutions of the input's numbering map through it. */
-enum { RCHOL_ORDER_GIVEN = 0, RCHOL_ORDER_NNZ_SORT = 1, RCHOL_ORDER_RANDOM = 2 };
+enum {
+    RCHOL_ORDER_GIVEN = 0,
+    RCHOL_ORDER_NNZ_SORT = 1,
+    RCHOL_ORDER_RANDOM = 2,
+    RCHOL_ORDER_RCM = 3,  /* reverse Cuthill-McKee (host, from the pattern) */
+    RCHOL_ORDER_ND = 4    /* nested dissection by level-structure bisection (host); the
+                             reference's "amd" / "nd" come from Julia's AMD / Metis
+                             (write_graph.jl:61-75), not part of this build */
+};
+/* Host-only: the RCHOL_ORDER_RCM or RCHOL_ORDER_ND order of a symmetric
+ * pattern (0-based triplets; the diagonal is ignored): order[k] = vertex
+ * placed at position k.  Reverse Cuthill-McKee runs a breadth-first search
+ * per component from a pseudo-peripheral vertex, neighbours by ascending
+ * degree, and reverses it; nested dissection cuts each region's
+ * breadth-first levels at the median level (the separator, numbered after
+ * both halves) down to regions of 64 vertices. */
+rchol_status rchol_ordering(int kind, int n, long long nnz, const int* rows, const int* cols, int* order);
 rchol_status rchol_set_sddm(rchol_ctx* ctx, int n, long long nnz, const int* rows, const int* cols,
                             const double* vals, int on_device, int ordering, unsigned long long order_seed,
                             int* perm, int* has_ground);

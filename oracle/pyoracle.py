@@ -241,12 +241,13 @@ def order_keys(n, seed):
         return _mix64(base ^ np.arange(n, dtype=np.uint64))
 
 
-def sddm_to_laplacian(n, rows, cols, vals, ordering=1, seed=0):
+def sddm_to_laplacian(n, rows, cols, vals, ordering=1, seed=0, order=None):
     """Restatement of the physics preprocessing (cpu_implementation/
     write_graph.jl:98-183) as rchol_set_sddm performs it: sign
     normalisation (and a diagonal of sum |off| per column when the input has
     none), the ordering (0 given, 1 ascending column nnz after the seeded
-    permutation, 2 the seeded permutation), and the ground vertex appended
+    permutation, 2 the seeded permutation, or an explicit `order`), and the
+    ground vertex appended
     when the entries sum to more than 1e-9.  Column sums are added in row
     order, the ground diagonal in column order.  Returns
     (N, colptr, rowind, val, perm, has_ground).  Small inputs only."""
@@ -257,7 +258,9 @@ def sddm_to_laplacian(n, rows, cols, vals, ordering=1, seed=0):
     append_diag = not np.any(rows == cols)
     cnt = np.bincount(cols, minlength=n)
     ident = np.arange(n)
-    if ordering == 0:
+    if order is not None:  # an order computed elsewhere (RCM, nested dissection)
+        order = np.asarray(order, np.int64)
+    elif ordering == 0:
         order = ident
     else:
         key = order_keys(n, seed)

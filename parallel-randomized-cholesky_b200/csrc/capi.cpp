@@ -464,8 +464,9 @@ extern "C" rchol_status rchol_set_sddm(rchol_ctx* ctx, int n, long long nnz, con
                                        int* perm, int* has_ground) {
     if (!ctx || n <= 0 || nnz < 0 || (nnz > 0 && (!rows || !cols || !vals)))
         return fail(ctx, RCHOL_ERR_INVALID, "bad triplet arguments");
-    if (ordering != RCHOL_ORDER_GIVEN && ordering != RCHOL_ORDER_NNZ_SORT && ordering != RCHOL_ORDER_RANDOM)
-        return fail(ctx, RCHOL_ERR_INVALID, "ordering must be RCHOL_ORDER_GIVEN, _NNZ_SORT or _RANDOM");
+    if (ordering != RCHOL_ORDER_GIVEN && ordering != RCHOL_ORDER_NNZ_SORT && ordering != RCHOL_ORDER_RANDOM &&
+        ordering != RCHOL_ORDER_RCM && ordering != RCHOL_ORDER_ND)
+        return fail(ctx, RCHOL_ERR_INVALID, "ordering must be one of RCHOL_ORDER_*");
     if (nnz + 2 * (long long)n + 2 >= (long long)INT32_MAX)
         return fail(ctx, RCHOL_ERR_INVALID, "matrix too large for int32 indices");
     cudaSetDevice(ctx->device);
@@ -495,8 +496,36 @@ extern "C" rchol_status rchol_set_sddm(rchol_ctx* ctx, int n, long long nnz, con
         dcols = c;
         dvals = v;
     }
+    // RCM and nested dissection are computed on the host from the pattern
+    int32_t* dorder = nullptr;
+    int dev_ordering = ordering;
+    if (ordering == RCHOL_ORDER_RCM || ordering == RCHOL_ORDER_ND) {
+        std::vector<int32_t> hr, hc;
+        const int32_t *pr = rows, *pc = cols;
+        if (on_device) {
+            hr.resize((size_t)nnz);
+            hc.resize((size_t)nnz);
+            if (nnz > 0) {
+                CK(cudaMemcpy(hr.data(), rows, sizeof(int32_t) * (size_t)nnz, cudaMemcpyDeviceToHost), "copy pattern");
+                CK(cudaMemcpy(hc.data(), cols, sizeof(int32_t) * (size_t)nnz, cudaMemcpyDeviceToHost), "copy pattern");
+            }
+            pr = hr.data();
+            pc = hc.data();
+        }
+        std::vector<int32_t> ord;
+        std::string err;
+        if (!rchol::host_ordering(ordering == RCHOL_ORDER_RCM ? rchol::kHostOrderRcm : rchol::kHostOrderNd, n, nnz, pr,
+                                  pc, ord, err))
+            return fail(ctx, RCHOL_ERR_INVALID, err);
+        CK(ctx->scratch.get(&dorder, n), "alloc order");
+        CK(cudaMemcpyAsync(dorder, ord.data(), sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream),
+           "upload order");
+        CK(cudaStreamSynchronize(ctx->stream), "upload order");
+        dev_ordering = rchol::kOrderExternal;
+    }
     rchol::SddmResult res;
-    CK(rchol::sddm_to_laplacian(n, nnz, drows, dcols, dvals, ordering, order_seed, ctx->scratch, ctx->stream, res),
+    CK(rchol::sddm_to_laplacian(n, nnz, drows, dcols, dvals, dev_ordering, order_seed, ctx->scratch, ctx->stream, res,
+                                dorder),
        "sddm conversion");
     if (res.status == rchol::SddmResult::kBadIndex) return fail(ctx, RCHOL_ERR_INVALID, "triplet index out of range");
     if (res.status == rchol::SddmResult::kNotDominant)
@@ -504,6 +533,18 @@ extern "C" rchol_status rchol_set_sddm(rchol_ctx* ctx, int n, long long nnz, con
     if (perm) CK(cudaMemcpy(perm, res.perm, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost), "copy permutation");
     if (has_ground) *has_ground = res.ground ? 1 : 0;
     return rchol_set_csc(ctx, res.n, res.colptr, res.rowind, res.val, 1, res.ground ? 1 : 0);
+}
+
+extern "C" rchol_status rchol_ordering(int kind, int n, long long nnz, const int* rows, const int* cols, int* order) {
+    if (n <= 0 || nnz < 0 || (nnz > 0 && (!rows || !cols)) || !order) return RCHOL_ERR_INVALID;
+    if (kind != RCHOL_ORDER_RCM && kind != RCHOL_ORDER_ND) return RCHOL_ERR_INVALID;
+    std::vector<int32_t> ord;
+    std::string err;
+    if (!rchol::host_ordering(kind == RCHOL_ORDER_RCM ? rchol::kHostOrderRcm : rchol::kHostOrderNd, n, nnz, rows, cols,
+                              ord, err))
+        return RCHOL_ERR_INVALID;
+    std::memcpy(order, ord.data(), sizeof(int) * (size_t)n);
+    return RCHOL_OK;
 }
 
 extern "C" rchol_status rchol_write_bin(const char* path, int n, const int* colptr, const int* rowind,

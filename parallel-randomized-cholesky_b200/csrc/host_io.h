@@ -36,6 +36,13 @@ bool write_csc_bin(const std::string& path, int32_t n, const int32_t* colptr, co
                    const double* val, int trim, std::string& err);
 bool read_csc_bin(const std::string& path, HostCsc& out, int& trim, std::string& err);
 
+// Host orderings of a symmetric pattern (0-based triplets, diagonal ignored):
+// order[k] = vertex placed at position k (host_order.cpp).
+constexpr int kHostOrderRcm = 3;  // reverse Cuthill-McKee
+constexpr int kHostOrderNd = 4;   // nested dissection by level-structure bisection
+bool host_ordering(int kind, int32_t n, int64_t nnz, const int32_t* rows, const int32_t* cols,
+                   std::vector<int32_t>& order, std::string& err);
+
 // sparse_matrix_processor preprocessing (pre_process.hpp:189-306, 338-356):
 // off-diagonals -> -|v|, diagonal -> |v|, diagonal appended as the column
 // sum of |off-diagonals| when the input has none, CSC sorted by (col,row),

@@ -192,10 +192,13 @@ __global__ void ground_append_kernel(int32_t n, const int32_t* __restrict__ colp
 }  // namespace
 
 cudaError_t sddm_to_laplacian(int32_t n, int64_t nnz, const int32_t* rows, const int32_t* cols, const double* vals,
-                              int ordering, uint64_t seed, Scratch& sc, cudaStream_t s, SddmResult& res) {
+                              int ordering, uint64_t seed, Scratch& sc, cudaStream_t s, SddmResult& res,
+                              const int32_t* order_in) {
     res = SddmResult();
     if (n <= 0 || nnz < 0 || nnz + 2 * (int64_t)n + 2 >= (int64_t)INT32_MAX) return cudaErrorInvalidValue;
-    if (ordering != kOrderGiven && ordering != kOrderNnzSort && ordering != kOrderRandom) return cudaErrorInvalidValue;
+    if (ordering != kOrderGiven && ordering != kOrderNnzSort && ordering != kOrderRandom &&
+        !(ordering == kOrderExternal && order_in))
+        return cudaErrorInvalidValue;
     int32_t *cnt = nullptr, *flags = nullptr, *order = nullptr;
     RCHOL_TRY(sc.get(&cnt, n));
     RCHOL_TRY(sc.get(&flags, 2));
@@ -214,9 +217,13 @@ cudaError_t sddm_to_laplacian(int32_t n, int64_t nnz, const int32_t* rows, const
     }
     const int append_diag = hf[1] ? 0 : 1;  // (every column then gains one: the count order is unchanged)
     // the permutation: order[k] = input vertex placed at position k
-    iota_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, order);
-    RCHOL_TRY(cudaGetLastError());
-    if (ordering != kOrderGiven) {
+    if (ordering == kOrderExternal) {
+        RCHOL_TRY(cudaMemcpyAsync(order, order_in, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+    } else {
+        iota_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, order);
+        RCHOL_TRY(cudaGetLastError());
+    }
+    if (ordering == kOrderNnzSort || ordering == kOrderRandom) {
         int32_t *klo = nullptr, *khi = nullptr;
         RCHOL_TRY(sc.get(&klo, n));
         RCHOL_TRY(sc.get(&khi, n));

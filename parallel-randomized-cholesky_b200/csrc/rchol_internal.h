@@ -300,7 +300,7 @@ cudaError_t stable_key_order_carried(const int32_t* key, int32_t n, int32_t nkey
                                      cudaStream_t s);
 
 // ---- SDDM -> ordered Laplacian (ordering.cu) ------------------------------
-constexpr int kOrderGiven = 0, kOrderNnzSort = 1, kOrderRandom = 2;
+constexpr int kOrderGiven = 0, kOrderNnzSort = 1, kOrderRandom = 2, kOrderExternal = -1;
 // A converted matrix: CSC (rows ascending per column, duplicates kept) in
 // the scratch arena, and the position of each input vertex.
 struct SddmResult {
@@ -319,8 +319,11 @@ struct SddmResult {
 // normalised, ordered (kOrder*; `seed` keys the random permutation), and a
 // ground vertex appended when the entries sum to more than 1e-9
 // (write_graph.jl:98-183).  Synchronises `s`.
+// kOrderExternal takes the order from `order_in` (device [n]: vertex placed
+// at each position).
 cudaError_t sddm_to_laplacian(int32_t n, int64_t nnz, const int32_t* rows, const int32_t* cols, const double* vals,
-                              int ordering, uint64_t seed, Scratch& sc, cudaStream_t s, SddmResult& res);
+                              int ordering, uint64_t seed, Scratch& sc, cudaStream_t s, SddmResult& res,
+                              const int32_t* order_in = nullptr);
 
 // ---- scans (scan.cu) -------------------------------------------------------
 // out[0] = 0, out[i+1] = sum(in[0..i]); out has n+1 entries.  Uses `tmp`

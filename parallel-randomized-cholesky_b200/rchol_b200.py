@@ -23,7 +23,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "i/o error", 3: "CUDA error", 4: "c
           5: "timeout", 6: "not converged", 7: "no CUDA device", 8: "numeric", 9: "no matrix"}
 PREC_FP64, PREC_FP32_FACTOR = 0, 1
 STOP_RELRES, STOP_PRECOND, STOP_ABS_R2 = 0, 1, 2
-ORDER_GIVEN, ORDER_NNZ_SORT, ORDER_RANDOM = 0, 1, 2
+ORDER_GIVEN, ORDER_NNZ_SORT, ORDER_RANDOM, ORDER_RCM, ORDER_ND = 0, 1, 2, 3, 4
 SPMV_AUTO, SPMV_CSR = 0, 1
 
 # every symbol include/rchol.h declares
@@ -35,7 +35,7 @@ EXPORTS = sorted([
     "rchol_factor_free", "rchol_pcg_solve", "rchol_precond_apply", "rchol_precond_apply_noalloc", "rchol_profile_solve", "rchol_spmv", "rchol_factorization_driver",
     "rchol_prepare_and_solve", "rchol_generate", "rchol_free_host", "rchol_write_mtx", "rchol_batch_set",
     "rchol_batch_solve", "rchol_zero_sum_vector", "rchol_set_sddm", "rchol_write_bin", "rchol_read_bin",
-    "rchol_save_bin", "rchol_load_bin", "rchol_autotune",
+    "rchol_save_bin", "rchol_load_bin", "rchol_autotune", "rchol_ordering",
 ])
 
 
@@ -149,6 +149,7 @@ def lib():
         L.rchol_save_bin.argtypes = [vp, C.c_char_p]
         L.rchol_load_bin.argtypes = [vp, C.c_char_p]
         L.rchol_autotune.argtypes = [vp, C.c_int, C.POINTER(TuneResult)]
+        L.rchol_ordering.argtypes = [C.c_int, C.c_int, C.c_longlong, vp, vp, vp]
         L.rchol_set_sddm.argtypes = [vp, C.c_int, C.c_longlong, vp, vp, vp, C.c_int, C.c_int, C.c_ulonglong, vp,
                                      i32p]
         L.rchol_batch_set.argtypes = [vp, C.c_int, C.POINTER(System), C.POINTER(C.c_longlong)]
@@ -261,6 +262,16 @@ def read_bin(path):
     finally:
         for p in (cp, ri, v):
             L.rchol_free_host(C.cast(p, C.c_void_p))
+    return out
+
+
+def ordering(kind, n, rows, cols):
+    """Host RCM (ORDER_RCM) or nested-dissection (ORDER_ND) order of a
+    symmetric pattern: order[k] = vertex placed at position k."""
+    rows = np.ascontiguousarray(rows, np.int32)
+    cols = np.ascontiguousarray(cols, np.int32)
+    out = np.zeros(n, np.int32)
+    _check(lib().rchol_ordering(int(kind), int(n), len(rows), _ptr(rows), _ptr(cols), _ptr(out)))
     return out
 
 

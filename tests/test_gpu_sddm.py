@@ -89,3 +89,29 @@ def test_set_sddm_solve_in_input_numbering():
         f.free()
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("ordering", [R.ORDER_RCM, R.ORDER_ND])
+def test_set_sddm_host_orderings(ordering):
+    """RCM and nested dissection are computed on the host from the pattern
+    (rchol_ordering) and applied by the device conversion; the factor of the
+    reordered system solves the input's system."""
+    n, r, c, v = _natural_sddm("grid3d", [13, 12, 11], wlo=1e-3, whi=1e3, log_weights=True, excess_frac=0.05,
+                               excess_lo=0.0, excess_hi=1e-2, seed=2)
+    order = R.ordering(ordering, n, r, c)
+    N, cp, ri, val, perm, g = O.sddm_to_laplacian(n, r, c, v, order=order)
+    ctx = R.Context(seed=6, tol=1e-8)
+    try:
+        dperm, dg = ctx.set_sddm(n, r, c, v, ordering=ordering)
+        Nd, cpd, rid, vald = ctx.matrix()
+        assert dg == g and np.array_equal(dperm, perm)
+        assert np.array_equal(cpd, cp) and np.array_equal(rid, ri) and np.array_equal(vald, val)
+        f = ctx.factor()
+        b = np.random.default_rng(1).standard_normal(n)
+        bp = np.empty(n)
+        bp[dperm] = b
+        xp, info = ctx.pcg_solve(f, bp)
+        assert info["converged"]
+        f.free()
+    finally:
+        ctx.close()

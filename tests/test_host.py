@@ -271,3 +271,57 @@ def test_binary_matrix_cache_roundtrip(tmp_path):
         f.write(np.array([n + 7], np.int32).tobytes())
     with pytest.raises(R.RcholError):
         R.read_bin(path)
+
+
+def _etree_height(n, rows, cols, order):
+    """Height of the elimination tree of the pattern in `order` (Liu's
+    algorithm with path compression)."""
+    pos = np.empty(n, np.int64)
+    pos[order] = np.arange(n)
+    pr, pc = pos[rows], pos[cols]
+    m = pr > pc
+    # rows of the permuted lower triangle, by column... the etree needs, for
+    # each row i, its columns j < i
+    byrow = [[] for _ in range(n)]
+    for i, j in zip(pr[m], pc[m]):
+        byrow[i].append(j)
+    parent = [-1] * n
+    anc = [-1] * n
+    for i in range(n):
+        for j in byrow[i]:
+            while j != -1 and j < i:
+                nxt = anc[j]
+                anc[j] = i
+                if nxt == -1:
+                    parent[j] = i
+                j = nxt
+    height = [0] * n
+    for i in range(n):
+        if parent[i] != -1:
+            height[parent[i]] = max(height[parent[i]], height[i] + 1)
+    return max(height)
+
+
+def test_host_orderings():
+    """RCM narrows the bandwidth of a randomly ordered grid; nested dissection
+    gives a shallow elimination tree; both are permutations, also of a
+    disconnected graph."""
+    n, r, c, v, g = R.generate("grid3d", [16, 15, 14], ordering=1, seed=3)
+    pos = lambda o: np.argsort(o)
+    m = r != c
+    rcm = R.ordering(R.ORDER_RCM, n, r, c)
+    nd = R.ordering(R.ORDER_ND, n, r, c)
+    for o in (rcm, nd):
+        assert np.array_equal(np.sort(o), np.arange(n))
+    bw = lambda o: np.abs(pos(o)[r[m]] - pos(o)[c[m]]).max()
+    assert bw(rcm) < 0.1 * bw(np.arange(n))
+    n2, r2, c2, v2, g2 = R.generate("grid2d", [40, 40], seed=4, ordering=2)
+    h_nd = _etree_height(n2, r2, c2, R.ordering(R.ORDER_ND, n2, r2, c2))
+    h_rcm = _etree_height(n2, r2, c2, R.ordering(R.ORDER_RCM, n2, r2, c2))
+    assert h_nd < 0.6 * h_rcm
+    # two disjoint grids
+    rr = np.concatenate([r2, r2 + n2])
+    cc = np.concatenate([c2, c2 + n2])
+    for kind in (R.ORDER_RCM, R.ORDER_ND):
+        o = R.ordering(kind, 2 * n2, rr, cc)
+        assert np.array_equal(np.sort(o), np.arange(2 * n2))
