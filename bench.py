@@ -74,9 +74,11 @@ def parse():
     p.add_argument("--no-autotune", action="store_true", help="secondary configs: keep the default options")
     p.add_argument("--profile-run", action="store_true",
                    help="one factorization + one PCG solve of the config (mixed form), for profilers")
-    p.add_argument("--size", type=int, default=0, help="grid side override for --profile-run (small ncu cases)")
+    p.add_argument("--size", type=int, default=0,
+                   help="--profile-run: grid side, or Chung-Lu vertex count (10 edges per vertex), for small ncu cases")
     p.add_argument("--max-iter", type=int, default=0, help="PCG iteration cap for --profile-run")
     p.add_argument("--rhs", type=int, default=1, help="right-hand sides of the --profile-run solve")
+    p.add_argument("--tail", type=int, default=0, help="cooperative tail vertices for --profile-run")
     return p.parse_args()
 
 
@@ -788,12 +790,16 @@ def profile_run(args, cfg):
     cfg = dict(cfg)
     if args.size and cfg["kind"].startswith("grid"):
         cfg["dims"] = [args.size] * len(cfg["dims"])
+    elif args.size and cfg["kind"] == "chunglu":
+        cfg["dims"] = [args.size, 10 * args.size] + list(cfg["dims"][2:])
     W = build_workload(cfg)
     n, ground = W["n"], W["ground"]
     ns = n - 1 if ground else n
     kw = dict(seed=1, precision=R.PREC_FP32_FACTOR, tol=cfg["tol"])
     if args.max_iter:
         kw["max_iter"] = args.max_iter
+    if args.tail:
+        kw["tail_vertices"] = args.tail
     ctx = R.Context(**kw)
     ctx.set_csc(n, W["colptr"], W["rowind"], W["val"], trim_ground=ground)
     f = ctx.factor()
