@@ -355,6 +355,13 @@ def run_b200(args, cfg, rank, world, local):
     peak, peak_src = measured_peaks()
     achieved = ab[dom] / (per_launch[dom] / 1000.0) / 1e9
     traffic = committed_traffic().get(dom)
+    # latency floor of the k = 1 solves: DAG depth x the measured store -> poll hop
+    hop_ns, hop_sms = ctx["mixed"].hop_latency(4096)
+    lat = {"hop_ns": round(hop_ns, 1), "hop_sms": list(hop_sms)}
+    for name, depth in (("fwd_solve", fi32.solve_depth), ("bwd_solve", fi32.solve_depth_b)):
+        floor_ms = depth * hop_ns / 1e6
+        lat[name] = {"depth": int(depth), "floor_ms": round(floor_ms, 4), "achieved_ms": round(per_launch[name], 4),
+                     "frac": round(floor_ms / per_launch[name], 3)}
 
     # 32 right-hand sides through one block solve vs the single-RHS solve
     k32 = 32
@@ -416,6 +423,7 @@ def run_b200(args, cfg, rank, world, local):
                      "frac": round(achieved / peak, 4), "peak_source": peak_src,
                      "traffic": traffic, "algorithmic_bytes": ab[dom],
                      "all_kernels_GBps": {k: round(ab[k] / (per_launch[k] / 1000.0) / 1e9, 1) for k in ab}},
+        "latency_roofline": lat,
         "e2e": {"value": round(e2e_s, 6), "unit": "s",
                 "h2d_bytes_per_step": int(W["colptr"].nbytes + W["rowind"].nbytes + W["val"].nbytes + b.nbytes),
                 "d2h_bytes_per_step": int(ns * 8), "statistic": "median of 5 calls",

@@ -76,6 +76,9 @@ typedef struct rchol_opts {
                                  power-law graphs); 0 = none; rchol_autotune picks it */
     int rhs_block;            /* multi-RHS PCG: solve k right-hand sides in blocks of this width
                                  (1, 2, 4, 8, 16, 32; 0 = all k at once); rchol_autotune picks it */
+    int bwd_head;             /* one-RHS PCG (exact backward levels): solve the narrow first levels
+                                 of the backward DAG in one CTA with the values in shared memory
+                                 before the persistent kernel (default 1; 0 = off) */
 } rchol_opts;
 
 typedef struct rchol_factor_info {
@@ -104,6 +107,9 @@ typedef struct rchol_factor_info {
     const double* lr_val;
     const double* diag;       /* D [n] */
     int tail_vertices;        /* vertices eliminated by the cooperative tail pass */
+    int solve_depth_b;        /* levels of the backward-solve DAG (exact levels) */
+    int bwd_head_levels;      /* backward levels solved by the one-CTA head kernel (0: none) */
+    int bwd_head_rows;        /* rows in those levels */
 } rchol_factor_info;
 
 typedef struct rchol_solve_info {
@@ -286,6 +292,13 @@ rchol_status rchol_autotune(rchol_ctx* ctx, int max_rhs, rchol_tune_result* out)
  * iterations on this factor with k right-hand sides: ms_out[0] SpMV +
  * vector update, ms_out[1] forward solve, ms_out[2] backward solve. */
 rchol_status rchol_profile_solve(rchol_ctx* ctx, const rchol_factor_t* f, int k, int reps, float* ms_out);
+/* The latency floor of the sync-free triangular solves: the mean time (ns)
+ * of one producer -> consumer hop, a relaxed store on one SM seen by a
+ * polling load on another, measured by two co-resident CTAs passing a
+ * counter back and forth `rounds` times (64 .. 2^20) on the context's device.
+ * A solve of depth d cannot finish in less than d hops.  sm_pair (may be
+ * NULL) receives the two CTAs' SM ids.  No reference counterpart. */
+rchol_status rchol_hop_latency(rchol_ctx* ctx, int rounds, double* ns_per_hop, int* sm_pair);
 /* Y = A X with the (trimmed) matrix of the context. */
 rchol_status rchol_spmv(rchol_ctx* ctx, int k, const double* X, double* Y, int ldb, int on_device);
 

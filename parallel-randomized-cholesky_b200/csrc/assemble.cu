@@ -531,6 +531,49 @@ cudaError_t dmalloc(T** p, int64_t n) {
     return cudaMalloc((void**)p, sizeof(T) * (size_t)(n > 0 ? n : 1));
 }
 
+// Level table of the backward schedule's first lvcap levels: lv[l] = {first
+// task, first slab unit, first position} of level l, written by the task that
+// opens the level (levels are contiguous in task order), plus the end of
+// the last level when it falls inside the table.  split_min receives the
+// lowest level holding a part task.
+__global__ void head_level_kernel(int32_t npt, const int4* __restrict__ pack, const int32_t* __restrict__ order,
+                                  const int32_t* __restrict__ level, int32_t n, int32_t lvcap, int4* lv,
+                                  int32_t* split_min) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < npt; t += stride) {
+        const int4 d = pack[t];
+        const int32_t l = level[order[d.x]];
+        if (l > lvcap) continue;
+        if (t == 0 || level[order[pack[t - 1].x]] != l) lv[l] = make_int4((int)t, d.y, d.x, 0);
+        if (((d.z >> 11) & 1) && l < lvcap) atomicMin(split_min, l);
+        if (t == npt - 1 && l + 1 <= lvcap) lv[l + 1] = make_int4(npt, d.y + (d.w & 0xff), n, 0);
+    }
+}
+
+__global__ void invert_order_kernel(int32_t n, const int32_t* __restrict__ order, int32_t* pos) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) pos[order[p]] = (int32_t)p;
+}
+
+// Head slab slots with row indices replaced by positions in order_b; a
+// position outside the head (which the level structure rules out) sets bad.
+__global__ void head_idx_kernel(int64_t nslots, const int32_t* __restrict__ pidx, const int32_t* __restrict__ pos,
+                                int32_t rows, int32_t* out, int32_t* bad) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += stride) {
+        const int32_t j = pidx[s];
+        int32_t q = -1;
+        if (j >= 0) {
+            q = pos[j];
+            if (q >= rows) {
+                *bad = 1;
+                q = -1;
+            }
+        }
+        out[s] = q;
+    }
+}
+
 }  // namespace
 
 // (Re)allocate a persistent buffer that shares the capacity `cap` with its
@@ -556,7 +599,7 @@ static cudaError_t ensure(T** p, int64_t& cap, int64_t need) {
 }
 
 cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp32, int epl, bool exact_bwd,
-                            double timeout_s, Scratch& sc, DevFactor& f, cudaStream_t s) {
+                            bool bwd_head, double timeout_s, Scratch& sc, DevFactor& f, cudaStream_t s) {
     const int32_t nout = trim_ground ? w.n - 1 : w.n;
     const int32_t ground = trim_ground ? w.n - 1 : -1;
     f.n = nout;
@@ -666,7 +709,7 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
         to_f32_kernel<<<grid_for(nout, 256), 256, 0, s>>>(f.diag, f.diag32, nout);
         RCHOL_TRY(cudaGetLastError());
     }
-    RCHOL_TRY(build_solve_schedule(f, w.level, epl, exact_bwd, timeout_s, sc, s));
+    RCHOL_TRY(build_solve_schedule(f, w.level, epl, exact_bwd, bwd_head, timeout_s, sc, s));
     RCHOL_TRY(cudaStreamSynchronize(s));
     sc.reset();
     return cudaSuccess;
@@ -861,9 +904,63 @@ static cudaError_t build_layouts(DevFactor& f, const int32_t* level_f, const int
     return cudaSuccess;
 }
 
-cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bool exact_bwd, double timeout_s,
-                                 Scratch& sc, cudaStream_t s) {
+// The backward head (see DevFactor::hb_nlev): levels from the first while
+// each holds at most kHeadMaxRows rows, kHeadMaxTasks tasks and no part
+// task, and the head's rows, level table and largest stage (FP64 values, so
+// that either value type fits) fit the kernel's shared memory.  Fewer than
+// kHeadMinLevels such levels leave the head empty.
+static cudaError_t build_bwd_head(DevFactor& f, const int32_t* levb, Scratch& sc, cudaStream_t s) {
+    f.hb_nlev = f.hb_ntask = f.hb_rows = f.hb_stage = 0;
+    const int32_t lvcap = std::min<int32_t>(f.depth_b, kHeadMaxLevels);
+    if (f.npt_b == 0 || lvcap < kHeadMinLevels) return cudaSuccess;
+    int4* lv = nullptr;
+    int32_t* flags = nullptr;  // [0] lowest split level, [1] bad index
+    RCHOL_TRY(sc.get(&lv, (int64_t)lvcap + 1));
+    RCHOL_TRY(sc.get(&flags, 2));
+    const int32_t init[2] = {INT32_MAX, 0};
+    RCHOL_TRY(cudaMemcpyAsync(flags, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    head_level_kernel<<<grid_for(f.npt_b, 256), 256, 0, s>>>(f.npt_b, f.pack_b, f.order_b, levb, f.n, lvcap, lv,
+                                                             flags);
+    RCHOL_TRY(cudaGetLastError());
+    std::vector<int4> h((size_t)lvcap + 1);
+    int32_t hf[2] = {0, 0};
+    RCHOL_TRY(cudaMemcpyAsync(h.data(), lv, sizeof(int4) * h.size(), cudaMemcpyDeviceToHost, s));
+    RCHOL_TRY(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, s));
+    RCHOL_TRY(cudaStreamSynchronize(s));
+    int nlev = 0, stage = 0;
+    for (int l = 0; l < lvcap && l < hf[0]; ++l) {
+        const int ntask = h[l + 1].x - h[l].x, units = h[l + 1].y - h[l].y, rows = h[l + 1].z - h[l].z;
+        if (rows > kHeadMaxRows || ntask > kHeadMaxTasks) break;
+        const int st = std::max(stage, head_stage_bytes(ntask, units, rows, 8));
+        if (head_smem_bytes(h[l + 1].z, l + 1, st) > kHeadSmem) break;
+        stage = st;
+        nlev = l + 1;
+    }
+    if (nlev < kHeadMinLevels) return cudaSuccess;
+    const int32_t rows = h[nlev].z;
+    const int64_t nslots = (int64_t)h[nlev].y * 32;
+    int32_t* pos = nullptr;
+    RCHOL_TRY(sc.get(&pos, f.n));
+    RCHOL_TRY(ensure(&f.hb_lv, f.cap_hl, (int64_t)kHeadMaxLevels + 1));
+    RCHOL_TRY(ensure(&f.hb_idx, f.cap_hi, std::max<int64_t>(nslots, 32)));
+    invert_order_kernel<<<grid_for(f.n, 256), 256, 0, s>>>(f.n, f.order_b, pos);
+    head_idx_kernel<<<grid_for(nslots, 256), 256, 0, s>>>(nslots, f.pb_idx, pos, rows, f.hb_idx, flags + 1);
+    RCHOL_TRY(cudaGetLastError());
+    RCHOL_TRY(cudaMemcpyAsync(f.hb_lv, lv, sizeof(int4) * ((size_t)nlev + 1), cudaMemcpyDeviceToDevice, s));
+    RCHOL_TRY(cudaMemcpyAsync(&hf[1], flags + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    RCHOL_TRY(cudaStreamSynchronize(s));
+    if (hf[1] != 0) return cudaSuccess;  // not a head after all: leave it empty
+    f.hb_nlev = nlev;
+    f.hb_ntask = h[nlev].x;
+    f.hb_rows = rows;
+    f.hb_stage = stage;
+    return cudaSuccess;
+}
+
+cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bool exact_bwd, bool bwd_head,
+                                 double timeout_s, Scratch& sc, cudaStream_t s) {
     if (epl < 1) epl = 1;
+    f.hb_nlev = f.hb_ntask = f.hb_rows = f.hb_stage = 0;
     {
         const bool grow_n = f.cap_n < (int64_t)f.n + 1;
         const int64_t capn = std::max<int64_t>(f.cap_n, (int64_t)f.n + 1);
@@ -905,6 +1002,7 @@ cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bo
     RCHOL_TRY(build_one_schedule(levb, f.lc_ptr, f.n, f.depth_b, 0, epl, sc, f.order_b, &f.tasks_b, f.cap_tb,
                                  &f.ntasks_b, s));
     RCHOL_TRY(build_layouts(f, level, levb, 1, sc, s));
+    if (bwd_head) RCHOL_TRY(build_bwd_head(f, levb, sc, s));
     return cudaStreamSynchronize(s);
 }
 

@@ -110,7 +110,8 @@ void free_factor(DevFactor& f) {
                   f.lr_val32, f.diag, f.diag32, f.order_f, f.order_b, f.tasks_f, f.tasks_b,
                   f.sf_ptr, f.sf_idx, f.sf_val, f.sf_val32, f.sb_ptr, f.sb_idx, f.sb_val, f.sb_val32,
                   f.pack_f, f.pack_b, f.pf_idx, f.pf_val, f.pf_val32, f.pb_idx, f.pb_val, f.pb_val32,
-                  f.split_f, f.split_b, f.psum_f, f.psum_b, f.pcount_f, f.pcount_b, f.srow_f, f.srow_b};
+                  f.split_f, f.split_b, f.psum_f, f.psum_b, f.pcount_f, f.pcount_b, f.srow_f, f.srow_b,
+                  f.hb_lv, f.hb_idx};
     for (void* p : ps) cudaFree(p);
     f = DevFactor();
 }
@@ -269,6 +270,7 @@ extern "C" rchol_status rchol_opts_default(rchol_opts* o) {
     o->spmv_layout = RCHOL_SPMV_AUTO;
     o->tail_vertices = 0;
     o->rhs_block = 0;
+    o->bwd_head = 1;
     return RCHOL_OK;
 }
 
@@ -290,6 +292,7 @@ static rchol_status check_opts(const rchol_opts* o, std::string& why) {
     else if (o->rhs_block != 0 && o->rhs_block != 1 && o->rhs_block != 2 && o->rhs_block != 4 && o->rhs_block != 8 &&
              o->rhs_block != 16 && o->rhs_block != 32)
         why = "rhs_block must be 0 or 1, 2, 4, 8, 16, 32";
+    else if (o->bwd_head != 0 && o->bwd_head != 1) why = "bwd_head must be 0 or 1";
     else return RCHOL_OK;
     return RCHOL_ERR_INVALID;
 }
@@ -723,7 +726,8 @@ extern "C" rchol_status rchol_factor(rchol_ctx* ctx, rchol_factor_t** out) {
     f->F = ctx->spare;  // reuse the buffers of the last released factor
     ctx->spare = DevFactor();
     cudaError_t e = rchol::assemble_factor(w, ctx->trim, o.precision == RCHOL_PREC_FP32_FACTOR, o.sched_epl,
-                                           o.exact_bwd_levels != 0, o.timeout_s, ctx->scratch, f->F, ctx->stream);
+                                           o.exact_bwd_levels != 0, o.bwd_head != 0, o.timeout_s, ctx->scratch,
+                                           f->F, ctx->stream);
     if (e != cudaSuccess) {
         free_factor(f->F);
         delete f;
@@ -753,6 +757,9 @@ extern "C" rchol_status rchol_factor(rchol_ctx* ctx, rchol_factor_t** out) {
     info.factor_grid = grid;
     info.attempts = attempt + 1;
     info.solve_depth = f->F.depth;
+    info.solve_depth_b = f->F.depth_b;
+    info.bwd_head_levels = f->F.hb_nlev;
+    info.bwd_head_rows = f->F.hb_rows;
     // setup (count, 3-pass scan, scatter, queue) + elimination + assembly
     // (counts, scans, scatter, transpose, maxima, row sorts, level order)
     info.kernel_launches = 6 + 1 + 1 + 3 + 1 + 3 + 1 + 2 + 1 + 1 + 1 + 3 + 1 +
@@ -767,6 +774,8 @@ extern "C" rchol_status rchol_factor(rchol_ctx* ctx, rchol_factor_t** out) {
     info.fills = (long long)c64[1];
     info.tail_vertices = std::min<int32_t>(std::max(0, o.tail_vertices), ctx->A.n);
     if (info.tail_vertices > 0) ++info.kernel_launches;
+    // backward head: level table, then (when built) the inverse order and its slab indices
+    if (o.exact_bwd_levels && o.bwd_head) info.kernel_launches += 1 + (f->F.hb_nlev > 0 ? 2 : 0);
     f->info = info;
     *out = f;
     return RCHOL_OK;
@@ -868,7 +877,8 @@ rchol_status factor_from_host_csc(rchol_ctx* ctx, int32_t n, const std::vector<i
             for (int32_t i = 0; i < n; ++i) longest = std::max(longest, rp[(size_t)i + 1] - rp[(size_t)i]);
             epl = rchol::auto_sched_epl(longest);
         }
-        e = rchol::build_solve_schedule(F, dlev, epl, ctx->o.exact_bwd_levels != 0, ctx->o.timeout_s,
+        e = rchol::build_solve_schedule(F, dlev, epl, ctx->o.exact_bwd_levels != 0, ctx->o.bwd_head != 0,
+                                        ctx->o.timeout_s,
                                         ctx->scratch, ctx->stream);
         ctx->scratch.reset();
     }
@@ -890,6 +900,9 @@ rchol_status factor_from_host_csc(rchol_ctx* ctx, int32_t n, const std::vector<i
     f->info.lr_val = F.lr_val;
     f->info.diag = F.diag;
     f->info.solve_depth = depth;
+    f->info.solve_depth_b = F.depth_b;
+    f->info.bwd_head_levels = F.hb_nlev;
+    f->info.bwd_head_rows = F.hb_rows;
     *out = f;
     return RCHOL_OK;
 }
@@ -1387,6 +1400,15 @@ extern "C" rchol_status rchol_profile_solve(rchol_ctx* ctx, const rchol_factor_t
     CK(cudaMemcpyAsync(ctx->dB, b.data(), sizeof(double) * elems, cudaMemcpyHostToDevice, ctx->stream), "upload");
     CK(rchol::pcg_profile(ctx->solver, ctx->dB, ctx->dX, reps, ms_out), "profile");
     CK(cudaStreamSynchronize(ctx->stream), "sync");
+    return RCHOL_OK;
+}
+
+extern "C" rchol_status rchol_hop_latency(rchol_ctx* ctx, int rounds, double* ns_per_hop, int* sm_pair) {
+    if (!ctx || !ns_per_hop || rounds < 64 || rounds > (1 << 20)) return fail(ctx, RCHOL_ERR_INVALID, "bad argument");
+    cudaSetDevice(ctx->device);
+    const cudaError_t e = rchol::hop_latency(rounds, ns_per_hop, sm_pair);
+    if (e == cudaErrorTimeout) return fail(ctx, RCHOL_ERR_TIMEOUT, "hop probe: a wait ran out (2 s)");
+    CK(e, "hop probe");
     return RCHOL_OK;
 }
 

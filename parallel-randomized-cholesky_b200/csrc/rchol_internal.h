@@ -215,6 +215,17 @@ struct DevFactor {
             cap_pwb = 0;
     int32_t depth = 0;        // number of levels of the forward solve DAG
     int32_t depth_b = 0;      // levels of the backward schedule
+    // Backward head: the first hb_nlev levels of the backward schedule
+    // (exact levels only), narrow levels of the vertices eliminated last
+    // whose rows depend only on earlier head rows.  One CTA solves them
+    // before the persistent kernel, which then starts at task hb_ntask.
+    // hb_lv[l] = {first task, first slab unit, first position in order_b, 0}
+    // for l <= hb_nlev; hb_idx holds the head's slab slots with every index
+    // replaced by its position in order_b (-1 past a row's end).
+    int32_t hb_nlev = 0, hb_ntask = 0, hb_rows = 0, hb_stage = 0;
+    int4* hb_lv = nullptr;
+    int32_t* hb_idx = nullptr;
+    int64_t cap_hl = 0, cap_hi = 0;
     // allocated capacities (buffers of a released factor are reused)
     int64_t cap_n = 0, cap_nnz = 0, cap_tf = 0, cap_tb = 0, cap_ln = 0, cap_lz = 0;
 };
@@ -239,8 +250,33 @@ constexpr int kLaneClasses = 6;
 // (stencil factors; measured 2-4% faster solves), else 2 (power-law factors,
 // whose long rows run slower with fewer lanes).
 inline int auto_sched_epl(int64_t max_row_len) { return max_row_len <= 1024 ? 3 : 2; }
-cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bool exact_bwd, double timeout_s,
-                                 Scratch& sc, cudaStream_t s);
+// Shared-memory plan of the backward-head kernel: the head holds at most
+// kHeadMaxLevels levels of at most kHeadMaxRows rows and kHeadMaxTasks
+// tasks each; its stages (one level each, kHeadStages in flight) and the
+// per-row arrays fit kHeadSmem.
+constexpr int kHeadThreads = 512;
+constexpr int kHeadStages = 5;
+constexpr int kHeadMaxLevels = 1024;
+constexpr int kHeadMaxRows = 1024;
+// one task per warp of the 16-warp CTA: levels with more tasks than warps
+// took longer in the head kernel than in the persistent one
+constexpr int kHeadMaxTasks = kHeadThreads / 32;
+constexpr int kHeadMinLevels = 8;
+constexpr int kHeadSmem = 220 * 1024;
+// Bytes of one head stage (a level's descriptors, slab slots and row
+// scalars) for value size vb, each part 16-byte aligned.
+inline int head_stage_bytes(int ntask, int units, int rows, int vb) {
+    auto al = [](int x) { return (x + 15) & ~15; };
+    return 16 * ntask + 128 * units + 32 * vb * units + 2 * al(8 * rows) + al(vb * rows);
+}
+// Dynamic shared memory of the head kernel: row ids and z values of every
+// head row, the level table and the stages.
+inline int head_smem_bytes(int rows, int nlev, int stage) {
+    return ((4 * rows + 15) & ~15) + ((8 * rows + 15) & ~15) + 16 * (nlev + 1) + kHeadStages * stage;
+}
+// bwd_head (exact levels only): build the backward head (DevFactor::hb_nlev).
+cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bool exact_bwd, bool bwd_head,
+                                 double timeout_s, Scratch& sc, cudaStream_t s);
 
 struct FactorLaunch {
     int grid = 0;
@@ -265,7 +301,7 @@ size_t factor_smem_bytes(int block, int smem_slab);
 // `f` may hold the buffers of a released factor; they are reused when large
 // enough.
 cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp32, int epl, bool exact_bwd,
-                            double timeout_s, Scratch& sc, DevFactor& f, cudaStream_t s);
+                            bool bwd_head, double timeout_s, Scratch& sc, DevFactor& f, cudaStream_t s);
 // Drop the last row/column of A (ground vertex) into `out`, whose buffers
 // are reused when large enough (else reallocated).
 cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, Scratch& sc, cudaStream_t s);
@@ -416,5 +452,8 @@ constexpr long long kNoAllocMaxElems = 1LL << 22;
 // kNoAllocMaxElems.
 cudaError_t precond_apply_noalloc(const DevFactor& F, const double* r, double* z, int k, bool fp32, int* status,
                                   double timeout_s, cudaStream_t s);
+// Mean time of one store -> poll hop between two CTAs of the current device
+// (rounds round trips, the first few untimed); the CTAs' SM ids in sm_pair.
+cudaError_t hop_latency(int rounds, double* ns_per_hop, int* sm_pair);
 
 }  // namespace rchol

@@ -46,6 +46,7 @@ struct PcgScalars {
     int phase;               // 0: the next bwd pass initialises rz (start/restart)
     int status;              // device error code
     unsigned ticket[4];
+    double hrz;              // r.z over the backward head's rows
 };
 
 namespace {
@@ -101,6 +102,11 @@ struct SolveArgs {
     int32_t* pcount_b;
     const int32_t* __restrict__ srow_b;
     int32_t nsplit_b;
+    // backward head (see DevFactor::hb_nlev); the persistent backward
+    // kernel starts at task hb_ntask (0: no head)
+    const int4* __restrict__ hb_lv;
+    const int32_t* __restrict__ hb_idx;
+    int32_t hb_nlev, hb_ntask, hb_rows, hb_stage;
     // vectors (n x K row-major)
     const double* __restrict__ b;
     double* x;
@@ -967,9 +973,11 @@ __global__ void __launch_bounds__(kBlock, RCHOL_PACK_MINB) bwd_pack_kernel(Solve
     const unsigned long long t0 = global_timer_ns();
     bool ok = true;
     PackLane<TV> cur, nxt;
-    if (warp < a.ntasks_b) pack_load(cur, a.pack_b[warp], lane, a.order_b, a.pb_idx, pval);
-    int4 dn = warp + nwarps < a.ntasks_b ? a.pack_b[warp + nwarps] : make_int4(0, 0, 0, 0);
-    for (int64_t t = warp; t < a.ntasks_b && ok; t += nwarps) {
+    // the head's tasks were solved by bwd_head_kernel
+    const int64_t tb = a.hb_ntask + warp;
+    if (tb < a.ntasks_b) pack_load(cur, a.pack_b[tb], lane, a.order_b, a.pb_idx, pval);
+    int4 dn = tb + nwarps < a.ntasks_b ? a.pack_b[tb + nwarps] : make_int4(0, 0, 0, 0);
+    for (int64_t t = tb; t < a.ntasks_b && ok; t += nwarps) {
         const int cls = (cur.d.z >> 8) & 7, cnt = cur.d.z & 0xff;
         const int G = 1 << cls;
         const bool lead = (lane >> cls) < cnt && (lane & (G - 1)) == 0;
@@ -1015,6 +1023,7 @@ __global__ void __launch_bounds__(kBlock, RCHOL_PACK_MINB) bwd_pack_kernel(Solve
     if (last_block(&a.sc->ticket[3])) {
         sum_partials<1>(a.part + (size_t)2 * a.grid_max, gridDim.x, a.sc->pq);
         if (threadIdx.x == 0) {
+            if (a.hb_ntask > 0) a.sc->pq[0] += a.sc->hrz;
             if (a.nsplit_b) {  // split rows in id order
                 double extra = a.sc->pq[0];
                 for (int q = 0; q < a.nsplit_b; ++q) {
@@ -1025,6 +1034,176 @@ __global__ void __launch_bounds__(kBlock, RCHOL_PACK_MINB) bwd_pack_kernel(Solve
             }
             bwd_scalars(a, 1);
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Backward head: z for the rows of the first hb_nlev backward levels, solved
+// by one CTA level by level.  These levels are narrow (the vertices
+// eliminated last) and every dependency of a head row is an earlier head
+// row, so the z values live in shared memory and a level costs one CTA
+// barrier instead of a store -> poll hop between SMs.  Each level's task
+// descriptors and slab slots (contiguous ranges) and its rows' y, r and D
+// (gathers) are staged by cp.async kHeadStages - 1 levels ahead.  A lane's
+// products are added in slot order and a row's lanes by the same shuffle
+// tree as bwd_pack_kernel, so z is the persistent kernel's bit for bit;
+// r.z over the head goes to sc->hrz for the backward kernel's reduction.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Byte offsets of one level's stage (head_stage_bytes with the value size of TV).
+struct HeadLevel {
+    int ntask, units, rows, o_idx, o_val, o_y, o_r, o_d;
+};
+
+template <typename TV>
+__device__ __forceinline__ HeadLevel head_level(const int4& lo, const int4& hi) {
+    HeadLevel L;
+    L.ntask = hi.x - lo.x;
+    L.units = hi.y - lo.y;
+    L.rows = hi.z - lo.z;
+    L.o_idx = 16 * L.ntask;
+    L.o_val = L.o_idx + 128 * L.units;
+    L.o_y = L.o_val + 32 * (int)sizeof(TV) * L.units;
+    L.o_r = L.o_y + ((8 * L.rows + 15) & ~15);
+    L.o_d = L.o_r + ((8 * L.rows + 15) & ~15);
+    return L;
+}
+
+// Copies of level l into its stage, spread over threads tid of nthr.
+template <typename TV>
+__device__ __forceinline__ void head_issue(const SolveArgs& a, const int4* lv, const int32_t* rows_s, int l,
+                                           char* buf, int tid, int nthr) {
+    const int4 lo = lv[l], hi = lv[l + 1];
+    const HeadLevel L = head_level<TV>(lo, hi);
+    for (int i = tid; i < L.ntask; i += nthr) cp_async16(buf + 16 * i, a.pack_b + lo.x + i);
+    const char* gi = reinterpret_cast<const char*>(a.hb_idx + (size_t)lo.y * 32);
+    for (int i = tid; i < 8 * L.units; i += nthr) cp_async16(buf + L.o_idx + 16 * i, gi + 16 * i);
+    const char* gv = reinterpret_cast<const char*>(a.pb_val) + (size_t)lo.y * 32 * sizeof(TV);
+    for (int i = tid; i < 2 * (int)sizeof(TV) * L.units; i += nthr) cp_async16(buf + L.o_val + 16 * i, gv + 16 * i);
+    const TV* dv = reinterpret_cast<const TV*>(a.diag);
+    for (int i = tid; i < L.rows; i += nthr) {
+        const int32_t j = rows_s[lo.z + i];
+        cp_async8(buf + L.o_y + 8 * i, a.y + j);
+        if (a.reduce) cp_async8(buf + L.o_r + 8 * i, a.r + j);
+        if (sizeof(TV) == 4) cp_async4(buf + L.o_d + 4 * i, dv + j);
+        else cp_async8(buf + L.o_d + 8 * i, dv + j);
+    }
+}
+
+template <typename TV>
+__global__ void __launch_bounds__(kHeadThreads, 1) bwd_head_kernel(SolveArgs a) {
+    if ((a.reduce || a.seg) && ld_relaxed(&a.sc->done)) return;
+    extern __shared__ __align__(16) char hsm[];
+    const int R = a.hb_rows, nlev = a.hb_nlev;
+    // layout of head_smem_bytes: row ids | z | level table | stages
+    int32_t* rows_s = reinterpret_cast<int32_t*>(hsm);
+    double* zs = reinterpret_cast<double*>(hsm + ((4 * R + 15) & ~15));
+    int4* lv = reinterpret_cast<int4*>(hsm + ((4 * R + 15) & ~15) + ((8 * R + 15) & ~15));
+    char* ring = reinterpret_cast<char*>(lv + nlev + 1);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < R; i += kHeadThreads) rows_s[i] = a.order_b[i];
+    for (int i = tid; i <= nlev; i += kHeadThreads) lv[i] = a.hb_lv[i];
+    __syncthreads();
+    constexpr int NW = kHeadThreads / 32;
+    // levels 0 .. kHeadStages - 2 in flight; one commit group per level
+    for (int l = 0; l < kHeadStages - 1; ++l) {
+        if (l < nlev) head_issue<TV>(a, lv, rows_s, l, ring + (size_t)l * a.hb_stage, tid, kHeadThreads);
+        cp_async_commit();
+    }
+    double acc = 0.0;
+    for (int l = 0; l < nlev; ++l) {
+        // level l's copies have landed (this thread's, then everyone's), and
+        // every warp is done with level l - 1, whose stage is refilled with
+        // level l + kHeadStages - 1 by the warps that hold no task of level l
+        // (all warps when every warp holds one)
+        cp_async_wait<kHeadStages - 2>();
+        __syncthreads();
+        const char* buf = ring + (size_t)(l % kHeadStages) * a.hb_stage;
+        const int4 lo = lv[l];
+        const HeadLevel L = head_level<TV>(lo, lv[l + 1]);
+        {
+            const int lf = l + kHeadStages - 1;
+            const int busy = L.ntask < NW ? L.ntask : 0;
+            if (lf < nlev && warp >= busy)
+                head_issue<TV>(a, lv, rows_s, lf, ring + (size_t)(lf % kHeadStages) * a.hb_stage, tid - 32 * busy,
+                               kHeadThreads - 32 * busy);
+            cp_async_commit();
+        }
+        const int4* desc = reinterpret_cast<const int4*>(buf);
+        const int32_t* idx_s = reinterpret_cast<const int32_t*>(buf + L.o_idx);
+        const TV* val_s = reinterpret_cast<const TV*>(buf + L.o_val);
+        const double* y_s = reinterpret_cast<const double*>(buf + L.o_y);
+        const double* r_s = reinterpret_cast<const double*>(buf + L.o_r);
+        const TV* d_s = reinterpret_cast<const TV*>(buf + L.o_d);
+        for (int ti = warp; ti < L.ntask; ti += NW) {
+            const int4 d = desc[ti];
+            const int cls = (d.z >> 8) & 7, cnt = d.z & 0xff, m = d.w & 0xff;
+            const int G = 1 << cls;
+            const int ub = d.y - lo.y;
+            double sum = 0.0;
+            int k = 0;
+            for (; k + 4 <= m; k += 4) {  // four slots' loads in flight, added in slot order
+                const int sl = (ub + k) * 32 + lane;
+                const int32_t i0 = idx_s[sl], i1 = idx_s[sl + 32], i2 = idx_s[sl + 64], i3 = idx_s[sl + 96];
+                const double w0 = to_d(val_s[sl]), w1 = to_d(val_s[sl + 32]), w2 = to_d(val_s[sl + 64]),
+                             w3 = to_d(val_s[sl + 96]);
+                const double v0 = i0 >= 0 ? zs[i0] : 0.0, v1 = i1 >= 0 ? zs[i1] : 0.0;
+                const double v2 = i2 >= 0 ? zs[i2] : 0.0, v3 = i3 >= 0 ? zs[i3] : 0.0;
+                sum += w0 * v0;
+                sum += w1 * v1;
+                sum += w2 * v2;
+                sum += w3 * v3;
+            }
+            for (; k < m; ++k) {
+                const int sl = (ub + k) * 32 + lane;
+                const int32_t ix = idx_s[sl];
+                const double v = ix >= 0 ? zs[ix] : 0.0;
+                sum += to_d(val_s[sl]) * v;
+            }
+            sum = group_sum(sum, G);
+            const int qrow = lane >> cls;
+            if (qrow < cnt && (lane & (G - 1)) == 0) {
+                const int pos = d.x + qrow;
+                const int rl = pos - lo.z;
+                const double dj = to_d(d_s[rl]);
+                double tj = y_s[rl];
+                if (dj != 0.0) tj = tj / dj;
+                const double zj = tj - sum;
+                zs[pos] = zj;
+                a.z[rows_s[pos]] = zj;
+                if (a.reduce) acc += r_s[rl] * zj;
+            }
+        }
+    }
+    cp_async_wait<0>();
+    if (!a.reduce) return;
+    // r.z over the head: warps in order, lanes by a fixed tree
+    __shared__ double red[kHeadThreads / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+    if (lane == 0) red[warp] = acc;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kHeadThreads / 32; ++w) t += red[w];
+        a.sc->hrz = t;
     }
 }
 
@@ -1116,6 +1295,31 @@ cudaError_t clear_split_counters(const DevFactor& F, cudaStream_t s) {
     return cudaSuccess;
 }
 
+// The solve kernels deal tasks statically (warp w takes tasks w, w + nwarps,
+// ...) and wait on tasks dealt to other warps, so every CTA of the grid must
+// be resident at once.  A cooperative launch guarantees that or fails
+// (cudaErrorCooperativeLaunchTooLarge); it never starts part of the grid
+// while work on another stream holds the SMs that the rest would need.
+cudaError_t launch_coresident(const void* fn, int grid, void** params, cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kBlock);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, fn, params);
+}
+
+template <typename Arg>
+cudaError_t launch_coresident(const void* fn, int grid, Arg& a, cudaStream_t s) {
+    void* params[] = {&a};
+    return launch_coresident(fn, grid, params, s);
+}
+
 int resident_blocks(const void* fn, int device) {
     int per_sm = 0, sms = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0);
@@ -1148,6 +1352,9 @@ class PcgSolver {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
     void *k_init = nullptr, *k_spmv = nullptr, *k_fwd = nullptr, *k_bwd = nullptr, *k_true = nullptr,
          *k_restart = nullptr;
+    void* k_head = nullptr;  // backward head (K = 1)
+
+    bool use_head() const { return k_head && F.hb_nlev > 0; }
 
     SolveArgs args(const double* b, double* x) const {
         SolveArgs a;
@@ -1185,6 +1392,14 @@ class PcgSolver {
         a.pcount_b = F.pcount_b;
         a.srow_b = F.srow_b;
         a.nsplit_b = F.nsplit_b;
+        if (use_head()) {
+            a.hb_lv = F.hb_lv;
+            a.hb_idx = F.hb_idx;
+            a.hb_nlev = F.hb_nlev;
+            a.hb_ntask = F.hb_ntask;
+            a.hb_rows = F.hb_rows;
+            a.hb_stage = F.hb_stage;
+        }
         a.b = b;
         a.x = x;
         a.r = r;
@@ -1209,7 +1424,19 @@ class PcgSolver {
 
     cudaError_t launch(void* fn, int grid, SolveArgs& a) {
         void* params[] = {&a};
+        if (fn == k_fwd || fn == k_bwd) return launch_coresident(fn, grid, params, stream);
         return cudaLaunchKernel(fn, dim3(grid), dim3(kBlock), params, 0, stream);
+    }
+
+    // z = L^-T D^+ y: the backward head (one CTA) first, then the rest
+    cudaError_t launch_bwd(SolveArgs& a) {
+        if (a.hb_nlev > 0) {
+            void* params[] = {&a};
+            const size_t smem = (size_t)head_smem_bytes(a.hb_rows, a.hb_nlev, a.hb_stage);
+            cudaError_t e = cudaLaunchKernel(k_head, dim3(1), dim3(kHeadThreads), params, smem, stream);
+            if (e != cudaSuccess) return e;
+        }
+        return launch(k_bwd, grid_bwd, a);
     }
 
     cudaError_t launch_iteration(const double* b, double* x) {
@@ -1217,7 +1444,7 @@ class PcgSolver {
         cudaError_t e;
         if ((e = launch(k_spmv, grid_spmv, a)) != cudaSuccess) return e;
         if ((e = launch(k_fwd, grid_fwd, a)) != cudaSuccess) return e;
-        return launch(k_bwd, grid_bwd, a);
+        return launch_bwd(a);
     }
 
     // fwd (no update) + bwd with phase 0: z = M r, rz = rz0 = r.z
@@ -1228,7 +1455,7 @@ class PcgSolver {
         cudaError_t e;
         // fwd with reduce=1 but update=0: no x/r change, no rr test
         if ((e = launch(k_fwd, grid_fwd, a)) != cudaSuccess) return e;
-        return launch(k_bwd, grid_bwd, a);
+        return launch_bwd(a);
     }
 };
 
@@ -1240,6 +1467,7 @@ static void bind_kernels(PcgSolver* s) {
     s->k_bwd = K == 1 ? (void*)bwd_pack_kernel<TV> : (void*)bwd_kernel<K, TV>;
     s->k_true = (void*)true_residual_kernel<K>;
     s->k_restart = (void*)restart_kernel<K>;
+    s->k_head = K == 1 ? (void*)bwd_head_kernel<TV> : nullptr;
 }
 
 template <typename TV>
@@ -1290,7 +1518,8 @@ PcgSolver* pcg_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cf
     s->grid_max = std::max(std::max(s->grid_fwd, s->grid_bwd), std::max(s->grid_spmv, s->grid_vec));
     const size_t nv = (size_t)A.n * (size_t)cfg.k;
     cudaError_t e = cudaSuccess;
-    e = cudaMalloc(&s->r, sizeof(double) * std::max<size_t>(nv, 1));
+    if (s->k_head) e = cudaFuncSetAttribute(s->k_head, cudaFuncAttributeMaxDynamicSharedMemorySize, kHeadSmem);
+    if (e == cudaSuccess) e = cudaMalloc(&s->r, sizeof(double) * std::max<size_t>(nv, 1));
     if (e == cudaSuccess) e = cudaMalloc(&s->p, sizeof(double) * std::max<size_t>(nv, 1));
     if (e == cudaSuccess) e = cudaMalloc(&s->q, sizeof(double) * std::max<size_t>(nv, 1));
     if (e == cudaSuccess) e = cudaMalloc(&s->y, sizeof(double) * std::max<size_t>(nv, 1));
@@ -1382,7 +1611,9 @@ cudaError_t pcg_solve(PcgSolver* s, const double* dB, double* dX, SolveResult* r
     SolveArgs a = s->args(dB, dX);
     if ((e = s->launch(s->k_init, s->grid_vec, a)) != cudaSuccess) return e;
     if ((e = s->launch_start(dB, dX)) != cudaSuccess) return e;
-    res->kernel_launches += 3;
+    // per iteration: SpMV, forward, backward (+ the backward head)
+    const int per_it = s->use_head() ? 4 : 3;
+    res->kernel_launches += per_it;
     if ((e = cudaEventRecord(s->ev1, s->stream)) != cudaSuccess) return e;
     int restarts = 0;
     while (true) {
@@ -1391,11 +1622,11 @@ cudaError_t pcg_solve(PcgSolver* s, const double* dB, double* dX, SolveResult* r
             if (s->cfg.use_graph) {
                 if ((e = cudaGraphLaunch(s->graph_exec, s->stream)) != cudaSuccess) return e;
                 res->graph_launches++;
-                res->kernel_launches += 3 * s->cfg.unroll;
+                res->kernel_launches += per_it * s->cfg.unroll;
             } else {
                 for (int u = 0; u < s->cfg.unroll; ++u)
                     if ((e = s->launch_iteration(dB, dX)) != cudaSuccess) return e;
-                res->kernel_launches += 3 * s->cfg.unroll;
+                res->kernel_launches += per_it * s->cfg.unroll;
             }
             if ((e = cudaMemcpyAsync(s->sc_host, s->sc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s->stream)) !=
                 cudaSuccess)
@@ -1442,7 +1673,7 @@ cudaError_t pcg_solve(PcgSolver* s, const double* dB, double* dX, SolveResult* r
             cudaSuccess)
             return e;
         if ((e = s->launch_start(dB, dX)) != cudaSuccess) return e;
-        res->kernel_launches += 4;
+        res->kernel_launches += per_it + 1;
     }
     if ((e = cudaEventRecord(s->ev2, s->stream)) != cudaSuccess) return e;
     if ((e = cudaEventSynchronize(s->ev2)) != cudaSuccess) return e;
@@ -1492,7 +1723,7 @@ cudaError_t pcg_profile(PcgSolver* s, const double* dB, double* dX, int reps, fl
         cudaEventRecord(ev[1], s->stream);
         if (e == cudaSuccess) e = s->launch(s->k_fwd, s->grid_fwd, it);
         cudaEventRecord(ev[2], s->stream);
-        if (e == cudaSuccess) e = s->launch(s->k_bwd, s->grid_bwd, it);
+        if (e == cudaSuccess) e = s->launch_bwd(it);
         cudaEventRecord(ev[3], s->stream);
         cudaEventSynchronize(ev[3]);
         float m;
@@ -1779,6 +2010,11 @@ class BatchSolver {
     }
     SolveArgs solve_args(const double* b, double* x) {
         SolveArgs a = base->args(b, x);
+        // the batched iteration launches no backward head: every task runs
+        // in the persistent kernel
+        a.hb_lv = nullptr;
+        a.hb_idx = nullptr;
+        a.hb_nlev = a.hb_ntask = a.hb_rows = a.hb_stage = 0;
         a.reduce = 0;
         a.update = 1;
         a.seg = seg;
@@ -1787,6 +2023,7 @@ class BatchSolver {
     }
     cudaError_t launch(void* fn, int g, void* arg) {
         void* params[] = {arg};
+        if (fn == base->k_fwd || fn == base->k_bwd) return launch_coresident(fn, g, params, base->stream);
         return cudaLaunchKernel(fn, dim3(g), dim3(kBlock), params, 0, base->stream);
     }
     cudaError_t iteration(const double* b, double* x) {
@@ -2076,18 +2313,11 @@ static cudaError_t precond_apply_t(const DevFactor& F, const double* r, double* 
     a.timeout_ns = (unsigned long long)(timeout_s * 1e9);
     const int64_t total = (int64_t)F.n * K;
     fill_pending_kernel<<<grid_for(total, kBlock, 8), kBlock, 0, s>>>(y, total);
-    if (K == 1) {
-        int gf = resident_blocks((void*)fwd_pack_kernel<TV>, device);
-        int gb = resident_blocks((void*)bwd_pack_kernel<TV>, device);
-        fwd_pack_kernel<TV><<<gf, kBlock, 0, s>>>(a);
-        bwd_pack_kernel<TV><<<gb, kBlock, 0, s>>>(a);
-    } else {
-        int gf = resident_blocks((void*)fwd_kernel<K, TV>, device);
-        int gb = resident_blocks((void*)bwd_kernel<K, TV>, device);
-        fwd_kernel<K, TV><<<gf, kBlock, 0, s>>>(a);
-        bwd_kernel<K, TV><<<gb, kBlock, 0, s>>>(a);
-    }
     e = cudaGetLastError();
+    const void* kf = K == 1 ? (const void*)fwd_pack_kernel<TV> : (const void*)fwd_kernel<K, TV>;
+    const void* kb = K == 1 ? (const void*)bwd_pack_kernel<TV> : (const void*)bwd_kernel<K, TV>;
+    if (e == cudaSuccess) e = launch_coresident(kf, resident_blocks(kf, device), a, s);
+    if (e == cudaSuccess) e = launch_coresident(kb, resident_blocks(kb, device), a, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(status, &sc->status, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFree(sc);
@@ -2191,14 +2421,11 @@ cudaError_t precond_apply_noalloc_t(const DevFactor& F, const double* r, double*
     a.reduce = 0;
     a.timeout_ns = (unsigned long long)(timeout_s * 1e9);
     fill_pending_kernel<<<grid_for((int64_t)F.n * K, kBlock, 8), kBlock, 0, s>>>(y, (int64_t)F.n * K);
-    if (K == 1) {
-        fwd_pack_kernel<TV><<<resident_blocks((void*)fwd_pack_kernel<TV>, device), kBlock, 0, s>>>(a);
-        bwd_pack_kernel<TV><<<resident_blocks((void*)bwd_pack_kernel<TV>, device), kBlock, 0, s>>>(a);
-    } else {
-        fwd_kernel<K, TV><<<resident_blocks((void*)fwd_kernel<K, TV>, device), kBlock, 0, s>>>(a);
-        bwd_kernel<K, TV><<<resident_blocks((void*)bwd_kernel<K, TV>, device), kBlock, 0, s>>>(a);
-    }
     e = cudaGetLastError();
+    const void* kf = K == 1 ? (const void*)fwd_pack_kernel<TV> : (const void*)fwd_kernel<K, TV>;
+    const void* kb = K == 1 ? (const void*)bwd_pack_kernel<TV> : (const void*)bwd_kernel<K, TV>;
+    if (e == cudaSuccess) e = launch_coresident(kf, resident_blocks(kf, device), a, s);
+    if (e == cudaSuccess) e = launch_coresident(kb, resident_blocks(kb, device), a, s);
     int st = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&st, &sc->status, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -2232,6 +2459,68 @@ cudaError_t precond_apply_noalloc(const DevFactor& F, const double* r, double* z
             return cudaErrorInvalidValue;
     }
 #undef RCHOL_PAN
+}
+
+
+// ---------------------------------------------------------------------------
+// The hop floor of the sync-free solves: two CTAs pass a counter back and
+// forth through one global word with the solves' own relaxed store and poll
+// (no back-off), so one hop is a store on one SM seen by a poll on another.
+// The first kHopWarm round trips are not timed (launch skew).  Every wait is
+// bounded by limit_ns; on expiry out[1] = 1 and the CTA returns.
+// out: [0] ns for 2 * (rounds - kHopWarm) hops, [1] error, [2..3] SM ids.
+// ---------------------------------------------------------------------------
+constexpr int kHopWarm = 16;
+
+__global__ void hop_probe_kernel(double* cell, int rounds, unsigned long long limit_ns, long long* out) {
+    if (threadIdx.x != 0) return;
+    const int me = blockIdx.x;
+    unsigned smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    out[2 + me] = smid;
+    const unsigned long long t0 = global_timer_ns();
+    unsigned long long ts = t0;
+    for (int i = 0; i <= rounds; ++i) {
+        if (me == 1 && i == rounds) break;
+        const double want = (double)(2 * i + me);
+        unsigned spins = 0;
+        while (ld_relaxed_f64(cell) != want) {
+            if ((++spins & 63u) == 0 && global_timer_ns() - t0 > limit_ns) {
+                out[1] = 1;
+                return;
+            }
+        }
+        if (me == 0 && i == kHopWarm) ts = global_timer_ns();
+        if (i < rounds) st_relaxed_f64(cell, want + 1.0);
+    }
+    if (me == 0) out[0] = (long long)(global_timer_ns() - ts);
+}
+
+cudaError_t hop_latency(int rounds, double* ns_per_hop, int* sm_pair) {
+    if (rounds <= kHopWarm) return cudaErrorInvalidValue;
+    char* buf = nullptr;
+    cudaError_t e = cudaMalloc((void**)&buf, 256);
+    if (e != cudaSuccess) return e;
+    double* cell = reinterpret_cast<double*>(buf);
+    long long* out = reinterpret_cast<long long*>(buf + 128);
+    long long h[4] = {0, 0, 0, 0};
+    e = cudaMemset(buf, 0, 256);
+    if (e == cudaSuccess) {
+        unsigned long long limit = 2000000000ull;  // 2 s
+        void* params[] = {&cell, &rounds, &limit, &out};
+        // cooperative: both CTAs are resident together or the launch fails
+        e = cudaLaunchCooperativeKernel((const void*)hop_probe_kernel, dim3(2), dim3(32), params, 0, 0);
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(h, out, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(buf);
+    if (e != cudaSuccess) return e;
+    if (h[1] != 0) return cudaErrorTimeout;
+    *ns_per_hop = (double)h[0] / (2.0 * (rounds - kHopWarm));
+    if (sm_pair) {
+        sm_pair[0] = (int)h[2];
+        sm_pair[1] = (int)h[3];
+    }
+    return cudaSuccess;
 }
 
 }  // namespace rchol

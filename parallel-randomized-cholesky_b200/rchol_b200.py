@@ -36,6 +36,7 @@ EXPORTS = sorted([
     "rchol_prepare_and_solve", "rchol_generate", "rchol_free_host", "rchol_write_mtx", "rchol_batch_set",
     "rchol_batch_solve", "rchol_zero_sum_vector", "rchol_set_sddm", "rchol_write_bin", "rchol_read_bin",
     "rchol_save_bin", "rchol_load_bin", "rchol_autotune", "rchol_ordering",
+    "rchol_hop_latency",
 ])
 
 
@@ -52,7 +53,7 @@ class Opts(C.Structure):
                 ("unroll", C.c_int), ("use_graph", C.c_int), ("device", C.c_int), ("timeout_s", C.c_double),
                 ("verbose", C.c_int), ("poll_ns", C.c_int),
                 ("sched_epl", C.c_int), ("exact_bwd_levels", C.c_int), ("spmv_layout", C.c_int),
-                ("tail_vertices", C.c_int), ("rhs_block", C.c_int)]
+                ("tail_vertices", C.c_int), ("rhs_block", C.c_int), ("bwd_head", C.c_int)]
 
 
 class FactorInfo(C.Structure):
@@ -64,7 +65,8 @@ class FactorInfo(C.Structure):
                 ("solve_depth", C.c_int), ("kernel_launches", C.c_int),
                 ("lc_ptr", C.c_void_p), ("lc_idx", C.c_void_p), ("lc_val", C.c_void_p),
                 ("lr_ptr", C.c_void_p), ("lr_idx", C.c_void_p), ("lr_val", C.c_void_p), ("diag", C.c_void_p),
-                ("tail_vertices", C.c_int)]
+                ("tail_vertices", C.c_int), ("solve_depth_b", C.c_int), ("bwd_head_levels", C.c_int),
+                ("bwd_head_rows", C.c_int)]
 
 
 class TuneResult(C.Structure):
@@ -132,6 +134,7 @@ def lib():
         L.rchol_precond_apply_noalloc.argtypes = [vp, C.c_int, vp, vp, C.c_int, vp]
         L.rchol_spmv.argtypes = [vp, C.c_int, vp, vp, C.c_int, C.c_int]
         L.rchol_profile_solve.argtypes = [vp, vp, C.c_int, C.c_int, C.POINTER(C.c_float)]
+        L.rchol_hop_latency.argtypes = [vp, C.c_int, C.POINTER(C.c_double), i32p]
         L.rchol_factorization_driver.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_int]
         L.rchol_prepare_and_solve.argtypes = [C.c_int, C.c_longlong, vp, vp, vp, vp, vp, vp, vp, C.c_double,
                                               C.c_int, C.c_longlong, C.c_int, vp, C.POINTER(SolveInfo)]
@@ -521,6 +524,14 @@ class Context:
         ms = (C.c_float * 3)()
         _check(lib().rchol_profile_solve(self.h, factor.h, k, reps, ms), self.h)
         return list(ms)
+
+    def hop_latency(self, rounds=4096):
+        """(ns per store -> poll hop between two SMs, (sm_a, sm_b)): the latency
+        floor per level of the sync-free triangular solves."""
+        ns = C.c_double()
+        sm = (C.c_int * 2)()
+        _check(lib().rchol_hop_latency(self.h, rounds, C.byref(ns), sm), self.h)
+        return ns.value, (sm[0], sm[1])
 
     def spmv(self, X):
         X = np.asarray(X, np.float64)

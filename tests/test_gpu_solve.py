@@ -364,3 +364,55 @@ def test_solver_kept_across_factors():
         f.free()
         c_.close()
     np.testing.assert_array_equal(xs[0], xs[1])
+
+
+def test_hop_latency_floor():
+    """The store -> poll hop between two SMs that bounds the sync-free
+    solves from below: a finite positive time of the order of an L2 round
+    trip, and a solve of depth d takes at least d of them."""
+    ctx = R.Context()
+    try:
+        ns, sms = ctx.hop_latency(2048)
+        assert 20.0 < ns < 20000.0
+        assert all(s >= 0 for s in sms)
+        with pytest.raises(R.RcholError):
+            ctx.hop_latency(8)
+        n, r, c, v, g = grid_laplacian((24, 24, 24), seed=3, excess_frac=0.05)
+        ctx.set_triplets(n, r, c, v, trim_ground=g)
+        f = ctx.factor()
+        fi = f.info()
+        assert fi.solve_depth > 1 and fi.solve_depth_b > 1
+        ms = ctx.profile_solve(f, 1, reps=3)
+        assert ms[1] * 1e6 >= fi.solve_depth * ns * 0.5
+        assert ms[2] * 1e6 >= fi.solve_depth_b * ns * 0.5
+        f.free()
+    finally:
+        ctx.close()
+
+
+@pytest.mark.parametrize("precision", [R.PREC_FP64, R.PREC_FP32_FACTOR])
+def test_backward_head_matches_persistent_kernel(precision):
+    """The first backward levels solved by the one-CTA head kernel: the
+    factor of a 3-D grid gets a head, and PCG with it reaches the same
+    iterate as with the head switched off (same z bit for bit; only the
+    grouping of the r.z sum differs) and the oracle's iteration count."""
+    n, r, c, v, g = grid_laplacian((20, 22, 24), seed=45, excess_frac=0.05, wlo=1e-2, whi=1e2)
+    out = {}
+    for head in (1, 0):
+        ctx = R.Context(seed=4, precision=precision, tol=1e-8, bwd_head=head)
+        ctx.set_triplets(n, r, c, v, trim_ground=g)
+        f = ctx.factor()
+        fi = f.info()
+        b = zero_sum_normal(fi.n, 11)
+        x, info = ctx.pcg_solve(f, b)
+        ctx.set_opts(max_iter=2)
+        x2, _ = ctx.pcg_solve(f, b)
+        out[head] = (fi.bwd_head_levels, fi.bwd_head_rows, x, info, x2)
+        f.free()
+        ctx.close()
+    (hl, hr, xh, ih, x2h), (nl, nr, xn, inn, x2n) = out[1], out[0]
+    assert hl >= 8 and hr > 0 and nl == 0 and nr == 0
+    assert ih["converged"] and inn["converged"]
+    assert abs(ih["iterations"] - inn["iterations"]) <= 1
+    np.testing.assert_allclose(x2h, x2n, rtol=0, atol=1e-12 * np.abs(x2n).max())
+    assert np.linalg.norm(xh - xn) <= 1e-7 * np.linalg.norm(xn)
