@@ -23,13 +23,20 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.skipif(not os.path.exists(O.REF_BIN), reason="reference CPU factor not built (oracle/_ref)")
-@pytest.mark.parametrize("config", ["grid2d_256_unit", "grid3d_32_sddm",
+@pytest.mark.parametrize("config", ["grid2d_256_unit", "grid3d_32_sddm", "chunglu_200k", "grid27_48_sddm",
                                     pytest.param("grid3d_128_sddm", marks=pytest.mark.slow)])
 def test_statistical_parity_with_reference(config):
     """grid3d_128_sddm is the benchmark's headline input itself (128^3 SDDM,
-    2,097,152 unknowns); it takes a few minutes of host time."""
+    2,097,152 unknowns); it takes a few minutes of host time.  chunglu_200k
+    and grid27_48_sddm are the power-law and anisotropic 27-point families
+    of the secondary benchmarks at a size the host finishes in seconds."""
     if config == "grid2d_256_unit":
         n, r, c, v, g = R.generate("grid2d", [256, 256], seed=0)
+    elif config == "chunglu_200k":
+        n, r, c, v, g = R.generate("chunglu", [200_000, 2_000_000, 2, 20_000], wlo=1.0, whi=10.0, seed=3)
+    elif config == "grid27_48_sddm":
+        n, r, c, v, g = R.generate("grid3d27", [48, 48, 48], wlo=0.1, whi=10.0, log_weights=True, aniso_z=100.0,
+                                   excess_frac=1.0, excess_lo=1e-4, excess_hi=1e-4, seed=5)
     else:
         side = 128 if config == "grid3d_128_sddm" else 32
         n, r, c, v, g = R.generate("grid3d", [side] * 3, wlo=1e-3, whi=1e3, log_weights=True, excess_frac=0.05,
