@@ -55,7 +55,8 @@ typedef struct rchol_opts {
                                  factor; 0 = the whole resident grid */
     int warps_per_block;      /* factor CTA size in warps (1..8) */
     int slab_entries;         /* per-warp shared-memory slab (power of two) */
-    int bucket_cap;           /* first fill chunk per column */
+    int bucket_cap;           /* first fill chunk per column (default 64; larger buckets
+                                 spare the overflow-chunk walks of big gathers) */
     double pool_mult;         /* factor pool capacity / nnz(strict lower A) */
     int max_iter;             /* PCG iteration cap */
     double tol;               /* PCG tolerance (meaning set by stop_rule) */
@@ -270,10 +271,12 @@ rchol_status rchol_precond_apply_noalloc(const rchol_factor_t* f, int k, const d
  *                  longest suffix in which 3/4 of the vertices gather >= 1024
  *                  entries), kept only when a timed factorization is faster;
  *   bucket_cap     the power of two covering 95% of the vertices' gathers,
- *                  kept only when faster;
+ *                  then twice and four times that (at most 128, and only
+ *                  while the buckets take at most a quarter of the free
+ *                  device memory), each kept only when faster;
  *   rhs_block      the block width (<= max_rhs) of least iteration time per
  *                  right-hand side.
- * One profiling factorization plus at most three timed trials; the choices
+ * One profiling factorization plus at most five timed trials; the choices
  * are written into the context's options and cached per process for the
  * same matrix fingerprint (n, nnz, trim, column-length histogram), GPU,
  * precision and max_rhs (from_cache = 1 on a hit). */

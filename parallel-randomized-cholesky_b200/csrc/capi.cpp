@@ -254,7 +254,7 @@ extern "C" rchol_status rchol_opts_default(rchol_opts* o) {
     o->num_blocks = 0;
     o->warps_per_block = 8;
     o->slab_entries = 256;
-    o->bucket_cap = 32;
+    o->bucket_cap = 64;
     o->pool_mult = 6.0;
     o->max_iter = 1000;
     o->tol = 1e-6;
@@ -1326,15 +1326,22 @@ extern "C" rchol_status rchol_autotune(rchol_ctx* ctx, int max_rhs, rchol_tune_r
         if (ms < best) best = ms;
         else o.tail_vertices = 0;
     }
-    // 3. bucket capacity: the power of two covering 95% of the gathers
+    // 3. bucket capacity: the power of two covering 95% of the gathers,
+    // then twice and four times that (fewer overflow-chunk walks for the
+    // big gathers), while the buckets fit a quarter of the free memory
     std::vector<int32_t> sorted(g);
     std::sort(sorted.begin(), sorted.end());
     const int32_t p95 = sorted.empty() ? 0 : sorted[(size_t)((sorted.size() - 1) * 95 / 100)];
     int cap = 8;
     while (cap < p95 && cap < 64) cap <<= 1;
-    if (cap != o.bucket_cap) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+    for (int c = cap; c <= std::min(4 * cap, 128); c <<= 1) {
+        if (c == o.bucket_cap) continue;
+        const double bytes = (double)n * (double)(c - o.bucket_cap) * 12.0;
+        if (bytes > 0.25 * (double)free_b) break;
         rchol_opts t = o;
-        t.bucket_cap = cap;
+        t.bucket_cap = c;
         const float ms = timed_factor(ctx, t, &st);
         if (st != RCHOL_OK) return st;
         if (ms < best) {

@@ -286,7 +286,7 @@ def test_autotune_choices_are_used_and_cached():
         ctx.set_triplets(n, r, c, v, trim_ground=g)
         t1 = ctx.autotune(max_rhs=32)
         assert not t1["from_cache"] and t1["max_gather"] > 32
-        assert t1["rhs_block"] in (1, 2, 4, 8, 16, 32) and t1["bucket_cap"] in (8, 16, 32, 64)
+        assert t1["rhs_block"] in (1, 2, 4, 8, 16, 32) and t1["bucket_cap"] in (8, 16, 32, 64, 128)
         assert t1["ms_factor_tuned"] <= t1["ms_factor_default"]
         assert all(x > 0 for x in t1["per_rhs_ms"])
         assert ctx.opts.tail_vertices == t1["tail_vertices"] and ctx.opts.rhs_block == t1["rhs_block"]
