@@ -297,13 +297,20 @@ __global__ void mask_mul_kernel(const int32_t* __restrict__ a, const int32_t* __
 
 // Parts of each scheduled task: 1, or ceil(len / kSplitLen) for a one-row
 // task of the widest class whose row is longer than kSplitMin.
-__global__ void pack_nsub_kernel(const int2* __restrict__ tasks, int32_t ntasks, const int64_t* __restrict__ optr,
-                                 int32_t* nsub, int32_t* issplit) {
+// Entries of the row at schedule position p: ptr[order[p]] .. ptr[order[p] + 1].
+__device__ __forceinline__ int64_t pos_len(const int32_t* __restrict__ order, const int64_t* __restrict__ ptr,
+                                           int64_t p) {
+    const int32_t i = order[p];
+    return ptr[i + 1] - ptr[i];
+}
+
+__global__ void pack_nsub_kernel(const int2* __restrict__ tasks, int32_t ntasks, const int32_t* __restrict__ order,
+                                 const int64_t* __restrict__ ptr, int32_t* nsub, int32_t* issplit) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntasks; t += stride) {
         const int2 d = tasks[t];
         const int cls = d.y >> 8, cnt = d.y & 0xff;
-        const int64_t len = cnt == 1 ? optr[d.x + 1] - optr[d.x] : 0;
+        const int64_t len = cnt == 1 ? pos_len(order, ptr, d.x) : 0;
         const int np = (cls == kLaneClasses - 1 && len > kSplitMin) ? (int)((len + kSplitLen - 1) / kSplitLen) : 1;
         nsub[t] = np;
         issplit[t] = np > 1 ? 1 : 0;
@@ -312,7 +319,7 @@ __global__ void pack_nsub_kernel(const int2* __restrict__ tasks, int32_t ntasks,
 
 // Expanded tasks {position, d.z bits, part count, part length or 0} and the
 // split bookkeeping of part tasks.
-__global__ void pack_expand_kernel(const int2* __restrict__ tasks, int32_t ntasks, const int64_t* __restrict__ optr,
+__global__ void pack_expand_kernel(const int2* __restrict__ tasks, int32_t ntasks, const int64_t* __restrict__ ptr,
                                    const int32_t* __restrict__ order, const int32_t* __restrict__ nsub,
                                    const int32_t* __restrict__ tbase, const int32_t* __restrict__ sid,
                                    const int32_t* __restrict__ pbase, int4* etask, int2* split, int32_t* srow) {
@@ -324,7 +331,7 @@ __global__ void pack_expand_kernel(const int2* __restrict__ tasks, int32_t ntask
             etask[tbase[t]] = make_int4(d.x, d.y, 1, 0);
             continue;
         }
-        const int64_t len = optr[d.x + 1] - optr[d.x];
+        const int64_t len = pos_len(order, ptr, d.x);
         srow[sid[t]] = order[d.x];
         for (int q = 0; q < np; ++q) {
             const int plen = (int)min((int64_t)kSplitLen, len - (int64_t)q * kSplitLen);
@@ -336,15 +343,15 @@ __global__ void pack_expand_kernel(const int2* __restrict__ tasks, int32_t ntask
 
 // slots per lane of each expanded task: the longest of its rows (or the
 // part's length) over G lanes
-__global__ void pack_m_kernel(const int4* __restrict__ etask, int32_t ntasks, const int64_t* __restrict__ optr,
-                              int32_t* m) {
+__global__ void pack_m_kernel(const int4* __restrict__ etask, int32_t ntasks, const int32_t* __restrict__ order,
+                              const int64_t* __restrict__ ptr, int32_t* m) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntasks; t += stride) {
         const int4 e = etask[t];
         const int cls = (e.y >> 8) & 7, cnt = e.y & 0xff;
         int64_t longest = e.w;
         if (!((e.y >> 11) & 1))
-            for (int r = 0; r < cnt; ++r) longest = max(longest, optr[e.x + r + 1] - optr[e.x + r]);
+            for (int r = 0; r < cnt; ++r) longest = max(longest, pos_len(order, ptr, e.x + r));
         m[t] = (int32_t)((longest + (1 << cls) - 1) >> cls);
     }
 }
@@ -362,8 +369,9 @@ __global__ void pack_desc_kernel(const int4* __restrict__ etask, int32_t ntasks,
 // except that entry 0 and the row's gate trade places.  The gate is the
 // dependency scheduled last (largest sign * level; the first such entry on
 // ties): the solve polls it alone before reading the rest of the row.
-__global__ void pack_fill_kernel(const int4* __restrict__ pack, int32_t ntasks, const int64_t* __restrict__ optr,
-                                 const int32_t* __restrict__ sidx, const double* __restrict__ sval,
+__global__ void pack_fill_kernel(const int4* __restrict__ pack, int32_t ntasks, const int32_t* __restrict__ order,
+                                 const int64_t* __restrict__ ptr, const int32_t* __restrict__ sidx,
+                                 const double* __restrict__ sval,
                                  const float* __restrict__ sval32, const int32_t* __restrict__ level, int sign,
                                  int32_t* pidx, double* pval, float* pval32) {
     const int lane = threadIdx.x & 31;
@@ -375,8 +383,9 @@ __global__ void pack_fill_kernel(const int4* __restrict__ pack, int32_t ntasks, 
         const int r = lane >> cls, gl = lane & (G - 1);
         int64_t s = 0, len = 0;
         if (r < cnt) {
-            s = optr[d.x + r];
-            len = optr[d.x + r + 1] - s;
+            const int32_t i = order[d.x + r];
+            s = ptr[i];
+            len = ptr[i + 1] - s;
             if ((d.z >> 11) & 1) {  // part task: its window of the row
                 const int64_t q0 = (int64_t)(d.z >> 12) * kSplitLen;
                 s += q0;
@@ -782,9 +791,10 @@ struct PackOut {
     int64_t* cap_r;
 };
 
-// Task slabs of one direction from its task list and schedule-ordered
-// layout; rows longer than kSplitMin are split into part tasks first.
-static cudaError_t build_pack(int32_t ntasks, const int2* tasks, const int32_t* order, const int64_t* optr,
+// Task slabs of one direction from its task list and row order over L's
+// rows (ptr, sidx, sval by row id); rows longer than kSplitMin are split
+// into part tasks first.
+static cudaError_t build_pack(int32_t ntasks, const int2* tasks, const int32_t* order, const int64_t* ptr,
                               const int32_t* sidx, const double* sval, const float* sval32, const int32_t* level,
                               int sign, const PackOut& o, Scratch& sc, cudaStream_t s) {
     const int64_t nt = std::max<int32_t>(ntasks, 1);
@@ -803,7 +813,7 @@ static cudaError_t build_pack(int32_t ntasks, const int2* tasks, const int32_t* 
         RCHOL_TRY(ensure(o.pack, *o.cap_d, 1));
         return cudaSuccess;
     }
-    pack_nsub_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(tasks, ntasks, optr, nsub, issplit);
+    pack_nsub_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(tasks, ntasks, order, ptr, nsub, issplit);
     RCHOL_TRY(exclusive_scan_i32_to_i32(nsub, tbase, ntasks, tmp, s));
     RCHOL_TRY(exclusive_scan_i32_to_i32(issplit, sid, ntasks, tmp, s));
     int32_t hs[2] = {0, 0};
@@ -835,9 +845,9 @@ static cudaError_t build_pack(int32_t ntasks, const int2* tasks, const int32_t* 
     RCHOL_TRY(ensure(o.pcount, *o.cap_c, std::max<int64_t>(nsp, 1)));
     RCHOL_TRY(ensure(o.srow, *o.cap_r, std::max<int64_t>(nsp, 1)));
     RCHOL_TRY(cudaMemsetAsync(*o.pcount, 0, sizeof(int32_t) * (size_t)std::max<int32_t>(nsp, 1), s));
-    pack_expand_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(tasks, ntasks, optr, order, nsub, tbase, sid, pbase, etask,
+    pack_expand_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(tasks, ntasks, ptr, order, nsub, tbase, sid, pbase, etask,
                                                              *o.split, *o.srow);
-    pack_m_kernel<<<grid_for(ne, 256), 256, 0, s>>>(etask, ne, optr, m);
+    pack_m_kernel<<<grid_for(ne, 256), 256, 0, s>>>(etask, ne, order, ptr, m);
     RCHOL_TRY(exclusive_scan_i32_to_i64(m, base, ne, tmp2, s));
     int64_t units = 0;
     RCHOL_TRY(cudaMemcpyAsync(&units, base + ne, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
@@ -858,48 +868,24 @@ static cudaError_t build_pack(int32_t ntasks, const int2* tasks, const int32_t* 
     }
     pack_desc_kernel<<<grid_for(ne, 256), 256, 0, s>>>(etask, ne, m, base, *o.pack);
     pack_fill_kernel<<<grid_for((int64_t)ne * 32, 256), 256, 0, s>>>(
-        *o.pack, ne, optr, sidx, sval, sval32, level, sign, *o.pidx, *o.pval, sval32 ? *o.pval32 : nullptr);
+        *o.pack, ne, order, ptr, sidx, sval, sval32, level, sign, *o.pidx, *o.pval, sval32 ? *o.pval32 : nullptr);
     return cudaGetLastError();
 }
 
-// The solve layouts (schedule-ordered copies of Lr and Lc) for the orders
-// already built; FP32 values are copied when the factor has them.
-static cudaError_t build_layouts(DevFactor& f, const int32_t* level_f, const int32_t* level_b, int sign_b,
+// The task slabs of both directions for the orders already built, read
+// from the rows of Lr (forward) and Lc (backward); FP32 values are copied
+// when the factor has them.
+static cudaError_t build_packs(DevFactor& f, const int32_t* level_f, const int32_t* level_b, int sign_b,
                                  Scratch& sc, cudaStream_t s) {
-    const bool grow_n = f.cap_ln < (int64_t)f.n + 1;
-    const int64_t capn = std::max<int64_t>(f.cap_ln, (int64_t)f.n + 1);
-    RCHOL_TRY(realloc_if(&f.sf_ptr, grow_n, capn));
-    RCHOL_TRY(realloc_if(&f.sb_ptr, grow_n, capn));
-    f.cap_ln = capn;
-    const bool fp32 = f.lr_val32 != nullptr;
-    const bool grow_z = f.cap_lz < f.nnz || (fp32 && !f.sf_val32);
-    const int64_t capz = std::max<int64_t>(f.cap_lz, f.nnz);
-    RCHOL_TRY(realloc_if(&f.sf_idx, grow_z, capz));
-    RCHOL_TRY(realloc_if(&f.sf_val, grow_z, capz));
-    RCHOL_TRY(realloc_if(&f.sb_idx, grow_z, capz));
-    RCHOL_TRY(realloc_if(&f.sb_val, grow_z, capz));
-    if (fp32) {
-        RCHOL_TRY(realloc_if(&f.sf_val32, grow_z, capz));
-        RCHOL_TRY(realloc_if(&f.sb_val32, grow_z, capz));
-    } else {
-        cudaFree(f.sf_val32);
-        cudaFree(f.sb_val32);
-        f.sf_val32 = f.sb_val32 = nullptr;
-    }
-    f.cap_lz = capz;
-    RCHOL_TRY(build_layout(f.n, f.order_f, f.lr_ptr, f.lr_idx, f.lr_val, f.lr_val32, f.sf_ptr, f.sf_idx, f.sf_val,
-                           f.sf_val32, sc, s));
-    RCHOL_TRY(build_layout(f.n, f.order_b, f.lc_ptr, f.lc_idx, f.lc_val, f.lc_val32, f.sb_ptr, f.sb_idx, f.sb_val,
-                           f.sb_val32, sc, s));
     const PackOut of{&f.pack_f, &f.cap_pdf, &f.pf_idx, &f.cap_pif, &f.pf_val, &f.cap_pvf, &f.pf_val32, &f.cap_pwf,
                      &f.slots_f, &f.npt_f, &f.nsplit_f, &f.split_f, &f.cap_sf, &f.psum_f, &f.cap_qf, &f.pcount_f,
                      &f.cap_cf, &f.srow_f, &f.cap_rf};
     const PackOut ob{&f.pack_b, &f.cap_pdb, &f.pb_idx, &f.cap_pib, &f.pb_val, &f.cap_pvb, &f.pb_val32, &f.cap_pwb,
                      &f.slots_b, &f.npt_b, &f.nsplit_b, &f.split_b, &f.cap_sb, &f.psum_b, &f.cap_qb, &f.pcount_b,
                      &f.cap_cb, &f.srow_b, &f.cap_rb};
-    RCHOL_TRY(build_pack(f.ntasks_f, f.tasks_f, f.order_f, f.sf_ptr, f.sf_idx, f.sf_val, f.sf_val32, level_f, 1, of,
+    RCHOL_TRY(build_pack(f.ntasks_f, f.tasks_f, f.order_f, f.lr_ptr, f.lr_idx, f.lr_val, f.lr_val32, level_f, 1, of,
                          sc, s));
-    RCHOL_TRY(build_pack(f.ntasks_b, f.tasks_b, f.order_b, f.sb_ptr, f.sb_idx, f.sb_val, f.sb_val32, level_b, sign_b,
+    RCHOL_TRY(build_pack(f.ntasks_b, f.tasks_b, f.order_b, f.lc_ptr, f.lc_idx, f.lc_val, f.lc_val32, level_b, sign_b,
                          ob, sc, s));
     return cudaSuccess;
 }
@@ -957,10 +943,45 @@ static cudaError_t build_bwd_head(DevFactor& f, const int32_t* levb, Scratch& sc
     return cudaSuccess;
 }
 
+cudaError_t build_solve_layouts(DevFactor& f, Scratch& sc, cudaStream_t s) {
+    if (f.lay_ready) return cudaSuccess;
+    const bool grow_n = f.cap_ln < (int64_t)f.n + 1;
+    const int64_t capn = std::max<int64_t>(f.cap_ln, (int64_t)f.n + 1);
+    RCHOL_TRY(realloc_if(&f.sf_ptr, grow_n, capn));
+    RCHOL_TRY(realloc_if(&f.sb_ptr, grow_n, capn));
+    f.cap_ln = capn;
+    const bool fp32 = f.lr_val32 != nullptr;
+    const bool grow_z = f.cap_lz < f.nnz || (fp32 && !f.sf_val32);
+    const int64_t capz = std::max<int64_t>(f.cap_lz, f.nnz);
+    RCHOL_TRY(realloc_if(&f.sf_idx, grow_z, capz));
+    RCHOL_TRY(realloc_if(&f.sf_val, grow_z, capz));
+    RCHOL_TRY(realloc_if(&f.sb_idx, grow_z, capz));
+    RCHOL_TRY(realloc_if(&f.sb_val, grow_z, capz));
+    if (fp32) {
+        RCHOL_TRY(realloc_if(&f.sf_val32, grow_z, capz));
+        RCHOL_TRY(realloc_if(&f.sb_val32, grow_z, capz));
+    } else {
+        cudaFree(f.sf_val32);
+        cudaFree(f.sb_val32);
+        f.sf_val32 = f.sb_val32 = nullptr;
+    }
+    f.cap_lz = capz;
+    sc.reset();
+    RCHOL_TRY(build_layout(f.n, f.order_f, f.lr_ptr, f.lr_idx, f.lr_val, f.lr_val32, f.sf_ptr, f.sf_idx, f.sf_val,
+                           f.sf_val32, sc, s));
+    RCHOL_TRY(build_layout(f.n, f.order_b, f.lc_ptr, f.lc_idx, f.lc_val, f.lc_val32, f.sb_ptr, f.sb_idx, f.sb_val,
+                           f.sb_val32, sc, s));
+    RCHOL_TRY(cudaStreamSynchronize(s));
+    sc.reset();
+    f.lay_ready = true;
+    return cudaSuccess;
+}
+
 cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bool exact_bwd, bool bwd_head,
                                  double timeout_s, Scratch& sc, cudaStream_t s) {
     if (epl < 1) epl = 1;
     f.hb_nlev = f.hb_ntask = f.hb_rows = f.hb_stage = 0;
+    f.lay_ready = false;
     {
         const bool grow_n = f.cap_n < (int64_t)f.n + 1;
         const int64_t capn = std::max<int64_t>(f.cap_n, (int64_t)f.n + 1);
@@ -977,7 +998,7 @@ cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bo
         RCHOL_TRY(build_one_schedule(level, f.lc_ptr, f.n, f.depth, 1, epl, sc, f.order_b, &f.tasks_b, f.cap_tb,
                                      &f.ntasks_b, s));
         // reversed forward levels: the backward gate is the dependency of least forward level
-        RCHOL_TRY(build_layouts(f, level, level, -1, sc, s));
+        RCHOL_TRY(build_packs(f, level, level, -1, sc, s));
         return cudaStreamSynchronize(s);
     }
     // true backward levels, visited in the reversed forward order
@@ -1001,7 +1022,7 @@ cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bo
     f.depth_b = hs[1] + 1;
     RCHOL_TRY(build_one_schedule(levb, f.lc_ptr, f.n, f.depth_b, 0, epl, sc, f.order_b, &f.tasks_b, f.cap_tb,
                                  &f.ntasks_b, s));
-    RCHOL_TRY(build_layouts(f, level, levb, 1, sc, s));
+    RCHOL_TRY(build_packs(f, level, levb, 1, sc, s));
     if (bwd_head) RCHOL_TRY(build_bwd_head(f, levb, sc, s));
     return cudaStreamSynchronize(s);
 }

@@ -108,10 +108,10 @@ void free_work(FactorWork& w) {
 void free_factor(DevFactor& f) {
     void* ps[] = {f.lc_ptr, f.lc_idx,  f.lc_val,  f.lc_val32, f.lr_ptr,  f.lr_idx, f.lr_val,
                   f.lr_val32, f.diag, f.diag32, f.order_f, f.order_b, f.tasks_f, f.tasks_b,
-                  f.sf_ptr, f.sf_idx, f.sf_val, f.sf_val32, f.sb_ptr, f.sb_idx, f.sb_val, f.sb_val32,
                   f.pack_f, f.pack_b, f.pf_idx, f.pf_val, f.pf_val32, f.pb_idx, f.pb_val, f.pb_val32,
                   f.split_f, f.split_b, f.psum_f, f.psum_b, f.pcount_f, f.pcount_b, f.srow_f, f.srow_b,
-                  f.hb_lv, f.hb_idx};
+                  f.hb_lv, f.hb_idx, f.sf_ptr, f.sf_idx, f.sf_val, f.sf_val32, f.sb_ptr, f.sb_idx, f.sb_val,
+                  f.sb_val32};
     for (void* p : ps) cudaFree(p);
     f = DevFactor();
 }
@@ -1008,8 +1008,24 @@ namespace {
 
 bool valid_k(int k) { return k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32; }
 
+// The multi-RHS layouts of a factor (rchol::build_solve_layouts), built on
+// its first k > 1 use: a cache of the factor's rows, so a const factor is
+// extended in place.  Uses the context's scratch, which holds nothing here.
+rchol_status ensure_layouts(rchol_ctx* ctx, const rchol_factor_t* f) {
+    rchol_factor_t* mf = const_cast<rchol_factor_t*>(f);
+    if (mf->F.lay_ready) return RCHOL_OK;
+    const cudaError_t e = rchol::build_solve_layouts(mf->F, ctx->scratch, ctx->stream);
+    ctx->scratch.reset();
+    CK(e, "multi-RHS layouts");
+    return RCHOL_OK;
+}
+
 rchol_status get_solver(rchol_ctx* ctx, const rchol_factor_t* f, int k) {
     const rchol_opts& o = ctx->o;
+    if (k > 1) {
+        const rchol_status ls = ensure_layouts(ctx, f);
+        if (ls != RCHOL_OK) return ls;
+    }
     const int fp32 = o.precision == RCHOL_PREC_FP32_FACTOR;
     const bool want_sell = k == 1 && o.spmv_layout == RCHOL_SPMV_AUTO;
     if (want_sell && !ctx->sell_tried) {
@@ -1190,7 +1206,9 @@ extern "C" rchol_status rchol_precond_apply(rchol_ctx* ctx, const rchol_factor_t
     if (!ctx->have || ctx->At.n != f->F.n) return fail(ctx, RCHOL_ERR_INVALID, "factor does not match the matrix");
     cudaSetDevice(ctx->device);
     const size_t elems = (size_t)f->F.n * (size_t)k;
-    rchol_status s = ensure_stage(ctx, 2 * elems);
+    rchol_status s = k > 1 ? ensure_layouts(ctx, f) : RCHOL_OK;
+    if (s != RCHOL_OK) return s;
+    s = ensure_stage(ctx, 2 * elems);
     if (s != RCHOL_OK) return s;
     s = stage_in(ctx, R, ldb, k, on_device, ctx->dB);
     if (s != RCHOL_OK) return s;
@@ -1517,6 +1535,10 @@ extern "C" rchol_status rchol_batch_solve(rchol_ctx* ctx, const rchol_factor_t* 
     cudaSetDevice(ctx->device);
     const rchol_opts& o = ctx->o;
     const int nsys = (int)ctx->batch_off.size() - 1;
+    if (k > 1) {
+        const rchol_status ls = ensure_layouts(ctx, f);
+        if (ls != RCHOL_OK) return ls;
+    }
     if (!(ctx->bsolver && ctx->bsolver_f == f && ctx->bsolver_k == k)) {
         drop_solver(ctx);
         rchol::SolveConfig cfg;
@@ -1529,7 +1551,7 @@ extern "C" rchol_status rchol_batch_solve(rchol_ctx* ctx, const rchol_factor_t* 
         cfg.use_graph = o.use_graph != 0;
         cfg.timeout_s = o.timeout_s;
         cfg.poll_ns = o.poll_ns;
-        if (cfg.fp32_factor && !f->F.sf_val32) return fail(ctx, RCHOL_ERR_INVALID, "factor has no FP32 copy");
+        if (cfg.fp32_factor && !f->F.lr_val32) return fail(ctx, RCHOL_ERR_INVALID, "factor has no FP32 copy");
         cudaError_t e = cudaSuccess;
         ctx->bsolver = rchol::batch_create(ctx->At, f->F, cfg, ctx->device, ctx->stream, ctx->batch_off.data(), nsys, &e);
         if (!ctx->bsolver) return cuda_fail(ctx, e, "create batch solver");

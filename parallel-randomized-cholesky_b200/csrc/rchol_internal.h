@@ -170,9 +170,13 @@ struct DevFactor {
     int2* tasks_f = nullptr;
     int2* tasks_b = nullptr;
     int32_t ntasks_f = 0, ntasks_b = 0;
-    // Solve layouts: the rows of Lr (forward) and of L^T = columns of Lc
-    // (backward) stored in schedule order, so that position p of order_f
-    // owns entries sf_ptr[p]..sf_ptr[p+1] (same for the backward side).
+    // Multi-RHS layouts (built on the first k > 1 use, build_solve_layouts):
+    // the rows of Lr (forward) and of L^T = columns of Lc (backward) copied
+    // in schedule order, so that position p of order_f owns entries
+    // sf_ptr[p]..sf_ptr[p+1] (same for the backward side) and consecutive
+    // rows of a schedule are adjacent in memory.  lay_ready is false until
+    // they hold this factor's rows (buffers of a released factor are reused).
+    bool lay_ready = false;
     int64_t* sf_ptr = nullptr;
     int32_t* sf_idx = nullptr;
     double* sf_val = nullptr;
@@ -250,6 +254,9 @@ constexpr int kLaneClasses = 6;
 // (stencil factors; measured 2-4% faster solves), else 2 (power-law factors,
 // whose long rows run slower with fewer lanes).
 inline int auto_sched_epl(int64_t max_row_len) { return max_row_len <= 1024 ? 3 : 2; }
+// The multi-RHS layouts of a factor (DevFactor::sf_ptr); no-op when built.
+cudaError_t build_solve_layouts(DevFactor& f, Scratch& sc, cudaStream_t s);
+
 // Shared-memory plan of the backward-head kernel: the head holds at most
 // kHeadMaxLevels levels of at most kHeadMaxRows rows and kHeadMaxTasks
 // tasks each; its stages (one level each, kHeadStages in flight) and the

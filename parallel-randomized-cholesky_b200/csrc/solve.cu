@@ -73,9 +73,10 @@ struct SolveArgs {
     const int64_t* __restrict__ s_ptr;
     const int32_t* __restrict__ s_idx;
     const double* __restrict__ s_val;
-    // factor
-    // forward / backward solve layouts: position p of order_f / order_b
-    // owns entries lr_ptr[p]..lr_ptr[p+1] / lc_ptr[p]..lc_ptr[p+1]
+    // factor for the k > 1 solves: with by_pos, the multi-RHS layouts
+    // (position p of order_f / order_b owns entries lr_ptr[p]..lr_ptr[p+1] /
+    // lc_ptr[p]..lc_ptr[p+1]); without, the strict CSR and CSC of L by row id
+    int32_t by_pos;
     const int64_t* __restrict__ lr_ptr;
     const int32_t* __restrict__ lr_idx;
     const void* __restrict__ lr_val;
@@ -630,7 +631,8 @@ __global__ void __launch_bounds__(kBlock) fwd_kernel(SolveArgs a) {
     bool ok = true;
     for (int64_t t = group; t < a.n && ok; t += ngroups) {
         const int64_t i = a.order_f[t];
-        const int64_t s = a.lr_ptr[t], e = a.lr_ptr[t + 1];
+        const int64_t ri_ = a.by_pos ? t : i;
+        const int64_t s = a.lr_ptr[ri_], e = a.lr_ptr[ri_ + 1];
         const size_t o = (size_t)i * K + c;
         double ri = a.r[o];
         if (a.update) {
@@ -680,7 +682,8 @@ __global__ void __launch_bounds__(kBlock) bwd_kernel(SolveArgs a) {
     bool ok = true;
     for (int64_t g = group; g < a.n && ok; g += ngroups) {
         const int64_t j = a.order_b[g];
-        const int64_t s = a.lc_ptr[g], e = a.lc_ptr[g + 1];
+        const int64_t rj_ = a.by_pos ? g : j;
+        const int64_t s = a.lc_ptr[rj_], e = a.lc_ptr[rj_ + 1];
         const double dj = to_d(dv[j]);
         const size_t o = (size_t)j * K + c;
         double t = a.y[o];
@@ -1320,6 +1323,27 @@ cudaError_t launch_coresident(const void* fn, int grid, Arg& a, cudaStream_t s) 
     return launch_coresident(fn, grid, params, s);
 }
 
+// The factor arrays of the k > 1 solves: the multi-RHS layouts when built,
+// else L's own rows and columns by row id.
+void set_factor_rows(SolveArgs& a, const DevFactor& F, bool fp32) {
+    a.by_pos = F.lay_ready ? 1 : 0;
+    if (F.lay_ready) {
+        a.lr_ptr = F.sf_ptr;
+        a.lr_idx = F.sf_idx;
+        a.lr_val = fp32 ? (const void*)F.sf_val32 : (const void*)F.sf_val;
+        a.lc_ptr = F.sb_ptr;
+        a.lc_idx = F.sb_idx;
+        a.lc_val = fp32 ? (const void*)F.sb_val32 : (const void*)F.sb_val;
+    } else {
+        a.lr_ptr = F.lr_ptr;
+        a.lr_idx = F.lr_idx;
+        a.lr_val = fp32 ? (const void*)F.lr_val32 : (const void*)F.lr_val;
+        a.lc_ptr = F.lc_ptr;
+        a.lc_idx = F.lc_idx;
+        a.lc_val = fp32 ? (const void*)F.lc_val32 : (const void*)F.lc_val;
+    }
+}
+
 int resident_blocks(const void* fn, int device) {
     int per_sm = 0, sms = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, 0);
@@ -1366,13 +1390,7 @@ class PcgSolver {
         a.s_ptr = S.sptr;
         a.s_idx = S.sidx;
         a.s_val = S.sval;
-        // the solves read the schedule-ordered layouts (row ranges by position)
-        a.lr_ptr = F.sf_ptr;
-        a.lr_idx = F.sf_idx;
-        a.lr_val = cfg.fp32_factor ? (const void*)F.sf_val32 : (const void*)F.sf_val;
-        a.lc_ptr = F.sb_ptr;
-        a.lc_idx = F.sb_idx;
-        a.lc_val = cfg.fp32_factor ? (const void*)F.sb_val32 : (const void*)F.sb_val;
+        set_factor_rows(a, F, cfg.fp32_factor);
         a.diag = cfg.fp32_factor ? (const void*)F.diag32 : (const void*)F.diag;
         a.order_f = F.order_f;
         a.order_b = F.order_b;
@@ -1498,7 +1516,7 @@ PcgSolver* pcg_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cf
     s->stream = stream;
     s->K = cfg.k;
     bool okk = cfg.fp32_factor ? bind_for_k<float>(s, cfg.k) : bind_for_k<double>(s, cfg.k);
-    if (!okk || (cfg.fp32_factor && !F.sf_val32)) {
+    if (!okk || (cfg.fp32_factor && !F.lr_val32)) {
         delete s;
         *err = cudaErrorInvalidValue;
         return nullptr;
@@ -1543,7 +1561,7 @@ PcgSolver* pcg_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cf
 cudaError_t pcg_rebind(PcgSolver* s, const DevCsc& A, const DevSell* sell, const DevFactor& F) {
     const bool want_sell = s->K == 1 && sell && sell->slots > 0 && sell->n == A.n;
     const bool has_sell = s->k_spmv == (void*)spmv_update_sell_kernel;
-    if (A.n != s->A.n || F.n != A.n || want_sell != has_sell || (s->cfg.fp32_factor && !F.sf_val32))
+    if (A.n != s->A.n || F.n != A.n || want_sell != has_sell || (s->cfg.fp32_factor && !F.lr_val32))
         return cudaErrorInvalidValue;
     s->A = A;
     s->S = want_sell ? *sell : DevSell();
@@ -2279,12 +2297,7 @@ static cudaError_t precond_apply_t(const DevFactor& F, const double* r, double* 
     SolveArgs a;
     memset(&a, 0, sizeof(a));
     a.n = F.n;
-    a.lr_ptr = F.sf_ptr;
-    a.lr_idx = F.sf_idx;
-    a.lr_val = std::is_same<TV, float>::value ? (const void*)F.sf_val32 : (const void*)F.sf_val;
-    a.lc_ptr = F.sb_ptr;
-    a.lc_idx = F.sb_idx;
-    a.lc_val = std::is_same<TV, float>::value ? (const void*)F.sb_val32 : (const void*)F.sb_val;
+    set_factor_rows(a, F, std::is_same<TV, float>::value);
     a.diag = std::is_same<TV, float>::value ? (const void*)F.diag32 : (const void*)F.diag;
     a.order_f = F.order_f;
     a.order_b = F.order_b;
@@ -2388,12 +2401,7 @@ cudaError_t precond_apply_noalloc_t(const DevFactor& F, const double* r, double*
     SolveArgs a;
     memset(&a, 0, sizeof(a));
     a.n = F.n;
-    a.lr_ptr = F.sf_ptr;
-    a.lr_idx = F.sf_idx;
-    a.lr_val = std::is_same<TV, float>::value ? (const void*)F.sf_val32 : (const void*)F.sf_val;
-    a.lc_ptr = F.sb_ptr;
-    a.lc_idx = F.sb_idx;
-    a.lc_val = std::is_same<TV, float>::value ? (const void*)F.sb_val32 : (const void*)F.sb_val;
+    set_factor_rows(a, F, std::is_same<TV, float>::value);
     a.diag = std::is_same<TV, float>::value ? (const void*)F.diag32 : (const void*)F.diag;
     a.order_f = F.order_f;
     a.order_b = F.order_b;

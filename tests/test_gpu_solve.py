@@ -416,3 +416,36 @@ def test_backward_head_matches_persistent_kernel(precision):
     assert abs(ih["iterations"] - inn["iterations"]) <= 1
     np.testing.assert_allclose(x2h, x2n, rtol=0, atol=1e-12 * np.abs(x2n).max())
     assert np.linalg.norm(xh - xn) <= 1e-7 * np.linalg.norm(xn)
+
+
+def test_multi_rhs_layouts_built_on_first_use():
+    """A factor's multi-RHS layouts (its rows copied in schedule order) are
+    built on its first k > 1 apply or solve; before that the k > 1 sweeps
+    read L's rows by row id.  Both forms sum the same entries in the same
+    order: the allocation-free apply gives the same bits before and after."""
+    torch = pytest.importorskip("torch")
+    n, r, c, v, g = grid_laplacian((18, 16, 14), seed=47, excess_frac=0.05)
+    ctx = R.Context(seed=5, precision=R.PREC_FP32_FACTOR)
+    try:
+        ctx.set_triplets(n, r, c, v, trim_ground=g)
+        f = ctx.factor()
+        ns = f.info().n
+        k = 4
+        Rh = np.random.default_rng(9).standard_normal((ns, k))
+        dev = torch.device("cuda", 0)
+        Rd = torch.from_numpy(Rh).to(dev).contiguous()
+        stream = torch.cuda.current_stream().cuda_stream
+        out = []
+        for step in range(2):
+            Zd = torch.full((ns, k), float("nan"), dtype=torch.float64, device=dev)
+            torch.cuda.synchronize()
+            ctx.precond_apply_noalloc(f, Rd.data_ptr(), Zd.data_ptr(), k, True, stream)
+            torch.cuda.synchronize()
+            out.append(Zd.cpu().numpy())
+            if step == 0:
+                ref = ctx.precond_apply(f, Rh, fp32=True)  # builds the layouts
+        assert np.array_equal(out[0], out[1])
+        np.testing.assert_allclose(out[1], ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+        f.free()
+    finally:
+        ctx.close()
