@@ -450,6 +450,16 @@ __global__ void permute_rows_kernel(int32_t n, const int32_t* __restrict__ order
     }
 }
 
+// flag = 1 unless colptr[0] = 0, colptr[n] = nnz and colptr never decreases
+__global__ void colptr_check_kernel(const int32_t* __restrict__ colptr, int32_t n, int32_t nnz, int32_t* flag) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += stride) {
+        const int32_t c = colptr[i];
+        const bool bad = (i == 0 && c != 0) || (i == n && c != nnz) || (i < n && colptr[i + 1] < c);
+        if (bad) *flag = 1;
+    }
+}
+
 __global__ void max_kernel(const int32_t* __restrict__ a, int64_t n, int32_t* out) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int32_t m = 0;
@@ -1029,6 +1039,12 @@ cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bo
 
 cudaError_t max_i32(const int32_t* v, int64_t n, int32_t* out, cudaStream_t s) {
     max_kernel<<<grid_for(n, 256), 256, 0, s>>>(v, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t check_colptr(const int32_t* colptr, int32_t n, int32_t nnz, int32_t* flag, cudaStream_t s) {
+    RCHOL_TRY(cudaMemsetAsync(flag, 0, sizeof(int32_t), s));
+    colptr_check_kernel<<<grid_for((int64_t)n + 1, 256), 256, 0, s>>>(colptr, n, nnz, flag);
     return cudaGetLastError();
 }
 

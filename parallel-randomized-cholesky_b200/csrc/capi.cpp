@@ -59,6 +59,11 @@ struct rchol_ctx {
     std::vector<rchol_factor_t*> live;
     // the autotuner's record of each vertex's gathered entries (device, n)
     int32_t* gsize = nullptr;
+    // device flag of the input checks
+    int32_t* dflag = nullptr;
+    // second stream: input checks and counts under the value upload
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_struct = nullptr;
 };
 
 struct rchol_factor {
@@ -178,8 +183,9 @@ rchol_status alloc_work(rchol_ctx* ctx, const PoolPlan& pp) {
 }
 
 // Strict-lower nnz of the loaded matrix (device count + scan).
-rchol_status lower_nnz(rchol_ctx* ctx, int64_t* out) {
+rchol_status lower_nnz(rchol_ctx* ctx, int64_t* out, cudaStream_t st = nullptr) {
     const int32_t n = ctx->A.n;
+    if (!st) st = ctx->stream;
     int32_t* cnt = nullptr;
     int64_t* ptr = nullptr;
     void* tmp = nullptr;
@@ -191,17 +197,17 @@ rchol_status lower_nnz(rchol_ctx* ctx, int64_t* out) {
     CK(ctx->scratch.get(&cnt, n), "alloc counts");
     CK(ctx->scratch.get(&ptr, (int64_t)n + 1), "alloc ptr");
     CK(ctx->scratch.get((char**)&tmp, (int64_t)rchol::scan_tmp_bytes(n)), "alloc scan");
-    CK(rchol::launch_count_lower(ctx->A, cnt, ctx->stream), "count lower");
-    CK(rchol::exclusive_scan_i32_to_i64(cnt, ptr, n, tmp, ctx->stream), "scan lower");
-    CK(cudaMemcpyAsync(out, ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream), "copy lnnz");
-    CK(cudaStreamSynchronize(ctx->stream), "sync lnnz");
+    CK(rchol::launch_count_lower(ctx->A, cnt, st), "count lower");
+    CK(rchol::exclusive_scan_i32_to_i64(cnt, ptr, n, tmp, st), "scan lower");
+    CK(cudaMemcpyAsync(out, ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st), "copy lnnz");
+    CK(cudaStreamSynchronize(st), "sync lnnz");
     // the largest strict-lower column (the scan scratch's first word holds it)
     int32_t* dmax = reinterpret_cast<int32_t*>(tmp);
     int32_t hmax = 0;
-    CK(cudaMemsetAsync(dmax, 0, sizeof(int32_t), ctx->stream), "clear max");
-    CK(rchol::max_i32(cnt, n, dmax, ctx->stream), "max lower");
-    CK(cudaMemcpyAsync(&hmax, dmax, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream), "copy max");
-    CK(cudaStreamSynchronize(ctx->stream), "sync max");
+    CK(cudaMemsetAsync(dmax, 0, sizeof(int32_t), st), "clear max");
+    CK(rchol::max_i32(cnt, n, dmax, st), "max lower");
+    CK(cudaMemcpyAsync(&hmax, dmax, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "copy max");
+    CK(cudaStreamSynchronize(st), "sync max");
     ctx->max_lower = hmax;
     return RCHOL_OK;
 }
@@ -332,6 +338,9 @@ extern "C" void rchol_destroy(rchol_ctx* ctx) {
     cudaFree(ctx->dB);
     cudaFree(ctx->dX);
     cudaFree(ctx->gsize);
+    cudaFree(ctx->dflag);
+    if (ctx->ev_struct) cudaEventDestroy(ctx->ev_struct);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -385,8 +394,6 @@ extern "C" rchol_status rchol_set_csc(rchol_ctx* ctx, int n, const int* colptr, 
         CK(cudaMemcpy(&nnz32, colptr + n, sizeof(int32_t), cudaMemcpyDeviceToHost), "read nnz");
     } else {
         nnz32 = colptr[n];
-        for (int i = 0; i < n; ++i)
-            if (colptr[i + 1] < colptr[i]) return fail(ctx, RCHOL_ERR_INVALID, "colptr is not monotone");
     }
     if (nnz32 < 0) return fail(ctx, RCHOL_ERR_INVALID, "negative nnz");
     // a matrix of the same shape reuses every device buffer (new values or a
@@ -419,10 +426,28 @@ extern "C" rchol_status rchol_set_csc(rchol_ctx* ctx, int n, const int* colptr, 
     }
     ctx->have = false;
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (!ctx->dflag) CK(cudaMalloc(&ctx->dflag, sizeof(int32_t)), "alloc flag");
+    if (!ctx->side) CK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking), "side stream");
+    if (!ctx->ev_struct) CK(cudaEventCreateWithFlags(&ctx->ev_struct, cudaEventDisableTiming), "event");
     CK(cudaMemcpyAsync(A.colptr, colptr, sizeof(int32_t) * ((size_t)n + 1), kind, ctx->stream), "copy colptr");
     CK(cudaMemcpyAsync(A.rowind, rowind, sizeof(int32_t) * (size_t)A.nnz, kind, ctx->stream), "copy rowind");
+    CK(cudaEventRecord(ctx->ev_struct, ctx->stream), "record");
     CK(cudaMemcpyAsync(A.val, val, sizeof(double) * (size_t)A.nnz, kind, ctx->stream), "copy val");
     ctx->A = A;
+    // under the value upload, on the side stream: colptr checked on the
+    // device (the host arrays are not walked), then the strict-lower counts
+    // that decide whether the factor work can be kept
+    int32_t bad = 0;
+    CK(cudaStreamWaitEvent(ctx->side, ctx->ev_struct, 0), "wait structure");
+    CK(rchol::check_colptr(A.colptr, n, nnz32, ctx->dflag, ctx->side), "check colptr");
+    CK(cudaMemcpyAsync(&bad, ctx->dflag, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->side), "read flag");
+    CK(cudaStreamSynchronize(ctx->side), "sync check");
+    const bool recount = same && ctx->w_ready && !bad;
+    int64_t lnnz = 0;
+    rchol_status ls = recount ? lower_nnz(ctx, &lnnz, ctx->side) : RCHOL_OK;
+    CK(cudaStreamSynchronize(ctx->stream), "sync upload");
+    if (bad) return fail(ctx, RCHOL_ERR_INVALID, "colptr is not monotone (or colptr[0] != 0)");
+    if (ls != RCHOL_OK) return ls;
     ctx->trim = trim_ground != 0;
     if (ctx->trim) {
         rchol::DevCsc At = ctx->At;
@@ -435,10 +460,7 @@ extern "C" rchol_status rchol_set_csc(rchol_ctx* ctx, int n, const int* colptr, 
     }
     CK(cudaStreamSynchronize(ctx->stream), "sync upload");
     ctx->have = true;
-    if (same && ctx->w_ready) {
-        int64_t lnnz = 0;
-        rchol_status s = lower_nnz(ctx, &lnnz);
-        if (s != RCHOL_OK) return s;
+    if (recount) {
         if (lnnz != old_lnnz || 4 * (int64_t)ctx->max_lower > ctx->w.hscratch_entries) {
             free_work(ctx->w);
             ctx->w_ready = false;

@@ -311,6 +311,9 @@ cudaError_t assemble_factor(const FactorWork& w, bool trim_ground, bool make_fp3
                             bool bwd_head, double timeout_s, Scratch& sc, DevFactor& f, cudaStream_t s);
 // Drop the last row/column of A (ground vertex) into `out`, whose buffers
 // are reused when large enough (else reallocated).
+// flag (device int) = 1 unless colptr[0] = 0, colptr[n] = nnz and colptr
+// is monotone.
+cudaError_t check_colptr(const int32_t* colptr, int32_t n, int32_t nnz, int32_t* flag, cudaStream_t s);
 cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, Scratch& sc, cudaStream_t s);
 
 // Return the CUDA error of `x` from the enclosing function.

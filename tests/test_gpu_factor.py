@@ -204,6 +204,30 @@ def test_invalid_inputs_report_status():
         ctx.close()
 
 
+def test_bad_colptr_is_rejected_on_the_device():
+    """set_csc checks colptr (starts at 0, never decreases, ends at nnz) on
+    the device after the upload; a bad one reports RCHOL_ERR_INVALID and
+    leaves the context without a matrix, and a good one loads after it."""
+    n, r, c, v, _ = grid_laplacian((6, 5), seed=2)
+    cp, ri, val = R.csc_from_triplets(n, r, c, v)
+    ctx = R.Context()
+    try:
+        bad = cp.copy()
+        bad[3], bad[4] = bad[4], bad[3]
+        with pytest.raises(R.RcholError) as e:
+            ctx.set_csc(n, bad, ri, val)
+        assert e.value.status == 1
+        with pytest.raises(R.RcholError) as e:
+            ctx.factor()
+        assert e.value.status == 9
+        ctx.set_csc(n, cp, ri, val)
+        f = ctx.factor()
+        assert f.info().n == n
+        f.free()
+    finally:
+        ctx.close()
+
+
 def test_factor_timeout_is_reported_then_recovers():
     """A wait limit far below the elimination's queue waits: the factor
     kernel gives up with RCHOL_ERR_TIMEOUT (bounded device waits, no hang),
