@@ -474,35 +474,38 @@ __device__ bool eliminate_small(const FactorArgs& a, int32_t k, int total, int32
     const unsigned hb = __ballot_sync(kFull, head);
     const int m = __popc(hb);
     const int src = lane < m ? (int)__fns(hb, 0, lane + 1) : 0;
-    int32_t mrow = __shfl_sync(kFull, row, src);
+    // merged entries in row order, entry `lane` in this lane
+    int32_t orow = __shfl_sync(kFull, row, src);
+    int ocnt = __shfl_sync(kFull, cnt, src);
     double mval = __shfl_sync(kFull, acc, src);
-    int mcnt = __shfl_sync(kFull, cnt, src);
-    int pos = lane;  // position in row order
     if (lane >= m) {
-        mrow = INT_MAX;
+        orow = INT_MAX;
+        ocnt = 0;
         mval = __longlong_as_double((long long)kInfBits);
-        mcnt = 0;
     }
-    // sort by (value, row) carrying (multiplicity, row-order position)
+    int pos = lane;  // position in row order
+    // sort by (value, row) carrying the row-order position.  Rows are unique
+    // and ascend with the position, so ties in value break on the position
+    // exactly as on the row (padding, all +inf, sorts last in any order);
+    // the row and multiplicity are fetched by position afterwards, which
+    // keeps two shuffles per stage off the shared-memory/shuffle pipe.
 #pragma unroll
     for (int kk = 2; kk <= 32; kk <<= 1) {
 #pragma unroll
         for (int j = kk >> 1; j > 0; j >>= 1) {
             const double v2 = __shfl_xor_sync(kFull, mval, j);
-            const int32_t r2 = __shfl_xor_sync(kFull, mrow, j);
-            const int c2 = __shfl_xor_sync(kFull, mcnt, j);
             const int p2 = __shfl_xor_sync(kFull, pos, j);
             const bool keep_min = ((lane & j) == 0) == ((lane & kk) == 0);
-            const bool self_gt = (mval > v2) || (mval == v2 && mrow > r2);
-            const bool other_gt = (v2 > mval) || (v2 == mval && r2 > mrow);
+            const bool self_gt = (mval > v2) || (mval == v2 && pos > p2);
+            const bool other_gt = (v2 > mval) || (v2 == mval && p2 > pos);
             if (keep_min ? self_gt : other_gt) {
                 mval = v2;
-                mrow = r2;
-                mcnt = c2;
                 pos = p2;
             }
         }
     }
+    const int32_t mrow = __shfl_sync(kFull, orow, pos);
+    const int mcnt = __shfl_sync(kFull, ocnt, pos);
     // inclusive prefix sum (one 32-wide Kogge-Stone chunk)
     double cum = lane < m ? mval : 0.0;
 #pragma unroll
