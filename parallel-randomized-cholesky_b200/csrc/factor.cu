@@ -31,7 +31,7 @@ constexpr unsigned long long kInfBits = 0x7ff0000000000000ull;
 constexpr int kSlabBytesPerEntry = 32;     // 8 (a_val) + 8 (b_val) + 8 (b_aux) + 4 + 4
 
 enum Counter { kQHead = 0, kQTail = 1, kChunkCursor = 2, kStatus = 3, kAbort = 4, kBigCount = 5,
-               kMaxGather = 6, kOverflowFills = 7, kDone = 8 };
+               kMaxGather = 6, kOverflowFills = 7, kDone = 8, kTailTicket = 9 };
 
 __device__ __forceinline__ int pow2_at_least(int x) {
     int p = 1;
@@ -940,11 +940,14 @@ __global__ void __launch_bounds__(256, 3) factor_kernel(FactorArgs a) {
 
 // ---- cooperative elimination of the tail -----------------------------------
 // The last vertices of a power-law graph (hubs and the dense core) depend
-// on one another in a chain and gather thousands of entries each; a warp
-// per vertex leaves the rest of the GPU idle while it sorts.  Vertices
-// >= tail are therefore eliminated after factor_kernel by one CTA of
-// kTailThreads threads, in index order (every dependency of a vertex has a
-// smaller index, so each column is final when its turn comes).  The steps
+// on one another in long chains and gather thousands of entries each; a
+// warp per vertex leaves the rest of the GPU idle while it sorts.  Vertices
+// >= tail are therefore eliminated after factor_kernel by kHugeSlabs CTAs of
+// kTailThreads threads, a whole CTA per vertex.  A CTA claims the next
+// vertex in index order and waits on its dependency counter (every
+// dependency has a smaller index, hence was claimed earlier by a running
+// CTA), then keeps the counters as factor_kernel does: +1 per fill row,
+// -multiplicity per neighbour once the column is written.  The steps
 // and their rounding are those of eliminate_slab<true> -- the same radix
 // orders, duplicate runs added in sorted order, 32-wide Kogge-Stone chunks
 // with the carry chained in chunk order, the same sampling search -- so the
@@ -1121,12 +1124,51 @@ __global__ void __launch_bounds__(kTailThreads, 1) factor_tail_kernel(FactorArgs
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     long long fills = 0;
-    int max_gather = 0, done = 0;
+    int max_gather = 0;
+    __shared__ int32_t sh_k;
     if (threadIdx.x == 0) sh_stop = 0;
     __syncthreads();
-    Slab s = make_global_slab(a.hscratch, (int)a.hscratch_entries);
-    for (int32_t k = a.tail; k < a.n; ++k) {
-        if (aborted(a)) break;
+    // CTA b works in huge slab b (the persistent kernel, which shares them
+    // under locks, has finished)
+    Slab s = make_global_slab(a.hscratch + (size_t)blockIdx.x * (size_t)a.hscratch_entries * kGlobalSlabBytes,
+                              (int)a.hscratch_entries);
+    const unsigned long long t0 = global_timer_ns();
+    while (true) {
+        // claim the next tail vertex in index order and wait until every
+        // column it depends on is eliminated (all have lower indices, so
+        // they were claimed earlier by running CTAs); the wait is bounded
+        // by time without progress of the eliminated count
+        if (threadIdx.x == 0) {
+            int32_t k = a.tail + atomicAdd(a.counters + kTailTicket, 1);
+            if (k < a.n) {
+                unsigned spins = 0;
+                int seen = -1;
+                unsigned long long since = t0;
+                while (ld_acquire(a.dep + k) > 0) {
+                    if ((++spins & 63u) == 0) {
+                        if (aborted(a)) {
+                            k = a.n;
+                            break;
+                        }
+                        const int d = ld_relaxed(a.counters + kDone);
+                        const unsigned long long now = global_timer_ns();
+                        if (d != seen) {
+                            seen = d;
+                            since = now;
+                        } else if (now - since > a.timeout_ns) {
+                            fail(a, kDevTimeout);
+                            k = a.n;
+                            break;
+                        }
+                    }
+                }
+            }
+            sh_k = k;
+        }
+        __syncthreads();
+        const int32_t k = sh_k;
+        if (k >= a.n) break;
+        __threadfence();
         const int nf = ld_relaxed(a.fcnt + k);
         const int oc0 = a.lcolptr[k];
         const int ocnt = a.lcolptr[k + 1] - oc0;
@@ -1134,13 +1176,14 @@ __global__ void __launch_bounds__(kTailThreads, 1) factor_tail_kernel(FactorArgs
         const int no = ocnt - min(ocnt, a.c0);
         const int total = nf + no;
         if (a.gsize && threadIdx.x == 0) a.gsize[k] = total;
-        ++done;
         if (total == 0) {
             if (threadIdx.x == 0) {
                 a.diag[k] = 0.0;
                 a.pcnt[k] = 0;
                 a.pstart[k] = 0;
+                atomicAdd(a.counters + kDone, 1);
             }
+            __syncthreads();
             continue;
         }
         if (total > max_gather) max_gather = total;
@@ -1299,6 +1342,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) factor_tail_kernel(FactorArgs
             const int32_t gcol = r_i > r_j ? r_j : r_i;
             const double gval = __ddiv_rn(__dmul_rn(s.b_val[i], rem_i), S);
             if (!append_fill(a, gcol, grow, gval)) ok = false;
+            atomicAdd(a.dep + grow, 1);
         }
         // rows of L column k are one level below k (the solve schedules)
         const int lk = ld_relaxed(a.level + k) + 1;
@@ -1307,11 +1351,16 @@ __global__ void __launch_bounds__(kTailThreads, 1) factor_tail_kernel(FactorArgs
             if (threadIdx.x == 0) fail(a, kDevCapacity);
             break;
         }
+        // fills, pool writes and levels visible before any neighbour is
+        // released: each neighbour's counter drops by its multiplicity
         __threadfence();
+        __syncthreads();
+        for (int i = threadIdx.x; i < m; i += blockDim.x)
+            atom_add_acq_rel(a.dep + s.b_row[i], -(int)(s.b_aux[i] >> 32));
+        if (threadIdx.x == 0) atomicAdd(a.counters + kDone, 1);
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        atomicAdd(a.counters + kDone, done);
         atomicMax(a.counters + kMaxGather, max_gather);
         atomicAdd(a.pool_cursor + 1, (unsigned long long)fills);
     }
@@ -1564,10 +1613,11 @@ cudaError_t launch_factor(FactorWork& w, const FactorLaunch& cfg, cudaStream_t s
     factor_kernel<<<cfg.grid, cfg.block, smem, s>>>(a);
     RCHOL_TRY(cudaGetLastError());
     if (a.tail < w.n) {
-        // the tail, one CTA, in index order, after the rest is eliminated
+        // the tail after the rest is eliminated: kHugeSlabs CTAs, each a
+        // vertex at a time, claimed in index order
         const size_t tsmem = tail_smem_bytes();
         RCHOL_TRY(cudaFuncSetAttribute(factor_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
-        factor_tail_kernel<<<1, kTailThreads, tsmem, s>>>(a);
+        factor_tail_kernel<<<kHugeSlabs, kTailThreads, tsmem, s>>>(a);
         RCHOL_TRY(cudaGetLastError());
     }
     return cudaSuccess;
