@@ -172,10 +172,15 @@ rchol_status alloc_work(rchol_ctx* ctx, const PoolPlan& pp) {
     CK(dalloc(&w.level, n), "alloc levels");
     CK(cudaMalloc((void**)&w.gscratch, (size_t)warps * (size_t)w.gscratch_entries * rchol::kGlobalSlabBytes),
        "alloc slab scratch");
-    CK(cudaMalloc((void**)&w.hscratch, (size_t)rchol::kHugeSlabs * (size_t)w.hscratch_entries * rchol::kGlobalSlabBytes),
+    {
+        const size_t slab = (size_t)w.hscratch_entries * rchol::kGlobalSlabBytes;
+        w.nhuge = (int32_t)std::max<size_t>(rchol::kHugeSlabsMin,
+                                            std::min<size_t>(rchol::kHugeSlabsMax, rchol::kHugeSlabBudget / slab));
+    }
+    CK(cudaMalloc((void**)&w.hscratch, (size_t)w.nhuge * (size_t)w.hscratch_entries * rchol::kGlobalSlabBytes),
        "alloc shared slabs");
-    CK(dalloc(&w.hlock, rchol::kHugeSlabs), "alloc slab locks");
-    CK(cudaMemset(w.hlock, 0, sizeof(int32_t) * rchol::kHugeSlabs), "clear slab locks");
+    CK(dalloc(&w.hlock, w.nhuge), "alloc slab locks");
+    CK(cudaMemset(w.hlock, 0, sizeof(int32_t) * w.nhuge), "clear slab locks");
     CK(dalloc(&w.counters, 16), "alloc counters");
     CK(dalloc(&w.counters64, 4), "alloc counters64");
     CK(cudaMalloc(&w.scan_tmp, rchol::scan_tmp_bytes(n)), "alloc scan scratch");
@@ -683,7 +688,7 @@ extern "C" rchol_status rchol_factor(rchol_ctx* ctx, rchol_factor_t** out) {
         pp.c0 = o.bucket_cap;
         pp.nchunks = (int32_t)std::min<int64_t>(INT32_MAX / 64, std::max<int64_t>(4096, lnnz / 16 + ctx->A.n / 8));
         pp.pool_cap = (int64_t)(o.pool_mult * (double)lnnz) + ctx->A.n + (int64_t)max_grid * (block / 32) * 1024;
-        // per-warp scratch up to 4096 entries; larger gathers share kHugeSlabs slabs
+        // per-warp scratch up to 4096 entries; larger gathers share nhuge slabs
         const int64_t want = std::max<int64_t>(1024, pow2_ge(4 * (int64_t)ctx->max_lower));
         pp.gscratch_entries = std::min<int64_t>(want, 4096);
         pp.hscratch_entries = want;

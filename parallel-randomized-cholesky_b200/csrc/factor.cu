@@ -318,6 +318,7 @@ struct FactorArgs {
     int64_t gscratch_entries;
     unsigned char* hscratch;
     int64_t hscratch_entries;
+    int32_t nhuge;
     int32_t* hlock;
     int32_t* counters;
     unsigned long long* pool_cursor;
@@ -585,7 +586,7 @@ __device__ int acquire_huge(const FactorArgs& a, int lane) {
         const unsigned long long t0 = global_timer_ns();
         unsigned spins = 0;
         while (got < 0) {
-            for (int i = 0; i < kHugeSlabs && got < 0; ++i)
+            for (int i = 0; i < a.nhuge && got < 0; ++i)
                 if (atomicCAS(a.hlock + i, 0, 1) == 0) got = i;
             if (got >= 0 || aborted(a)) break;
             if ((++spins & 63u) == 0 && global_timer_ns() - t0 > a.timeout_ns) {
@@ -942,7 +943,7 @@ __global__ void __launch_bounds__(256, 3) factor_kernel(FactorArgs a) {
 // The last vertices of a power-law graph (hubs and the dense core) depend
 // on one another in long chains and gather thousands of entries each; a
 // warp per vertex leaves the rest of the GPU idle while it sorts.  Vertices
-// >= tail are therefore eliminated after factor_kernel by kHugeSlabs CTAs of
+// >= tail are therefore eliminated after factor_kernel by nhuge CTAs of
 // kTailThreads threads, a whole CTA per vertex.  A CTA claims the next
 // vertex in index order and waits on its dependency counter (every
 // dependency has a smaller index, hence was claimed earlier by a running
@@ -1543,7 +1544,7 @@ cudaError_t launch_init_factor_state(FactorWork& w, cudaStream_t s) {
     if ((e = cudaMemsetAsync(w.level, 0, sizeof(int32_t) * (size_t)w.n, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.counters, 0, sizeof(int32_t) * 16, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.counters64, 0, sizeof(unsigned long long) * 4, s)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(w.hlock, 0, sizeof(int32_t) * kHugeSlabs, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(w.hlock, 0, sizeof(int32_t) * w.nhuge, s)) != cudaSuccess) return e;
     prefill_bucket_kernel<<<grid_for((int64_t)w.n * 32, 256), 256, 0, s>>>(w.n, w.c0, w.lcolptr, w.lrow, w.lval,
                                                                             w.fcnt, w.brow, w.bval);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1597,6 +1598,7 @@ cudaError_t launch_factor(FactorWork& w, const FactorLaunch& cfg, cudaStream_t s
     a.gscratch_entries = w.gscratch_entries;
     a.hscratch = w.hscratch;
     a.hscratch_entries = w.hscratch_entries;
+    a.nhuge = w.nhuge;
     a.hlock = w.hlock;
     a.counters = w.counters;
     a.pool_cursor = w.counters64;
@@ -1613,11 +1615,11 @@ cudaError_t launch_factor(FactorWork& w, const FactorLaunch& cfg, cudaStream_t s
     factor_kernel<<<cfg.grid, cfg.block, smem, s>>>(a);
     RCHOL_TRY(cudaGetLastError());
     if (a.tail < w.n) {
-        // the tail after the rest is eliminated: kHugeSlabs CTAs, each a
-        // vertex at a time, claimed in index order
+        // the tail after the rest is eliminated: one CTA per shared slab,
+        // each a vertex at a time, claimed in index order
         const size_t tsmem = tail_smem_bytes();
         RCHOL_TRY(cudaFuncSetAttribute(factor_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
-        factor_tail_kernel<<<kHugeSlabs, kTailThreads, tsmem, s>>>(a);
+        factor_tail_kernel<<<w.nhuge, kTailThreads, tsmem, s>>>(a);
         RCHOL_TRY(cudaGetLastError());
     }
     return cudaSuccess;

@@ -133,6 +133,7 @@ struct FactorWork {
     // a few shared slabs for vertices larger than the per-warp scratch,
     // each taken with a lock word (hlock[i] = 1 while held)
     int64_t hscratch_entries = 0; // entries per shared slab
+    int32_t nhuge = 0;            // shared slabs (and cooperative-tail CTAs)
     unsigned char* hscratch = nullptr;
     int32_t* hlock = nullptr;
     // counters: [0] queue head, [1] queue tail, [2] chunk cursor, [3] status,
@@ -323,8 +324,12 @@ cudaError_t trim_matrix(const DevCsc& A, DevCsc& out, Scratch& sc, cudaStream_t 
         if (e__ != cudaSuccess) return e__; \
     } while (0)
 
-// Shared large slabs of the elimination kernel.
-constexpr int kHugeSlabs = 8;
+// Shared large slabs of the elimination kernel: between kHugeSlabsMin and
+// kHugeSlabsMax (as many as fit kHugeSlabBudget bytes); the cooperative
+// tail runs one CTA per slab.
+constexpr int kHugeSlabsMin = 8;
+constexpr int kHugeSlabsMax = 32;
+constexpr size_t kHugeSlabBudget = size_t(512) << 20;
 // Bytes per entry of elimination slabs in global memory (with radix-sort buffers).
 constexpr int kGlobalSlabBytes = 56;
 
