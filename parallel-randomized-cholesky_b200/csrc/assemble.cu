@@ -928,7 +928,7 @@ static cudaError_t build_bwd_head(DevFactor& f, const int32_t* levb, Scratch& sc
         const int ntask = h[l + 1].x - h[l].x, units = h[l + 1].y - h[l].y, rows = h[l + 1].z - h[l].z;
         if (rows > kHeadMaxRows || ntask > kHeadMaxTasks) break;
         const int st = std::max(stage, head_stage_bytes(ntask, units, rows, 8));
-        if (head_smem_bytes(h[l + 1].z, l + 1, st) > kHeadSmem) break;
+        if (head_smem_bytes(h[l + 1].z, st) > kHeadSmem) break;
         stage = st;
         nlev = l + 1;
     }

@@ -264,7 +264,11 @@ cudaError_t build_solve_layouts(DevFactor& f, Scratch& sc, cudaStream_t s);
 // per-row arrays fit kHeadSmem.
 constexpr int kHeadThreads = 512;
 constexpr int kHeadStages = 5;
-constexpr int kHeadMaxLevels = 1024;
+constexpr int kHeadMaxLevels = 16384;
+// level-table entries the head kernel keeps in shared memory (a ring filled
+// kHeadLvAhead levels ahead)
+constexpr int kHeadLvRing = 16;
+constexpr int kHeadLvAhead = 9;
 constexpr int kHeadMaxRows = 1024;
 // one task per warp of the 16-warp CTA: levels with more tasks than warps
 // took longer in the head kernel than in the persistent one
@@ -278,9 +282,9 @@ inline int head_stage_bytes(int ntask, int units, int rows, int vb) {
     return 16 * ntask + 128 * units + 32 * vb * units + 2 * al(8 * rows) + al(vb * rows);
 }
 // Dynamic shared memory of the head kernel: row ids and z values of every
-// head row, the level table and the stages.
-inline int head_smem_bytes(int rows, int nlev, int stage) {
-    return ((4 * rows + 15) & ~15) + ((8 * rows + 15) & ~15) + 16 * (nlev + 1) + kHeadStages * stage;
+// head row, the level-table ring and the stages.
+inline int head_smem_bytes(int rows, int stage) {
+    return ((4 * rows + 15) & ~15) + ((8 * rows + 15) & ~15) + 16 * kHeadLvRing + kHeadStages * stage;
 }
 // bwd_head (exact levels only): build the backward head (DevFactor::hb_nlev).
 cudaError_t build_solve_schedule(DevFactor& f, const int32_t* level, int epl, bool exact_bwd, bool bwd_head,

@@ -1089,11 +1089,12 @@ __device__ __forceinline__ HeadLevel head_level(const int4& lo, const int4& hi) 
     return L;
 }
 
-// Copies of level l into its stage, spread over threads tid of nthr.
+// Copies of level l into its stage, spread over threads tid of nthr; lv is
+// the shared ring of level-table entries (entry x in slot x % kHeadLvRing).
 template <typename TV>
 __device__ __forceinline__ void head_issue(const SolveArgs& a, const int4* lv, const int32_t* rows_s, int l,
                                            char* buf, int tid, int nthr) {
-    const int4 lo = lv[l], hi = lv[l + 1];
+    const int4 lo = lv[l & (kHeadLvRing - 1)], hi = lv[(l + 1) & (kHeadLvRing - 1)];
     const HeadLevel L = head_level<TV>(lo, hi);
     for (int i = tid; i < L.ntask; i += nthr) cp_async16(buf + 16 * i, a.pack_b + lo.x + i);
     const char* gi = reinterpret_cast<const char*>(a.hb_idx + (size_t)lo.y * 32);
@@ -1115,14 +1116,17 @@ __global__ void __launch_bounds__(kHeadThreads, 1) bwd_head_kernel(SolveArgs a) 
     if ((a.reduce || a.seg) && ld_relaxed(&a.sc->done)) return;
     extern __shared__ __align__(16) char hsm[];
     const int R = a.hb_rows, nlev = a.hb_nlev;
-    // layout of head_smem_bytes: row ids | z | level table | stages
+    // layout of head_smem_bytes: row ids | z | level-table ring | stages
     int32_t* rows_s = reinterpret_cast<int32_t*>(hsm);
     double* zs = reinterpret_cast<double*>(hsm + ((4 * R + 15) & ~15));
     int4* lv = reinterpret_cast<int4*>(hsm + ((4 * R + 15) & ~15) + ((8 * R + 15) & ~15));
-    char* ring = reinterpret_cast<char*>(lv + nlev + 1);
+    char* ring = reinterpret_cast<char*>(lv + kHeadLvRing);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < R; i += kHeadThreads) rows_s[i] = a.order_b[i];
-    for (int i = tid; i <= nlev; i += kHeadThreads) lv[i] = a.hb_lv[i];
+    // entries 0 .. kHeadLvAhead - 1 now; entry l + kHeadLvAhead rides in the
+    // commit group of level l, so it has landed by level l + 4 (whose issue
+    // reads entries up to l + kHeadLvAhead)
+    for (int i = tid; i < kHeadLvAhead && i <= nlev; i += kHeadThreads) lv[i] = a.hb_lv[i];
     __syncthreads();
     constexpr int NW = kHeadThreads / 32;
     // levels 0 .. kHeadStages - 2 in flight; one commit group per level
@@ -1139,14 +1143,16 @@ __global__ void __launch_bounds__(kHeadThreads, 1) bwd_head_kernel(SolveArgs a) 
         cp_async_wait<kHeadStages - 2>();
         __syncthreads();
         const char* buf = ring + (size_t)(l % kHeadStages) * a.hb_stage;
-        const int4 lo = lv[l];
-        const HeadLevel L = head_level<TV>(lo, lv[l + 1]);
+        const int4 lo = lv[l & (kHeadLvRing - 1)];
+        const HeadLevel L = head_level<TV>(lo, lv[(l + 1) & (kHeadLvRing - 1)]);
         {
             const int lf = l + kHeadStages - 1;
             const int busy = L.ntask < NW ? L.ntask : 0;
             if (lf < nlev && warp >= busy)
                 head_issue<TV>(a, lv, rows_s, lf, ring + (size_t)(lf % kHeadStages) * a.hb_stage, tid - 32 * busy,
                                kHeadThreads - 32 * busy);
+            const int le = l + kHeadLvAhead;
+            if (tid == kHeadThreads - 1 && le <= nlev) cp_async16(lv + (le & (kHeadLvRing - 1)), a.hb_lv + le);
             cp_async_commit();
         }
         const int4* desc = reinterpret_cast<const int4*>(buf);
@@ -1450,7 +1456,7 @@ class PcgSolver {
     cudaError_t launch_bwd(SolveArgs& a) {
         if (a.hb_nlev > 0) {
             void* params[] = {&a};
-            const size_t smem = (size_t)head_smem_bytes(a.hb_rows, a.hb_nlev, a.hb_stage);
+            const size_t smem = (size_t)head_smem_bytes(a.hb_rows, a.hb_stage);
             cudaError_t e = cudaLaunchKernel(k_head, dim3(1), dim3(kHeadThreads), params, smem, stream);
             if (e != cudaSuccess) return e;
         }

@@ -390,13 +390,18 @@ def test_hop_latency_floor():
         ctx.close()
 
 
-@pytest.mark.parametrize("precision", [R.PREC_FP64, R.PREC_FP32_FACTOR])
-def test_backward_head_matches_persistent_kernel(precision):
+@pytest.mark.parametrize("precision,graph", [(R.PREC_FP64, "grid"), (R.PREC_FP32_FACTOR, "grid"),
+                                             (R.PREC_FP32_FACTOR, "power_law")])
+def test_backward_head_matches_persistent_kernel(precision, graph):
     """The first backward levels solved by the one-CTA head kernel: the
-    factor of a 3-D grid gets a head, and PCG with it reaches the same
-    iterate as with the head switched off (same z bit for bit; only the
-    grouping of the r.z sum differs) and the oracle's iteration count."""
-    n, r, c, v, g = grid_laplacian((20, 22, 24), seed=45, excess_frac=0.05, wlo=1e-2, whi=1e2)
+    factor of a 3-D grid (a few dozen narrow levels) and of a power-law
+    graph (hundreds) gets a head, and PCG with it reaches the same iterate
+    as with the head switched off (same z bit for bit; only the grouping of
+    the r.z sum differs)."""
+    if graph == "grid":
+        n, r, c, v, g = grid_laplacian((20, 22, 24), seed=45, excess_frac=0.05, wlo=1e-2, whi=1e2)
+    else:
+        n, r, c, v, g = R.generate("chunglu", [60000, 600000, 2, 6000], wlo=1.0, whi=10.0, seed=11)
     out = {}
     for head in (1, 0):
         ctx = R.Context(seed=4, precision=precision, tol=1e-8, bwd_head=head)
