@@ -83,6 +83,11 @@ struct DevCsc {
     int64_t cap = 0;            // entries allocated in rowind / val (trim_matrix output)
 };
 
+// Rows longer than kLongRow entries (the hubs of power-law graphs) are left
+// out of the one-RHS SpMV kernels' tiles and slices: each gets a CTA of its
+// own (spmv_long_kernel).
+constexpr int kLongRow = 2048;
+
 // Sliced-ELL copy of a DevCsc for the one-RHS SpMV (sell.cu): slice s of
 // 32 rows owns slots [sptr[s] * 32, sptr[s + 1] * 32), column-major (slot
 // (sptr[s] + k) * 32 + lane = entry k of row 32 s + lane; index -1 past the

@@ -7,8 +7,8 @@
 // with one coalesced load per array and no row-pointer round trip, and each
 // lane adds its own row's products in CSR entry order.
 //
-// The copy is only made when the padding is small (stencil operators);
-// matrices with a few long rows among short ones keep the CSR SpMV.
+// Rows longer than kLongRow get no slots (each has a CTA of its own in the
+// solver).  The copy is only made when the padding is small.
 #include <cstdint>
 
 #include "device_common.cuh"
@@ -27,7 +27,8 @@ __global__ void __launch_bounds__(kSellBlock) sell_width_kernel(const int32_t* _
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nslices; s += nw) {
         const int64_t i = s * 32 + lane;
-        const int len = i < n ? ptr[i + 1] - ptr[i] : 0;
+        int len = i < n ? ptr[i + 1] - ptr[i] : 0;
+        if (len > kLongRow) len = 0;  // done by spmv_long_kernel
         const int w = __reduce_max_sync(kFull, len);
         if (lane == 0) width[s] = w;
     }
@@ -43,7 +44,8 @@ __global__ void __launch_bounds__(kSellBlock) sell_fill_kernel(const int32_t* __
     for (int64_t s = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nslices; s += nw) {
         const int64_t i = s * 32 + lane;
         const int ps = i < n ? ptr[i] : 0;
-        const int len = i < n ? ptr[i + 1] - ps : 0;
+        int len = i < n ? ptr[i + 1] - ps : 0;
+        if (len > kLongRow) len = 0;  // done by spmv_long_kernel
         const int64_t base = sptr[s], w = sptr[s + 1] - base;
         for (int64_t k = 0; k < w; ++k) {
             const int64_t slot = (base + k) * 32 + lane;

@@ -128,6 +128,11 @@ struct SolveArgs {
     int reduce;              // compute reductions / scalars
     int poll_ns;             // back-off between polls of a pending value
     unsigned long long timeout_ns;
+    // one-RHS CSR SpMV: rows longer than kLongRow entries (ascending), each
+    // done by a CTA of spmv_long_kernel; their p.q terms in lr_dot[k]
+    const int32_t* __restrict__ lrows;
+    double* lr_dot;
+    int32_t n_lrows;
     // batched systems: row -> system, per-(system, column) step lengths
     const int32_t* __restrict__ seg;
     const double* __restrict__ seg_alpha;
@@ -459,6 +464,46 @@ __global__ void __launch_bounds__(kBlock) spmv_update_kernel(SolveArgs a) {
 #endif
 constexpr int kSpmvChunk = RCHOL_SPMV_CHUNK;  // entries staged per warp and chunk
 
+// Rows longer than kLongRow entries (the hubs of power-law graphs): one
+// CTA per row, each thread adding every kBlock-th product of the row in
+// entry order, then the threads' sums in a fixed tree; the same q, p, y and
+// p.q term as the tile and sliced-ELL kernels, which skip these rows.
+
+// pq += the long rows' p.q terms (spmv_long_kernel ran first): each thread
+// every kBlock-th term in order, then the threads in a fixed tree.  Called
+// by every thread of the SpMV's last block.
+__device__ void add_long_row_terms(SolveArgs& a) {
+    if (a.n_lrows == 0) return;
+    double lt[1] = {0.0};
+    for (int k = threadIdx.x; k < a.n_lrows; k += blockDim.x) lt[0] += a.lr_dot[k];
+    block_partials<1>(lt, a.lr_dot + a.n_lrows);
+    if (threadIdx.x == 0) a.sc->pq[0] += a.lr_dot[a.n_lrows];
+}
+
+__global__ void __launch_bounds__(kBlock) spmv_long_kernel(SolveArgs a) {
+    if (ld_relaxed(&a.sc->done)) return;
+    __shared__ double red[kBlock / 32];
+    const int32_t i = a.lrows[blockIdx.x];
+    const int s = a.a_ptr[i], e = a.a_ptr[i + 1];
+    double sum = 0.0;
+    for (int p = s + (int)threadIdx.x; p < e; p += kBlock) sum += __dmul_rn(a.a_val[p], a.z[a.a_idx[p]]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kBlock / 32; ++w) t += red[w];
+        const double beta = a.sc->beta[0];
+        const double qi = t + beta * a.q[i];
+        const double pi = a.z[i] + beta * a.p[i];
+        a.q[i] = qi;
+        a.p[i] = pi;
+        a.y[i] = pending_value();
+        a.lr_dot[blockIdx.x] = pi * qi;
+    }
+}
+
 __global__ void __launch_bounds__(kBlock) spmv_update_tile_kernel(SolveArgs a) {
     if (ld_relaxed(&a.sc->done)) return;
     __shared__ double stage_all[kBlock / 32][kSpmvChunk];
@@ -479,6 +524,21 @@ __global__ void __launch_bounds__(kBlock) spmv_update_tile_kernel(SolveArgs a) {
         const int nb = __shfl_down_sync(kFull, ps, 1);
         const int pe = lane + 1 < rows ? nb : tile_end;
         const int tile_begin = __shfl_sync(kFull, ps, 0);
+        if (a.n_lrows > 0 && __any_sync(kFull, row && pe - ps > kLongRow)) {
+            // a tile holding a long row: the long rows are spmv_long_kernel's,
+            // every other row is added by its own lane in entry order
+            if (row && pe - ps <= kLongRow) {
+                double sum = 0.0;
+                for (int p = ps; p < pe; ++p) sum += __dmul_rn(a.a_val[p], a.z[a.a_idx[p]]);
+                const double qi = sum + beta * a.q[i];
+                const double pi = a.z[i] + beta * a.p[i];
+                a.q[i] = qi;
+                a.p[i] = pi;
+                a.y[i] = pending_value();
+                acc += pi * qi;
+            }
+            continue;
+        }
         // row vectors in flight while the products are formed
         double qo = 0.0, po = 0.0, zi = 0.0;
         if (row) {
@@ -525,6 +585,7 @@ __global__ void __launch_bounds__(kBlock) spmv_update_tile_kernel(SolveArgs a) {
     block_partials_lane<1>(acc, a.part + (size_t)blockIdx.x);
     if (last_block(&a.sc->ticket[1])) {
         sum_partials<1>(a.part, gridDim.x, a.sc->pq);
+        add_long_row_terms(a);
         if (threadIdx.x == 0) {
             const double pq = a.sc->pq[0];
             a.sc->alpha[0] = (a.sc->active[0] && pq != 0.0) ? a.sc->rz[0] / pq : 0.0;
@@ -590,7 +651,9 @@ __global__ void __launch_bounds__(kBlock) spmv_update_sell_kernel(SolveArgs a) {
             for (int k = 0; k < kSellCols; ++k)
                 if (idx[k] >= 0) sum = __dadd_rn(sum, __dmul_rn(val[k], zv[k]));
         }
-        if (row) {
+        // long rows hold no slots here: spmv_long_kernel did them
+        const bool mine = row && (a.n_lrows == 0 || a.a_ptr[i + 1] - a.a_ptr[i] <= kLongRow);
+        if (mine) {
             const double qi = sum + beta * qo;
             const double pi = zi + beta * po;
             a.q[i] = qi;
@@ -604,6 +667,7 @@ __global__ void __launch_bounds__(kBlock) spmv_update_sell_kernel(SolveArgs a) {
     block_partials_lane<1>(acc, a.part + (size_t)blockIdx.x);
     if (last_block(&a.sc->ticket[1])) {
         sum_partials<1>(a.part, gridDim.x, a.sc->pq);
+        add_long_row_terms(a);
         if (threadIdx.x == 0) {
             const double pq = a.sc->pq[0];
             a.sc->alpha[0] = (a.sc->active[0] && pq != 0.0) ? a.sc->rz[0] / pq : 0.0;
@@ -1329,6 +1393,19 @@ cudaError_t launch_coresident(const void* fn, int grid, Arg& a, cudaStream_t s) 
     return launch_coresident(fn, grid, params, s);
 }
 
+__global__ void long_flag_kernel(int32_t n, const int32_t* __restrict__ ptr, int32_t* flag) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        flag[i] = ptr[i + 1] - ptr[i] > kLongRow ? 1 : 0;
+}
+
+__global__ void long_scatter_kernel(int32_t n, const int32_t* __restrict__ flag, const int32_t* __restrict__ pos,
+                                    int32_t* rows) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        if (flag[i]) rows[pos[i]] = (int32_t)i;
+}
+
 // The factor arrays of the k > 1 solves: the multi-RHS layouts when built,
 // else L's own rows and columns by row id.
 void set_factor_rows(SolveArgs& a, const DevFactor& F, bool fp32) {
@@ -1383,8 +1460,56 @@ class PcgSolver {
     void *k_init = nullptr, *k_spmv = nullptr, *k_fwd = nullptr, *k_bwd = nullptr, *k_true = nullptr,
          *k_restart = nullptr;
     void* k_head = nullptr;  // backward head (K = 1)
+    // long rows of the one-RHS CSR SpMV (spmv_long_kernel)
+    int32_t* lrows = nullptr;
+    double* lr_dot = nullptr;
+    int32_t n_lrows = 0;
+    int64_t cap_lrows = 0;
 
     bool use_head() const { return k_head && F.hb_nlev > 0; }
+
+    // The rows of A longer than kLongRow, ascending (the one-RHS SpMV gives
+    // each its own CTA; the sliced-ELL copy leaves them out); none for k > 1.
+    cudaError_t find_long_rows() {
+        n_lrows = 0;
+        if (K != 1 || A.n == 0) return cudaSuccess;
+        const int32_t n = A.n;
+        int32_t *flag = nullptr, *pos = nullptr;
+        void* tmp = nullptr;
+        cudaError_t e = cudaMalloc(&flag, sizeof(int32_t) * (size_t)n);
+        if (e == cudaSuccess) e = cudaMalloc(&pos, sizeof(int32_t) * ((size_t)n + 1));
+        if (e == cudaSuccess) e = cudaMalloc(&tmp, scan_tmp_bytes(n));
+        if (e == cudaSuccess) {
+            long_flag_kernel<<<grid_for(n, kBlock), kBlock, 0, stream>>>(n, A.colptr, flag);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = exclusive_scan_i32_to_i32(flag, pos, n, tmp, stream);
+        int32_t cnt = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&cnt, pos + n, sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e == cudaSuccess && cnt > 0) {
+            if (cap_lrows < cnt) {
+                cudaFree(lrows);
+                cudaFree(lr_dot);
+                lrows = nullptr;
+                lr_dot = nullptr;
+                cap_lrows = 0;
+                e = cudaMalloc(&lrows, sizeof(int32_t) * (size_t)cnt);
+                if (e == cudaSuccess) e = cudaMalloc(&lr_dot, sizeof(double) * ((size_t)cnt + 1));
+                if (e == cudaSuccess) cap_lrows = cnt;
+            }
+            if (e == cudaSuccess) {
+                long_scatter_kernel<<<grid_for(n, kBlock), kBlock, 0, stream>>>(n, flag, pos, lrows);
+                e = cudaGetLastError();
+            }
+            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+            if (e == cudaSuccess) n_lrows = cnt;
+        }
+        cudaFree(flag);
+        cudaFree(pos);
+        cudaFree(tmp);
+        return e;
+    }
 
     SolveArgs args(const double* b, double* x) const {
         SolveArgs a;
@@ -1416,6 +1541,9 @@ class PcgSolver {
         a.pcount_b = F.pcount_b;
         a.srow_b = F.srow_b;
         a.nsplit_b = F.nsplit_b;
+        a.lrows = lrows;
+        a.lr_dot = lr_dot;
+        a.n_lrows = n_lrows;
         if (use_head()) {
             a.hb_lv = F.hb_lv;
             a.hb_idx = F.hb_idx;
@@ -1463,10 +1591,20 @@ class PcgSolver {
         return launch(k_bwd, grid_bwd, a);
     }
 
+    // q = A z + beta q, p = z + beta p, p.q (the long rows' CTAs first)
+    cudaError_t launch_spmv(SolveArgs& a) {
+        if (a.n_lrows > 0) {
+            void* params[] = {&a};
+            cudaError_t e = cudaLaunchKernel((void*)spmv_long_kernel, dim3(a.n_lrows), dim3(kBlock), params, 0, stream);
+            if (e != cudaSuccess) return e;
+        }
+        return launch(k_spmv, grid_spmv, a);
+    }
+
     cudaError_t launch_iteration(const double* b, double* x) {
         SolveArgs a = args(b, x);
         cudaError_t e;
-        if ((e = launch(k_spmv, grid_spmv, a)) != cudaSuccess) return e;
+        if ((e = launch_spmv(a)) != cudaSuccess) return e;
         if ((e = launch(k_fwd, grid_fwd, a)) != cudaSuccess) return e;
         return launch_bwd(a);
     }
@@ -1556,6 +1694,7 @@ PcgSolver* pcg_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cf
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev1);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev2);
+    if (e == cudaSuccess) e = s->find_long_rows();
     if (e != cudaSuccess || s->grid_fwd <= 0 || s->grid_bwd <= 0) {
         *err = e != cudaSuccess ? e : cudaErrorLaunchOutOfResources;
         pcg_destroy(s);
@@ -1572,7 +1711,7 @@ cudaError_t pcg_rebind(PcgSolver* s, const DevCsc& A, const DevSell* sell, const
     s->A = A;
     s->S = want_sell ? *sell : DevSell();
     s->F = F;
-    return cudaSuccess;
+    return s->find_long_rows();
 }
 
 void pcg_destroy(PcgSolver* s) {
@@ -1586,6 +1725,8 @@ void pcg_destroy(PcgSolver* s) {
     cudaFree(s->part);
     cudaFree(s->sc);
     cudaFree(s->react);
+    cudaFree(s->lrows);
+    cudaFree(s->lr_dot);
     if (s->sc_host) cudaFreeHost(s->sc_host);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
@@ -1636,7 +1777,7 @@ cudaError_t pcg_solve(PcgSolver* s, const double* dB, double* dX, SolveResult* r
     if ((e = s->launch(s->k_init, s->grid_vec, a)) != cudaSuccess) return e;
     if ((e = s->launch_start(dB, dX)) != cudaSuccess) return e;
     // per iteration: SpMV, forward, backward (+ the backward head)
-    const int per_it = s->use_head() ? 4 : 3;
+    const int per_it = 3 + (s->use_head() ? 1 : 0) + (s->n_lrows > 0 ? 1 : 0);
     res->kernel_launches += per_it;
     if ((e = cudaEventRecord(s->ev1, s->stream)) != cudaSuccess) return e;
     int restarts = 0;
@@ -1743,7 +1884,7 @@ cudaError_t pcg_profile(PcgSolver* s, const double* dB, double* dX, int reps, fl
     for (int r = 0; r < reps && e == cudaSuccess; ++r) {
         SolveArgs it = s->args(dB, dX);
         cudaEventRecord(ev[0], s->stream);
-        e = s->launch(s->k_spmv, s->grid_spmv, it);
+        e = s->launch_spmv(it);
         cudaEventRecord(ev[1], s->stream);
         if (e == cudaSuccess) e = s->launch(s->k_fwd, s->grid_fwd, it);
         cudaEventRecord(ev[2], s->stream);
@@ -2039,6 +2180,9 @@ class BatchSolver {
         a.hb_lv = nullptr;
         a.hb_idx = nullptr;
         a.hb_nlev = a.hb_ntask = a.hb_rows = a.hb_stage = 0;
+        a.lrows = nullptr;
+        a.lr_dot = nullptr;
+        a.n_lrows = 0;
         a.reduce = 0;
         a.update = 1;
         a.seg = seg;
