@@ -420,6 +420,35 @@ __global__ void __launch_bounds__(kBlock) init_kernel(SolveArgs a) {
 // ---------------------------------------------------------------------------
 // spmv_update: s = A z; q = s + beta q; p = z + beta p; (p.q); y = pending
 // ---------------------------------------------------------------------------
+// K right-hand sides of the long rows (spmv_long_kernel's multi-RHS form):
+// one CTA per row; thread t adds column t % K over every (kBlock / K)-th
+// entry from t / K in entry order, then column c's kBlock / K partial sums
+// are added in group order.  Terms of column c in lr_dot[k * K + c].
+template <int K>
+__global__ void __launch_bounds__(kBlock) spmv_long_k_kernel(SolveArgs a) {
+    if (ld_relaxed(&a.sc->done)) return;
+    constexpr int NG = kBlock / K;
+    __shared__ double red[NG][K];
+    const int32_t i = a.lrows[blockIdx.x];
+    const int s = a.a_ptr[i], e = a.a_ptr[i + 1];
+    const int c = threadIdx.x % K, g = threadIdx.x / K;
+    double sum = 0.0;
+    for (int p = s + g; p < e; p += NG) sum += __dmul_rn(a.a_val[p], a.z[(size_t)a.a_idx[p] * K + c]);
+    red[g][c] = sum;
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double t = 0.0;
+        for (int q = 0; q < NG; ++q) t += red[q][c];
+        const size_t o = (size_t)i * K + c;
+        const double qi = t + a.sc->beta[c] * a.q[o];
+        const double pi = a.z[o] + a.sc->beta[c] * a.p[o];
+        a.q[o] = qi;
+        a.p[o] = pi;
+        a.y[o] = pending_value();
+        a.lr_dot[(size_t)blockIdx.x * K + c] = pi * qi;
+    }
+}
+
 template <int K>
 __global__ void __launch_bounds__(kBlock) spmv_update_kernel(SolveArgs a) {
     if (ld_relaxed(&a.sc->done)) return;
@@ -433,6 +462,7 @@ __global__ void __launch_bounds__(kBlock) spmv_update_kernel(SolveArgs a) {
     double acc = 0.0;
     for (int64_t i = group; i < a.n; i += ngroups) {
         const int s = a.a_ptr[i], e = a.a_ptr[i + 1];
+        if (a.n_lrows > 0 && e - s > kLongRow) continue;  // spmv_long_k_kernel's
         const double sum = row_dot_plain<K>(a.a_idx, a.a_val, s, e, a.z, c);
         const size_t o = (size_t)i * K + c;
         const double qi = sum + beta * a.q[o];
@@ -445,6 +475,12 @@ __global__ void __launch_bounds__(kBlock) spmv_update_kernel(SolveArgs a) {
     block_partials_lane<K>(acc, a.part + (size_t)blockIdx.x * K);
     if (last_block(&a.sc->ticket[1])) {
         sum_partials<K>(a.part, gridDim.x, a.sc->pq);
+        if (threadIdx.x < K && a.n_lrows > 0) {
+            // the long rows' terms of column c, in row order
+            double t = 0.0;
+            for (int k = 0; k < a.n_lrows; ++k) t += a.lr_dot[(size_t)k * K + threadIdx.x];
+            a.sc->pq[threadIdx.x] += t;
+        }
         if (threadIdx.x < K) {
             int c = threadIdx.x;
             double pq = a.sc->pq[c];
@@ -1460,6 +1496,7 @@ class PcgSolver {
     void *k_init = nullptr, *k_spmv = nullptr, *k_fwd = nullptr, *k_bwd = nullptr, *k_true = nullptr,
          *k_restart = nullptr;
     void* k_head = nullptr;  // backward head (K = 1)
+    void* k_long = nullptr;  // long rows of the SpMV
     // long rows of the one-RHS CSR SpMV (spmv_long_kernel)
     int32_t* lrows = nullptr;
     double* lr_dot = nullptr;
@@ -1468,11 +1505,11 @@ class PcgSolver {
 
     bool use_head() const { return k_head && F.hb_nlev > 0; }
 
-    // The rows of A longer than kLongRow, ascending (the one-RHS SpMV gives
-    // each its own CTA; the sliced-ELL copy leaves them out); none for k > 1.
+    // The rows of A longer than kLongRow, ascending: the SpMV gives each its
+    // own CTA (the sliced-ELL copy leaves them out).
     cudaError_t find_long_rows() {
         n_lrows = 0;
-        if (K != 1 || A.n == 0) return cudaSuccess;
+        if (A.n == 0) return cudaSuccess;
         const int32_t n = A.n;
         int32_t *flag = nullptr, *pos = nullptr;
         void* tmp = nullptr;
@@ -1495,7 +1532,7 @@ class PcgSolver {
                 lr_dot = nullptr;
                 cap_lrows = 0;
                 e = cudaMalloc(&lrows, sizeof(int32_t) * (size_t)cnt);
-                if (e == cudaSuccess) e = cudaMalloc(&lr_dot, sizeof(double) * ((size_t)cnt + 1));
+                if (e == cudaSuccess) e = cudaMalloc(&lr_dot, sizeof(double) * ((size_t)cnt * K + 1));
                 if (e == cudaSuccess) cap_lrows = cnt;
             }
             if (e == cudaSuccess) {
@@ -1595,7 +1632,7 @@ class PcgSolver {
     cudaError_t launch_spmv(SolveArgs& a) {
         if (a.n_lrows > 0) {
             void* params[] = {&a};
-            cudaError_t e = cudaLaunchKernel((void*)spmv_long_kernel, dim3(a.n_lrows), dim3(kBlock), params, 0, stream);
+            cudaError_t e = cudaLaunchKernel(k_long, dim3(a.n_lrows), dim3(kBlock), params, 0, stream);
             if (e != cudaSuccess) return e;
         }
         return launch(k_spmv, grid_spmv, a);
@@ -1630,6 +1667,7 @@ static void bind_kernels(PcgSolver* s) {
     s->k_true = (void*)true_residual_kernel<K>;
     s->k_restart = (void*)restart_kernel<K>;
     s->k_head = K == 1 ? (void*)bwd_head_kernel<TV> : nullptr;
+    s->k_long = K == 1 ? (void*)spmv_long_kernel : (void*)spmv_long_k_kernel<K>;
 }
 
 template <typename TV>
