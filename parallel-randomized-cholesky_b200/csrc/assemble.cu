@@ -295,8 +295,6 @@ __global__ void mask_mul_kernel(const int32_t* __restrict__ a, const int32_t* __
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) out[t] = mask[t] ? a[t] : 0;
 }
 
-// Parts of each scheduled task: 1, or ceil(len / kSplitLen) for a one-row
-// task of the widest class whose row is longer than kSplitMin.
 // Entries of the row at schedule position p: ptr[order[p]] .. ptr[order[p] + 1].
 __device__ __forceinline__ int64_t pos_len(const int32_t* __restrict__ order, const int64_t* __restrict__ ptr,
                                            int64_t p) {
@@ -304,14 +302,17 @@ __device__ __forceinline__ int64_t pos_len(const int32_t* __restrict__ order, co
     return ptr[i + 1] - ptr[i];
 }
 
+// Parts of each scheduled task: 1, or ceil(len / split_len) for a one-row
+// task of the widest class whose row is longer than split_min.
 __global__ void pack_nsub_kernel(const int2* __restrict__ tasks, int32_t ntasks, const int32_t* __restrict__ order,
-                                 const int64_t* __restrict__ ptr, int32_t* nsub, int32_t* issplit) {
+                                 const int64_t* __restrict__ ptr, int split_min, int split_len, int32_t* nsub,
+                                 int32_t* issplit) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntasks; t += stride) {
         const int2 d = tasks[t];
         const int cls = d.y >> 8, cnt = d.y & 0xff;
         const int64_t len = cnt == 1 ? pos_len(order, ptr, d.x) : 0;
-        const int np = (cls == kLaneClasses - 1 && len > kSplitMin) ? (int)((len + kSplitLen - 1) / kSplitLen) : 1;
+        const int np = (cls == kLaneClasses - 1 && len > split_min) ? (int)((len + split_len - 1) / split_len) : 1;
         nsub[t] = np;
         issplit[t] = np > 1 ? 1 : 0;
     }
@@ -320,7 +321,7 @@ __global__ void pack_nsub_kernel(const int2* __restrict__ tasks, int32_t ntasks,
 // Expanded tasks {position, d.z bits, part count, part length or 0} and the
 // split bookkeeping of part tasks.
 __global__ void pack_expand_kernel(const int2* __restrict__ tasks, int32_t ntasks, const int64_t* __restrict__ ptr,
-                                   const int32_t* __restrict__ order, const int32_t* __restrict__ nsub,
+                                   const int32_t* __restrict__ order, int split_len, const int32_t* __restrict__ nsub,
                                    const int32_t* __restrict__ tbase, const int32_t* __restrict__ sid,
                                    const int32_t* __restrict__ pbase, int4* etask, int2* split, int32_t* srow) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -334,7 +335,7 @@ __global__ void pack_expand_kernel(const int2* __restrict__ tasks, int32_t ntask
         const int64_t len = pos_len(order, ptr, d.x);
         srow[sid[t]] = order[d.x];
         for (int q = 0; q < np; ++q) {
-            const int plen = (int)min((int64_t)kSplitLen, len - (int64_t)q * kSplitLen);
+            const int plen = (int)min((int64_t)split_len, len - (int64_t)q * split_len);
             etask[tbase[t] + q] = make_int4(d.x, d.y | (1 << 11) | (q << 12), np, plen);
             split[tbase[t] + q] = make_int2(sid[t], pbase[t]);
         }
@@ -370,7 +371,7 @@ __global__ void pack_desc_kernel(const int4* __restrict__ etask, int32_t ntasks,
 // dependency scheduled last (largest sign * level; the first such entry on
 // ties): the solve polls it alone before reading the rest of the row.
 __global__ void pack_fill_kernel(const int4* __restrict__ pack, int32_t ntasks, const int32_t* __restrict__ order,
-                                 const int64_t* __restrict__ ptr, const int32_t* __restrict__ sidx,
+                                 const int64_t* __restrict__ ptr, int split_len, const int32_t* __restrict__ sidx,
                                  const double* __restrict__ sval,
                                  const float* __restrict__ sval32, const int32_t* __restrict__ level, int sign,
                                  int32_t* pidx, double* pval, float* pval32) {
@@ -387,9 +388,9 @@ __global__ void pack_fill_kernel(const int4* __restrict__ pack, int32_t ntasks, 
             s = ptr[i];
             len = ptr[i + 1] - s;
             if ((d.z >> 11) & 1) {  // part task: its window of the row
-                const int64_t q0 = (int64_t)(d.z >> 12) * kSplitLen;
+                const int64_t q0 = (int64_t)(d.z >> 12) * split_len;
                 s += q0;
-                len = min((int64_t)kSplitLen, len - q0);
+                len = min((int64_t)split_len, len - q0);
             }
         }
         // gate of the row: best (key, entry) over the lane's entries, then over the G lanes
@@ -802,11 +803,11 @@ struct PackOut {
 };
 
 // Task slabs of one direction from its task list and row order over L's
-// rows (ptr, sidx, sval by row id); rows longer than kSplitMin are split
+// rows (ptr, sidx, sval by row id); rows longer than split_min are split
 // into part tasks first.
 static cudaError_t build_pack(int32_t ntasks, const int2* tasks, const int32_t* order, const int64_t* ptr,
                               const int32_t* sidx, const double* sval, const float* sval32, const int32_t* level,
-                              int sign, const PackOut& o, Scratch& sc, cudaStream_t s) {
+                              int sign, int split_min, int split_len, const PackOut& o, Scratch& sc, cudaStream_t s) {
     const int64_t nt = std::max<int32_t>(ntasks, 1);
     int32_t *nsub = nullptr, *issplit = nullptr, *tbase = nullptr, *sid = nullptr, *pbase = nullptr;
     void* tmp = nullptr;
@@ -823,7 +824,8 @@ static cudaError_t build_pack(int32_t ntasks, const int2* tasks, const int32_t* 
         RCHOL_TRY(ensure(o.pack, *o.cap_d, 1));
         return cudaSuccess;
     }
-    pack_nsub_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(tasks, ntasks, order, ptr, nsub, issplit);
+    pack_nsub_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(tasks, ntasks, order, ptr, split_min, split_len, nsub,
+                                                           issplit);
     RCHOL_TRY(exclusive_scan_i32_to_i32(nsub, tbase, ntasks, tmp, s));
     RCHOL_TRY(exclusive_scan_i32_to_i32(issplit, sid, ntasks, tmp, s));
     int32_t hs[2] = {0, 0};
@@ -855,8 +857,8 @@ static cudaError_t build_pack(int32_t ntasks, const int2* tasks, const int32_t* 
     RCHOL_TRY(ensure(o.pcount, *o.cap_c, std::max<int64_t>(nsp, 1)));
     RCHOL_TRY(ensure(o.srow, *o.cap_r, std::max<int64_t>(nsp, 1)));
     RCHOL_TRY(cudaMemsetAsync(*o.pcount, 0, sizeof(int32_t) * (size_t)std::max<int32_t>(nsp, 1), s));
-    pack_expand_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(tasks, ntasks, ptr, order, nsub, tbase, sid, pbase, etask,
-                                                             *o.split, *o.srow);
+    pack_expand_kernel<<<grid_for(ntasks, 256), 256, 0, s>>>(tasks, ntasks, ptr, order, split_len, nsub, tbase, sid,
+                                                             pbase, etask, *o.split, *o.srow);
     pack_m_kernel<<<grid_for(ne, 256), 256, 0, s>>>(etask, ne, order, ptr, m);
     RCHOL_TRY(exclusive_scan_i32_to_i64(m, base, ne, tmp2, s));
     int64_t units = 0;
@@ -878,7 +880,8 @@ static cudaError_t build_pack(int32_t ntasks, const int2* tasks, const int32_t* 
     }
     pack_desc_kernel<<<grid_for(ne, 256), 256, 0, s>>>(etask, ne, m, base, *o.pack);
     pack_fill_kernel<<<grid_for((int64_t)ne * 32, 256), 256, 0, s>>>(
-        *o.pack, ne, order, ptr, sidx, sval, sval32, level, sign, *o.pidx, *o.pval, sval32 ? *o.pval32 : nullptr);
+        *o.pack, ne, order, ptr, split_len, sidx, sval, sval32, level, sign, *o.pidx, *o.pval,
+        sval32 ? *o.pval32 : nullptr);
     return cudaGetLastError();
 }
 
@@ -893,10 +896,10 @@ static cudaError_t build_packs(DevFactor& f, const int32_t* level_f, const int32
     const PackOut ob{&f.pack_b, &f.cap_pdb, &f.pb_idx, &f.cap_pib, &f.pb_val, &f.cap_pvb, &f.pb_val32, &f.cap_pwb,
                      &f.slots_b, &f.npt_b, &f.nsplit_b, &f.split_b, &f.cap_sb, &f.psum_b, &f.cap_qb, &f.pcount_b,
                      &f.cap_cb, &f.srow_b, &f.cap_rb};
-    RCHOL_TRY(build_pack(f.ntasks_f, f.tasks_f, f.order_f, f.lr_ptr, f.lr_idx, f.lr_val, f.lr_val32, level_f, 1, of,
-                         sc, s));
+    RCHOL_TRY(build_pack(f.ntasks_f, f.tasks_f, f.order_f, f.lr_ptr, f.lr_idx, f.lr_val, f.lr_val32, level_f, 1,
+                         kSplitMinF, kSplitLenF, of, sc, s));
     RCHOL_TRY(build_pack(f.ntasks_b, f.tasks_b, f.order_b, f.lc_ptr, f.lc_idx, f.lc_val, f.lc_val32, level_b, sign_b,
-                         ob, sc, s));
+                         kSplitMinB, kSplitLenB, ob, sc, s));
     return cudaSuccess;
 }
 

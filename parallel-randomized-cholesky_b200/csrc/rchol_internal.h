@@ -206,7 +206,7 @@ struct DevFactor {
     double* pb_val = nullptr;
     float* pb_val32 = nullptr;
     int64_t slots_f = 0, slots_b = 0;
-    // Rows longer than kSplitMin entries run as several part tasks (flag
+    // Rows longer than kSplitMin* entries run as several part tasks (flag
     // 1 << 11 in d.z, part index in d.z >> 12, part count in d.w >> 8); part
     // tasks carry {split row id, first partial} in split_*, write partial
     // sums to psum_*, and the last part to finish (pcount_*) publishes the row.
@@ -240,10 +240,19 @@ struct DevFactor {
     int64_t cap_n = 0, cap_nnz = 0, cap_tf = 0, cap_tb = 0, cap_ln = 0, cap_lz = 0;
 };
 
-// Rows longer than kSplitMin entries run in the K = 1 solves as part tasks
-// of kSplitLen entries (shorter rows are faster in one warp).
-constexpr int kSplitMin = 1024;
-constexpr int kSplitLen = 512;
+// Rows longer than kSplitMin* entries run in the K = 1 solves as part tasks
+// of kSplitLen* entries (shorter rows are faster in one warp); F for the
+// forward solve (rows of L), B for the backward one (columns of L).
+#ifndef RCHOL_SPLIT_MIN_B
+#define RCHOL_SPLIT_MIN_B 1024
+#endif
+#ifndef RCHOL_SPLIT_LEN_B
+#define RCHOL_SPLIT_LEN_B 512
+#endif
+constexpr int kSplitMinF = 1024;
+constexpr int kSplitLenF = 512;
+constexpr int kSplitMinB = RCHOL_SPLIT_MIN_B;
+constexpr int kSplitLenB = RCHOL_SPLIT_LEN_B;
 
 // Lane classes of the K = 1 solves: a row gets G = 1, 2, 4, ..., 32 lanes,
 // the smallest G that leaves at most `epl` entries per lane (rows longer
