@@ -244,10 +244,10 @@ struct DevFactor {
 // of kSplitLen* entries (shorter rows are faster in one warp); F for the
 // forward solve (rows of L), B for the backward one (columns of L).
 #ifndef RCHOL_SPLIT_MIN_B
-#define RCHOL_SPLIT_MIN_B 1024
+#define RCHOL_SPLIT_MIN_B 512
 #endif
 #ifndef RCHOL_SPLIT_LEN_B
-#define RCHOL_SPLIT_LEN_B 512
+#define RCHOL_SPLIT_LEN_B 128
 #endif
 constexpr int kSplitMinF = 1024;
 constexpr int kSplitLenF = 512;
