@@ -40,6 +40,7 @@ struct rchol_ctx {
     // solver cache
     rchol::PcgSolver* solver = nullptr;
     const rchol_factor_t* solver_f = nullptr;
+    bool matrix_new = true;  // the solve matrix changed since the solver saw it
     int solver_k = 0, solver_fp32 = -1, solver_stop = -1, solver_maxit = -1, solver_poll = -1;
     double solver_tol = -1;
     // batched systems (block-diagonal stacking)
@@ -410,6 +411,7 @@ extern "C" rchol_status rchol_set_csc(rchol_ctx* ctx, int n, const int* colptr, 
     // buffers for a matrix of the same shape (refilled below / on first use)
     ctx->sell_tried = false;
     ctx->solver_f = nullptr;
+    ctx->matrix_new = true;
     ctx->batch_off.clear();
     if (ctx->bsolver) drop_solver(ctx);
     DevCsc A;
@@ -1073,7 +1075,8 @@ rchol_status get_solver(rchol_ctx* ctx, const rchol_factor_t* f, int k) {
         if (ctx->solver_f == f) return RCHOL_OK;
         // another factor, or a new matrix of the same shape: keep the
         // solver's vectors and graph
-        if (rchol::pcg_rebind(ctx->solver, ctx->At, sell, f->F) == cudaSuccess) {
+        if (rchol::pcg_rebind(ctx->solver, ctx->At, sell, f->F, ctx->matrix_new) == cudaSuccess) {
+            ctx->matrix_new = false;
             ctx->solver_f = f;
             return RCHOL_OK;
         }
@@ -1094,6 +1097,7 @@ rchol_status get_solver(rchol_ctx* ctx, const rchol_factor_t* f, int k) {
     cudaError_t e = cudaSuccess;
     ctx->solver = rchol::pcg_create(ctx->At, f->F, cfg, ctx->device, ctx->stream, &e, sell);
     if (!ctx->solver) return cuda_fail(ctx, e, "create solver");
+    ctx->matrix_new = false;
     ctx->solver_f = f;
     ctx->solver_k = k;
     ctx->solver_fp32 = fp32;

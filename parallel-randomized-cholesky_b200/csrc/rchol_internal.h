@@ -441,7 +441,9 @@ PcgSolver* pcg_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cf
 // copy, null for none) and another factor; its vectors, and its captured
 // iteration graph when the launch arguments come out equal, are kept.
 // Fails (cudaErrorInvalidValue) when the sizes or the SpMV form differ.
-cudaError_t pcg_rebind(PcgSolver* s, const DevCsc& A, const DevSell* sell, const DevFactor& F);
+// new_matrix: A's contents changed since the solver last saw it (its long
+// rows are found again)
+cudaError_t pcg_rebind(PcgSolver* s, const DevCsc& A, const DevSell* sell, const DevFactor& F, bool new_matrix);
 cudaError_t pcg_solve(PcgSolver* s, const double* dB, double* dX, SolveResult* res);
 void pcg_destroy(PcgSolver* s);
 // Mean device time of spmv_update / fwd / bwd over `reps` iterations.

@@ -1502,6 +1502,8 @@ class PcgSolver {
     double* lr_dot = nullptr;
     int32_t n_lrows = 0;
     int64_t cap_lrows = 0;
+    int32_t *lflag = nullptr, *lpos = nullptr;  // [n], [n + 1]
+    void* ltmp = nullptr;                       // scan scratch
 
     bool use_head() const { return k_head && F.hb_nlev > 0; }
 
@@ -1511,11 +1513,13 @@ class PcgSolver {
         n_lrows = 0;
         if (A.n == 0) return cudaSuccess;
         const int32_t n = A.n;
-        int32_t *flag = nullptr, *pos = nullptr;
-        void* tmp = nullptr;
-        cudaError_t e = cudaMalloc(&flag, sizeof(int32_t) * (size_t)n);
-        if (e == cudaSuccess) e = cudaMalloc(&pos, sizeof(int32_t) * ((size_t)n + 1));
-        if (e == cudaSuccess) e = cudaMalloc(&tmp, scan_tmp_bytes(n));
+        // the solver's matrix order is fixed, so these are allocated once
+        cudaError_t e = cudaSuccess;
+        if (!lflag) e = cudaMalloc(&lflag, sizeof(int32_t) * (size_t)n);
+        if (e == cudaSuccess && !lpos) e = cudaMalloc(&lpos, sizeof(int32_t) * ((size_t)n + 1));
+        if (e == cudaSuccess && !ltmp) e = cudaMalloc(&ltmp, scan_tmp_bytes(n));
+        int32_t *flag = lflag, *pos = lpos;
+        void* tmp = ltmp;
         if (e == cudaSuccess) {
             long_flag_kernel<<<grid_for(n, kBlock), kBlock, 0, stream>>>(n, A.colptr, flag);
             e = cudaGetLastError();
@@ -1542,9 +1546,6 @@ class PcgSolver {
             if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
             if (e == cudaSuccess) n_lrows = cnt;
         }
-        cudaFree(flag);
-        cudaFree(pos);
-        cudaFree(tmp);
         return e;
     }
 
@@ -1741,7 +1742,7 @@ PcgSolver* pcg_create(const DevCsc& A, const DevFactor& F, const SolveConfig& cf
     return s;
 }
 
-cudaError_t pcg_rebind(PcgSolver* s, const DevCsc& A, const DevSell* sell, const DevFactor& F) {
+cudaError_t pcg_rebind(PcgSolver* s, const DevCsc& A, const DevSell* sell, const DevFactor& F, bool new_matrix) {
     const bool want_sell = s->K == 1 && sell && sell->slots > 0 && sell->n == A.n;
     const bool has_sell = s->k_spmv == (void*)spmv_update_sell_kernel;
     if (A.n != s->A.n || F.n != A.n || want_sell != has_sell || (s->cfg.fp32_factor && !F.lr_val32))
@@ -1749,7 +1750,7 @@ cudaError_t pcg_rebind(PcgSolver* s, const DevCsc& A, const DevSell* sell, const
     s->A = A;
     s->S = want_sell ? *sell : DevSell();
     s->F = F;
-    return s->find_long_rows();
+    return new_matrix ? s->find_long_rows() : cudaSuccess;
 }
 
 void pcg_destroy(PcgSolver* s) {
@@ -1765,6 +1766,9 @@ void pcg_destroy(PcgSolver* s) {
     cudaFree(s->react);
     cudaFree(s->lrows);
     cudaFree(s->lr_dot);
+    cudaFree(s->lflag);
+    cudaFree(s->lpos);
+    cudaFree(s->ltmp);
     if (s->sc_host) cudaFreeHost(s->sc_host);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
