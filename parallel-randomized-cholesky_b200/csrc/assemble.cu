@@ -206,10 +206,19 @@ __device__ __forceinline__ int sched_key(int level, int64_t len, int epl) {
     return kLaneClasses * level + lane_class(len, epl);
 }
 
-// bucket key of every row and the bucket sizes (warp-aggregated counts)
+// Buckets counted in shared memory first when this many fit (32 KB).
+constexpr int kSchedSharedBins = 8192;
+
+// bucket key of every row and the bucket sizes (warp-aggregated counts; with
+// nsh > 0 bins, per block in shared memory and then one add per bin, so the
+// few buckets that hold most rows, the first level's, are not a hot spot)
 __global__ void sched_hist_kernel(const int32_t* __restrict__ level, const int64_t* __restrict__ ptr, int32_t n,
-                                  int32_t depth, int backward, int epl, int32_t* key, int32_t* hist) {
+                                  int32_t depth, int backward, int epl, int32_t* key, int32_t* hist, int nsh) {
+    extern __shared__ int32_t sh_hist[];
     const int lane = threadIdx.x & 31;
+    for (int b = threadIdx.x; b < nsh; b += blockDim.x) sh_hist[b] = 0;
+    if (nsh > 0) __syncthreads();
+    int32_t* h = nsh > 0 ? sh_hist : hist;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t n_up = ((int64_t)n + 31) / 32 * 32;  // whole warps iterate together
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_up; i += stride) {
@@ -220,8 +229,12 @@ __global__ void sched_hist_kernel(const int32_t* __restrict__ level, const int64
             key[i] = k;
         }
         const unsigned peers = __match_any_sync(0xffffffffu, k);
-        if (k >= 0 && (peers & ((1u << lane) - 1u)) == 0) atomicAdd(hist + k, __popc(peers));
+        if (k >= 0 && (peers & ((1u << lane) - 1u)) == 0) atomicAdd(h + k, __popc(peers));
     }
+    if (nsh == 0) return;
+    __syncthreads();
+    for (int b = threadIdx.x; b < nsh; b += blockDim.x)
+        if (sh_hist[b]) atomicAdd(hist + b, sh_hist[b]);
 }
 
 // Longest path from each row to a sink of the L^T solve DAG:
@@ -370,6 +383,9 @@ __global__ void pack_desc_kernel(const int4* __restrict__ etask, int32_t ntasks,
 // except that entry 0 and the row's gate trade places.  The gate is the
 // dependency scheduled last (largest sign * level; the first such entry on
 // ties): the solve polls it alone before reading the rest of the row.
+// entries per lane whose slab indices pack_fill_kernel keeps in registers
+constexpr int kFillRegs = 8;
+
 __global__ void pack_fill_kernel(const int4* __restrict__ pack, int32_t ntasks, const int32_t* __restrict__ order,
                                  const int64_t* __restrict__ ptr, int split_len, const int32_t* __restrict__ sidx,
                                  const double* __restrict__ sval,
@@ -393,9 +409,30 @@ __global__ void pack_fill_kernel(const int4* __restrict__ pack, int32_t ntasks, 
                 len = min((int64_t)split_len, len - q0);
             }
         }
-        // gate of the row: best (key, entry) over the lane's entries, then over the G lanes
+        // gate of the row: best (key, entry) over the lane's entries, then over
+        // the G lanes.  The lane's first kFillRegs entries (slot k holds entry
+        // gl + k * G) have their indices, then their levels, loaded as one
+        // batch each; the indices are kept for the copy below.
+        int32_t ix[kFillRegs];
+#pragma unroll
+        for (int j = 0; j < kFillRegs; ++j) {
+            const int64_t e = ((int64_t)j << cls) + gl;
+            ix[j] = e < len ? sidx[s + e] : 0;
+        }
+        int32_t lv[kFillRegs];
+#pragma unroll
+        for (int j = 0; j < kFillRegs; ++j) lv[j] = (((int64_t)j << cls) + gl) < len ? level[ix[j]] : 0;
         long long best_key = LLONG_MIN, best_e = 0;
-        for (int64_t e = gl; e < len; e += G) {
+#pragma unroll
+        for (int j = 0; j < kFillRegs; ++j) {
+            const int64_t e = ((int64_t)j << cls) + gl;
+            const long long key = (long long)sign * lv[j];
+            if (e < len && key > best_key) {
+                best_key = key;
+                best_e = e;
+            }
+        }
+        for (int64_t e = ((int64_t)kFillRegs << cls) + gl; e < len; e += G) {
             const long long key = (long long)sign * level[sidx[s + e]];
             if (key > best_key) {
                 best_key = key;
@@ -410,8 +447,34 @@ __global__ void pack_fill_kernel(const int4* __restrict__ pack, int32_t ntasks, 
                 best_e = oe;
             }
         }
+        // slot k takes entry (k << cls) + gl, with entries 0 and best_e swapped
         const int mslots = d.w & 0xff;
-        for (int k = 0; k < mslots; ++k) {
+        int32_t id[kFillRegs];
+        double vv[kFillRegs];
+        float vf[kFillRegs];
+#pragma unroll
+        for (int k = 0; k < kFillRegs; ++k) {
+            int64_t e = ((int64_t)k << cls) + gl;
+            const bool have = k < mslots && e < len;
+            int32_t x = ix[k];
+            if (have && best_e != 0 && (e == 0 || e == best_e)) {
+                e = e == 0 ? best_e : 0;
+                x = sidx[s + e];
+            }
+            id[k] = have ? x : -1;
+            vv[k] = have ? sval[s + e] : 0.0;
+            vf[k] = have && pval32 ? sval32[s + e] : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < kFillRegs; ++k) {
+            if (k < mslots) {
+                const size_t o = ((size_t)d.y + k) * 32 + lane;
+                pidx[o] = id[k];
+                pval[o] = vv[k];
+                if (pval32) pval32[o] = vf[k];
+            }
+        }
+        for (int k = kFillRegs; k < mslots; ++k) {
             int64_t e = ((int64_t)k << cls) + gl;
             const size_t o = ((size_t)d.y + k) * 32 + lane;
             const bool have = e < len;
@@ -751,7 +814,12 @@ static cudaError_t build_one_schedule(const int32_t* level, const int64_t* ptr, 
     RCHOL_TRY(sc.get(&tstart, (int64_t)nb + 1));
     RCHOL_TRY(sc.get((char**)&tmp, (int64_t)scan_tmp_bytes(nb)));
     RCHOL_TRY(cudaMemsetAsync(hist, 0, sizeof(int32_t) * (size_t)nb, s));
-    sched_hist_kernel<<<grid_for(n, 256), 256, 0, s>>>(level, ptr, n, depth, backward, epl, key, hist);
+    {
+        const int nsh = nb <= kSchedSharedBins ? nb : 0;
+        const int grid = nsh > 0 ? grid_for(n, 256, 4) : grid_for(n, 256);
+        sched_hist_kernel<<<grid, 256, sizeof(int32_t) * (size_t)nsh, s>>>(level, ptr, n, depth, backward, epl,
+                                                                           key, hist, nsh);
+    }
     RCHOL_TRY(exclusive_scan_i32_to_i32(hist, start, nb, tmp, s));
     sched_task_count_kernel<<<grid_for(nb, 256), 256, 0, s>>>(hist, nb, tcount);
     RCHOL_TRY(exclusive_scan_i32_to_i32(tcount, tstart, nb, tmp, s));

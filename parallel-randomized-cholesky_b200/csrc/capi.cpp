@@ -106,7 +106,7 @@ void free_csc(DevCsc& a) {
 void free_work(FactorWork& w) {
     void* ps[] = {w.lcolptr, w.lrow,  w.lval, w.dep,  w.queue,  w.fcnt,   w.brow,     w.bval,       w.chead,
                   w.cnext,   w.crow,  w.cval, w.prow, w.pval,   w.pstart, w.pcnt,     w.diag,       w.gscratch,
-                  w.counters, w.counters64, w.scan_tmp, w.level, w.hscratch, w.hlock};
+                  w.counters, w.counters64, w.scan_tmp, w.level, w.hscratch, w.hlock, w.hcols};
     for (void* p : ps) cudaFree(p);
     w = FactorWork();
 }
@@ -169,6 +169,7 @@ rchol_status alloc_work(rchol_ctx* ctx, const PoolPlan& pp) {
     CK(dalloc(&w.pval, w.pool_cap), "alloc pool values");
     CK(dalloc(&w.pstart, n), "alloc pool starts");
     CK(dalloc(&w.pcnt, n), "alloc pool counts");
+    CK(dalloc(&w.hcols, rchol::kHugeColCap + 1), "alloc long-column list");
     CK(dalloc(&w.diag, n), "alloc diag");
     CK(dalloc(&w.level, n), "alloc levels");
     CK(cudaMalloc((void**)&w.gscratch, (size_t)warps * (size_t)w.gscratch_entries * rchol::kGlobalSlabBytes),
@@ -193,6 +194,7 @@ rchol_status lower_nnz(rchol_ctx* ctx, int64_t* out, cudaStream_t st = nullptr) 
     const int32_t n = ctx->A.n;
     if (!st) st = ctx->stream;
     int32_t* cnt = nullptr;
+    int32_t* huge = nullptr;
     int64_t* ptr = nullptr;
     void* tmp = nullptr;
     // temporaries from the context's scratch arena (released on return)
@@ -201,9 +203,10 @@ rchol_status lower_nnz(rchol_ctx* ctx, int64_t* out, cudaStream_t st = nullptr) 
         ~Release() { sc.reset(); }
     } release{ctx->scratch};
     CK(ctx->scratch.get(&cnt, n), "alloc counts");
+    CK(ctx->scratch.get(&huge, rchol::kHugeColCap + 1), "alloc long-column list");
     CK(ctx->scratch.get(&ptr, (int64_t)n + 1), "alloc ptr");
     CK(ctx->scratch.get((char**)&tmp, (int64_t)rchol::scan_tmp_bytes(n)), "alloc scan");
-    CK(rchol::launch_count_lower(ctx->A, cnt, st), "count lower");
+    CK(rchol::launch_count_lower(ctx->A, cnt, huge, st), "count lower");
     CK(rchol::exclusive_scan_i32_to_i64(cnt, ptr, n, tmp, st), "scan lower");
     CK(cudaMemcpyAsync(out, ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st), "copy lnnz");
     CK(cudaStreamSynchronize(st), "sync lnnz");

@@ -1373,30 +1373,40 @@ size_t tail_smem_bytes() { return sizeof(int) * (size_t)kTailIntWords + sizeof(d
 
 // The first c0 strict-lower entries of each column go into its fill bucket
 // (fcnt = their count), so that a vertex's gather usually reads one place.
+// A thread per column: stencil columns hold a few entries, and a warp per
+// column spent most of its time on the two dependent loads of the bounds.
 __global__ void prefill_bucket_kernel(int32_t n, int c0, const int32_t* __restrict__ lcolptr,
                                       const int32_t* __restrict__ lrow, const double* __restrict__ lval,
                                       int32_t* fcnt, int32_t* brow, double* bval) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < n; c += warps) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += stride) {
         const int s = lcolptr[c];
         const int cnt = min(lcolptr[c + 1] - s, c0);
-        for (int t = lane; t < cnt; t += 32) {
-            brow[(size_t)c * (size_t)c0 + t] = lrow[s + t];
-            bval[(size_t)c * (size_t)c0 + t] = lval[s + t];
+        int32_t* br = brow + (size_t)c * (size_t)c0;
+        double* bv = bval + (size_t)c * (size_t)c0;
+#pragma unroll 4
+        for (int t = 0; t < cnt; ++t) {
+            br[t] = lrow[s + t];
+            bv[t] = lval[s + t];
         }
-        if (lane == 0) fcnt[c] = cnt;
+        fcnt[c] = cnt;
     }
 }
 
 // Per column: entries below the diagonal (lower_cnt) and above it (dep,
-// count_minimum_dependencies, pre_process.hpp:474-496).  One warp/column.
-// Columns with at most kLaneCol entries are handled by one lane each (32
-// columns per warp in flight); longer ones by the whole warp, one at a time.
+// count_minimum_dependencies, pre_process.hpp:474-496).  Columns with at
+// most kLaneCol entries are handled by one lane each (32 columns per warp in
+// flight); longer ones by the whole warp, one at a time.  Columns longer than
+// kHugeCol (a ground vertex joined to every row with a diagonal excess, say)
+// would keep one warp busy for thousands of round trips, so they go to a
+// list (list[0] = count, then column ids; at most kHugeColCap, the rest stay
+// with their warp) with zero counts, and count_huge_kernel adds them up
+// with the whole grid.
 constexpr int kLaneCol = 32;
 
 __global__ void count_lower_kernel(int32_t n, const int32_t* __restrict__ colptr,
-                                   const int32_t* __restrict__ rowind, int32_t* lower_cnt, int32_t* dep) {
+                                   const int32_t* __restrict__ rowind, int32_t* lower_cnt, int32_t* dep,
+                                   int32_t* huge) {
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t c0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; c0 < n; c0 += nw * 32) {
@@ -1418,7 +1428,13 @@ __global__ void count_lower_kernel(int32_t n, const int32_t* __restrict__ colptr
             const int cs = __shfl_sync(kFull, s, src), ce = __shfl_sync(kFull, e, src);
             const int64_t cc = c0 + src;
             int l2 = 0, u2 = 0;
-            for (int p0 = cs + lane; p0 < ce; p0 += 8 * 32) {
+            int slot = kHugeColCap;
+            if (ce - cs > kHugeCol) {
+                if (lane == 0) slot = atomicAdd(huge, 1);
+                slot = __shfl_sync(kFull, slot, 0);
+                if (slot < kHugeColCap && lane == 0) huge[1 + slot] = (int32_t)cc;
+            }
+            for (int p0 = cs + lane; slot >= kHugeColCap && p0 < ce; p0 += 8 * 32) {
                 int r[8];
 #pragma unroll
                 for (int q = 0; q < 8; ++q) r[q] = p0 + 32 * q < ce ? rowind[p0 + 32 * q] : (int)cc;
@@ -1442,6 +1458,47 @@ __global__ void count_lower_kernel(int32_t n, const int32_t* __restrict__ colptr
             lower_cnt[c] = lo;
             if (dep) dep[c] = up;
         }
+    }
+}
+
+// The listed long columns, each spread over every thread of the grid; one
+// atomic add per block and column onto the zero counts count_lower_kernel
+// left (integer sums: the result does not depend on the order).
+__global__ void count_huge_kernel(const int32_t* __restrict__ colptr, const int32_t* __restrict__ rowind,
+                                  const int32_t* __restrict__ huge, int32_t* lower_cnt, int32_t* dep) {
+    __shared__ int red[2][32];
+    const int nh = min(huge[0], kHugeColCap);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int q = 0; q < nh; ++q) {
+        const int32_t c = huge[1 + q];
+        const int64_t s = colptr[c], e = colptr[c + 1];
+        int lo = 0, up = 0;
+        for (int64_t p = s + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < e; p += stride) {
+            const int r = rowind[p];
+            lo += r > c;
+            up += r < c;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo += __shfl_xor_sync(kFull, lo, o);
+            up += __shfl_xor_sync(kFull, up, o);
+        }
+        if (lane == 0) {
+            red[0][warp] = lo;
+            red[1][warp] = up;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int tl = 0, tu = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+                tl += red[0][w];
+                tu += red[1][w];
+            }
+            if (tl) atomicAdd(lower_cnt + c, tl);
+            if (dep && tu) atomicAdd(dep + c, tu);
+        }
+        __syncthreads();
     }
 }
 
@@ -1518,15 +1575,24 @@ __global__ void init_queue_kernel(int32_t n, const int32_t* __restrict__ dep, in
 
 // ---------------------------------------------------------------------------
 
-cudaError_t launch_count_lower(const DevCsc& A, int32_t* lower_cnt, cudaStream_t s) {
-    count_lower_kernel<<<grid_for(A.n, 256), 256, 0, s>>>(A.n, A.colptr, A.rowind, lower_cnt, nullptr);
+// count_lower_kernel, then count_huge_kernel for the long columns it listed
+// in `huge` (kHugeColCap + 1 words of scratch).
+static cudaError_t count_lower(const DevCsc& A, int32_t* lower_cnt, int32_t* dep, int32_t* huge, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(huge, 0, sizeof(int32_t), s);
+    if (e != cudaSuccess) return e;
+    count_lower_kernel<<<grid_for(A.n, 256), 256, 0, s>>>(A.n, A.colptr, A.rowind, lower_cnt, dep, huge);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    count_huge_kernel<<<2 * current_sm_count(), 256, 0, s>>>(A.colptr, A.rowind, huge, lower_cnt, dep);
     return cudaGetLastError();
+}
+
+cudaError_t launch_count_lower(const DevCsc& A, int32_t* lower_cnt, int32_t* huge, cudaStream_t s) {
+    return count_lower(A, lower_cnt, nullptr, huge, s);
 }
 
 cudaError_t launch_lower_and_deps(const DevCsc& A, FactorWork& w, cudaStream_t s) {
     // lower counts go to w.pcnt (scratch), dependency counts to w.dep
-    count_lower_kernel<<<grid_for(A.n, 256), 256, 0, s>>>(A.n, A.colptr, A.rowind, w.pcnt, w.dep);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = count_lower(A, w.pcnt, w.dep, w.hcols, s);
     if (e != cudaSuccess) return e;
     e = exclusive_scan_i32_to_i32(w.pcnt, w.lcolptr, A.n, w.scan_tmp, s);
     if (e != cudaSuccess) return e;
@@ -1545,7 +1611,7 @@ cudaError_t launch_init_factor_state(FactorWork& w, cudaStream_t s) {
     if ((e = cudaMemsetAsync(w.counters, 0, sizeof(int32_t) * 16, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.counters64, 0, sizeof(unsigned long long) * 4, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(w.hlock, 0, sizeof(int32_t) * w.nhuge, s)) != cudaSuccess) return e;
-    prefill_bucket_kernel<<<grid_for((int64_t)w.n * 32, 256), 256, 0, s>>>(w.n, w.c0, w.lcolptr, w.lrow, w.lval,
+    prefill_bucket_kernel<<<grid_for(w.n, 256), 256, 0, s>>>(w.n, w.c0, w.lcolptr, w.lrow, w.lval,
                                                                             w.fcnt, w.brow, w.bval);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     init_queue_kernel<<<grid_for(w.n, 256), 256, 0, s>>>(w.n, w.dep, w.queue, w.counters);

@@ -88,6 +88,12 @@ struct DevCsc {
 // own (spmv_long_kernel).
 constexpr int kLongRow = 2048;
 
+// Columns of the input longer than kHugeCol entries are counted by the whole
+// grid rather than one warp (count_lower, factor.cu); the list that carries
+// them holds kHugeColCap ids after its count word.
+constexpr int kHugeCol = 4096;
+constexpr int kHugeColCap = 1024;
+
 // Sliced-ELL copy of a DevCsc for the one-RHS SpMV (sell.cu): slice s of
 // 32 rows owns slots [sptr[s] * 32, sptr[s + 1] * 32), column-major (slot
 // (sptr[s] + k) * 32 + lane = entry k of row 32 s + lane; index -1 past the
@@ -130,6 +136,7 @@ struct FactorWork {
     double* pval = nullptr;       // [pool_cap]  (w / sum, positive)
     int64_t* pstart = nullptr;    // [n] column start in the pool
     int32_t* pcnt = nullptr;      // [n] merged neighbour count
+    int32_t* hcols = nullptr;     // [kHugeColCap + 1] long input columns (count, ids)
     double* diag = nullptr;       // [n] D
     int32_t* level = nullptr;     // [n] forward level (longest dependency chain) of each row of L
     // per-warp scratch for vertices that do not fit the shared-memory slab
@@ -316,7 +323,7 @@ struct FactorLaunch {
 
 // ---- setup / factor / assembly (factor.cu) --------------------------------
 cudaError_t launch_lower_and_deps(const DevCsc& A, FactorWork& w, cudaStream_t s);
-cudaError_t launch_count_lower(const DevCsc& A, int32_t* lower_cnt, cudaStream_t s);
+cudaError_t launch_count_lower(const DevCsc& A, int32_t* lower_cnt, int32_t* huge, cudaStream_t s);
 cudaError_t launch_init_factor_state(FactorWork& w, cudaStream_t s);
 cudaError_t launch_factor(FactorWork& w, const FactorLaunch& cfg, cudaStream_t s);
 int factor_resident_grid(int block, int smem_slab, int device);

@@ -19,6 +19,9 @@ CASES = {
     "grid40_unit": dict(dims=(40, 40), seed=2, log_weights=False),
     "cube10_sddm": dict(dims=(10, 10, 10), seed=3, excess_frac=0.05, wlo=1e-3, whi=1e3),
     "cube24_logw": dict(dims=(24, 24, 24), seed=4, wlo=1e-3, whi=1e3),
+    # every row has a diagonal excess: the ground column holds 5,833 entries,
+    # more than one warp counts (the grid-wide long-column count)
+    "cube18_ground_all": dict(dims=(18, 18, 18), seed=6, excess_frac=1.0, wlo=1e-3, whi=1e3),
 }
 
 
