@@ -383,9 +383,6 @@ __global__ void pack_desc_kernel(const int4* __restrict__ etask, int32_t ntasks,
 // except that entry 0 and the row's gate trade places.  The gate is the
 // dependency scheduled last (largest sign * level; the first such entry on
 // ties): the solve polls it alone before reading the rest of the row.
-// entries per lane whose slab indices pack_fill_kernel keeps in registers
-constexpr int kFillRegs = 8;
-
 __global__ void pack_fill_kernel(const int4* __restrict__ pack, int32_t ntasks, const int32_t* __restrict__ order,
                                  const int64_t* __restrict__ ptr, int split_len, const int32_t* __restrict__ sidx,
                                  const double* __restrict__ sval,
@@ -409,30 +406,9 @@ __global__ void pack_fill_kernel(const int4* __restrict__ pack, int32_t ntasks, 
                 len = min((int64_t)split_len, len - q0);
             }
         }
-        // gate of the row: best (key, entry) over the lane's entries, then over
-        // the G lanes.  The lane's first kFillRegs entries (slot k holds entry
-        // gl + k * G) have their indices, then their levels, loaded as one
-        // batch each; the indices are kept for the copy below.
-        int32_t ix[kFillRegs];
-#pragma unroll
-        for (int j = 0; j < kFillRegs; ++j) {
-            const int64_t e = ((int64_t)j << cls) + gl;
-            ix[j] = e < len ? sidx[s + e] : 0;
-        }
-        int32_t lv[kFillRegs];
-#pragma unroll
-        for (int j = 0; j < kFillRegs; ++j) lv[j] = (((int64_t)j << cls) + gl) < len ? level[ix[j]] : 0;
+        // gate of the row: best (key, entry) over the lane's entries, then over the G lanes
         long long best_key = LLONG_MIN, best_e = 0;
-#pragma unroll
-        for (int j = 0; j < kFillRegs; ++j) {
-            const int64_t e = ((int64_t)j << cls) + gl;
-            const long long key = (long long)sign * lv[j];
-            if (e < len && key > best_key) {
-                best_key = key;
-                best_e = e;
-            }
-        }
-        for (int64_t e = ((int64_t)kFillRegs << cls) + gl; e < len; e += G) {
+        for (int64_t e = gl; e < len; e += G) {
             const long long key = (long long)sign * level[sidx[s + e]];
             if (key > best_key) {
                 best_key = key;
@@ -447,34 +423,8 @@ __global__ void pack_fill_kernel(const int4* __restrict__ pack, int32_t ntasks, 
                 best_e = oe;
             }
         }
-        // slot k takes entry (k << cls) + gl, with entries 0 and best_e swapped
         const int mslots = d.w & 0xff;
-        int32_t id[kFillRegs];
-        double vv[kFillRegs];
-        float vf[kFillRegs];
-#pragma unroll
-        for (int k = 0; k < kFillRegs; ++k) {
-            int64_t e = ((int64_t)k << cls) + gl;
-            const bool have = k < mslots && e < len;
-            int32_t x = ix[k];
-            if (have && best_e != 0 && (e == 0 || e == best_e)) {
-                e = e == 0 ? best_e : 0;
-                x = sidx[s + e];
-            }
-            id[k] = have ? x : -1;
-            vv[k] = have ? sval[s + e] : 0.0;
-            vf[k] = have && pval32 ? sval32[s + e] : 0.0f;
-        }
-#pragma unroll
-        for (int k = 0; k < kFillRegs; ++k) {
-            if (k < mslots) {
-                const size_t o = ((size_t)d.y + k) * 32 + lane;
-                pidx[o] = id[k];
-                pval[o] = vv[k];
-                if (pval32) pval32[o] = vf[k];
-            }
-        }
-        for (int k = kFillRegs; k < mslots; ++k) {
+        for (int k = 0; k < mslots; ++k) {
             int64_t e = ((int64_t)k << cls) + gl;
             const size_t o = ((size_t)d.y + k) * 32 + lane;
             const bool have = e < len;

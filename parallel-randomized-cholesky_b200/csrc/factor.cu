@@ -1373,8 +1373,8 @@ size_t tail_smem_bytes() { return sizeof(int) * (size_t)kTailIntWords + sizeof(d
 
 // The first c0 strict-lower entries of each column go into its fill bucket
 // (fcnt = their count), so that a vertex's gather usually reads one place.
-// A thread per column: stencil columns hold a few entries, and a warp per
-// column spent most of its time on the two dependent loads of the bounds.
+// A thread per column (stencil columns hold a few entries); the cost is the
+// bucket writes, a few entries into each column's own c0-slot row.
 __global__ void prefill_bucket_kernel(int32_t n, int c0, const int32_t* __restrict__ lcolptr,
                                       const int32_t* __restrict__ lrow, const double* __restrict__ lval,
                                       int32_t* fcnt, int32_t* brow, double* bval) {

@@ -449,8 +449,10 @@ __global__ void __launch_bounds__(kBlock) spmv_long_k_kernel(SolveArgs a) {
     }
 }
 
+// 8 CTAs per SM (32 registers): the grid is 8 per SM, and the gathers of z
+// rows need every warp in flight
 template <int K>
-__global__ void __launch_bounds__(kBlock) spmv_update_kernel(SolveArgs a) {
+__global__ void __launch_bounds__(kBlock, 8) spmv_update_kernel(SolveArgs a) {
     if (ld_relaxed(&a.sc->done)) return;
     // one RHS: a thread per row; K RHS: K lanes per row, lane c owns column c
     constexpr int G = K;
