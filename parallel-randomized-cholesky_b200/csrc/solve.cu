@@ -714,11 +714,17 @@ __global__ void __launch_bounds__(kBlock) spmv_update_sell_kernel(SolveArgs a) {
     }
 }
 
+// The k > 1 solve kernels are compiled for 5 CTAs per SM (48 registers).
+// With an FP64 factor copy that spills a few bytes and still gains the fifth
+// CTA (k = 32 forward 5.0 -> 4.4 ms, backward 4.3 -> 3.9 ms on a 27-point
+// 128^3 factor); the FP32 forms needed 48 registers already.
+constexpr int kSolveMinBlocks = 5;
+
 // ---------------------------------------------------------------------------
 // fwd: x += alpha p; r -= alpha q; (r.r); y = L^{-1} r  (rows ascending)
 // ---------------------------------------------------------------------------
 template <int K, typename TV>
-__global__ void __launch_bounds__(kBlock) fwd_kernel(SolveArgs a) {
+__global__ void __launch_bounds__(kBlock, kSolveMinBlocks) fwd_kernel(SolveArgs a) {
     // K >= 2 right-hand sides: K lanes per row, lane c owns column c
     if ((a.reduce || a.seg) && ld_relaxed(&a.sc->done)) return;
     constexpr int G = K;
@@ -769,7 +775,7 @@ __global__ void __launch_bounds__(kBlock) fwd_kernel(SolveArgs a) {
 // bwd: z = L^{-T} D^+ y  (rows descending); (r.z) -> rz, beta
 // ---------------------------------------------------------------------------
 template <int K, typename TV>
-__global__ void __launch_bounds__(kBlock) bwd_kernel(SolveArgs a) {
+__global__ void __launch_bounds__(kBlock, kSolveMinBlocks) bwd_kernel(SolveArgs a) {
     // K >= 2 right-hand sides: K lanes per row, lane c owns column c
     if ((a.reduce || a.seg) && ld_relaxed(&a.sc->done)) return;
     constexpr int G = K;
