@@ -111,3 +111,32 @@ def zero_sum_normal(n, seed):
     rng = np.random.default_rng(seed)
     b = rng.standard_normal(n)
     return b - b.mean()
+
+
+def disconnected_laplacian():
+    """A 12^2 grid, a 6^3 grid and one vertex with no edges (an explicit zero
+    diagonal), in one ascending-degree order with a seeded tie-break.
+    Returns (n, rows, cols, vals, iso, comp1, comp2): the isolated vertex's
+    index and each grid's vertex indices in the combined order."""
+    n1, r1, c1, v1, _ = grid_laplacian((12, 12), seed=41)
+    n2, r2, c2, v2, _ = grid_laplacian((6, 6, 6), seed=42)
+    n = n1 + n2 + 1
+    rows = np.concatenate([r1, r2 + n1, [n - 1]]).astype(np.int64)
+    cols = np.concatenate([c1, c2 + n1, [n - 1]]).astype(np.int64)
+    vals = np.concatenate([v1, v2, [0.0]])
+    deg = np.bincount(rows[rows != cols], minlength=n)
+    rng = np.random.default_rng(43)
+    perm = rng.permutation(n)
+    order = perm[np.argsort(deg[perm], kind="stable")]
+    inv = np.empty(n, np.int64)
+    inv[order] = np.arange(n)
+    r, c = inv[rows].astype(np.int32), inv[cols].astype(np.int32)
+    return n, r, c, vals, int(inv[n - 1]), inv[:n1], inv[n1:n1 + n2]
+
+
+def per_component_rhs(n, comp1, comp2):
+    """Zero sum on each grid component, zero on the isolated vertex."""
+    b = np.zeros(n)
+    b[comp1] = zero_sum_normal(len(comp1), 44)
+    b[comp2] = zero_sum_normal(len(comp2), 45)
+    return b

@@ -11,7 +11,7 @@ import pytest
 
 import pyoracle as O
 import rchol_b200 as R
-from helpers import OracleProblem, grid_laplacian, zero_sum_normal
+from helpers import OracleProblem, disconnected_laplacian, grid_laplacian, per_component_rhs, zero_sum_normal
 
 pytestmark = pytest.mark.gpu
 
@@ -461,21 +461,7 @@ def test_disconnected_graph_with_isolated_vertex():
     (zero degree, D = 0), in one ascending-degree order: the factor is
     bit-exact, and PCG on a right-hand side with zero sum on every component
     converges like the oracle's and leaves the isolated vertex at 0."""
-    n1, r1, c1, v1, _ = grid_laplacian((12, 12), seed=41)
-    n2, r2, c2, v2, _ = grid_laplacian((6, 6, 6), seed=42)
-    n = n1 + n2 + 1
-    rows = np.concatenate([r1, r2 + n1, [n - 1]]).astype(np.int64)
-    cols = np.concatenate([c1, c2 + n1, [n - 1]]).astype(np.int64)
-    vals = np.concatenate([v1, v2, [0.0]])
-    # ascending degree with a seeded tie-break across both components
-    deg = np.bincount(rows[rows != cols], minlength=n)
-    rng = np.random.default_rng(43)
-    perm = rng.permutation(n)
-    order = perm[np.argsort(deg[perm], kind="stable")]
-    inv = np.empty(n, np.int64)
-    inv[order] = np.arange(n)
-    r, c = inv[rows].astype(np.int32), inv[cols].astype(np.int32)
-    iso = int(inv[n - 1])
+    n, r, c, vals, iso, comp1, comp2 = disconnected_laplacian()
     P = OracleProblem(n, r, c, vals)
     orc = P.factor(seed=9)
     ctx = R.Context(seed=9)
@@ -486,10 +472,7 @@ def test_disconnected_graph_with_isolated_vertex():
         assert np.array_equal(cp, orc["colptr"]) and np.array_equal(ri, orc["rowind"])
         assert np.array_equal(val, orc["val"]) and np.array_equal(d, orc["diag"])
         assert d[iso] == 0.0
-        b = np.zeros(n)
-        comp1, comp2 = inv[:n1], inv[n1:n1 + n2]
-        b[comp1] = zero_sum_normal(n1, 44)
-        b[comp2] = zero_sum_normal(n2, 45)
+        b = per_component_rhs(n, comp1, comp2)
         x, info = ctx.pcg_solve(f, b)
         xo, io = P.pcg(orc, b, tol=1e-6)
         assert info["status"] == 0 and info["converged"] and info["relres_true"] <= 1e-6

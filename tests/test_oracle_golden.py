@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 import pyoracle as O
-from helpers import GOLDEN, OracleProblem, read_reference_factor
+from helpers import GOLDEN, OracleProblem, disconnected_laplacian, per_component_rhs, read_reference_factor
 
 
 def test_mt19937_standard_value():
@@ -127,3 +127,19 @@ def test_oracle_pcg_converges_on_golden():
     b = O.zero_sum_vector(P.ns, 0)
     x, info = P.pcg(f, b, tol=1e-10)
     assert info["converged"] and info["relres_true"] <= 1e-10
+
+
+def test_oracle_disconnected_graph_with_isolated_vertex():
+    """The oracle on two components and a zero-degree vertex: one D = 0 pivot
+    per component (its last vertex) plus the isolated vertex, an empty
+    column there, and a PCG that converges on a right-hand side with zero
+    sum per component without touching the isolated vertex."""
+    n, r, c, vals, iso, comp1, comp2 = disconnected_laplacian()
+    P = OracleProblem(n, r, c, vals)
+    f = P.factor(seed=9)
+    assert n == 361 and f["diag"][iso] == 0.0
+    assert int((f["diag"] == 0.0).sum()) == 3
+    assert f["colptr"][iso + 1] == f["colptr"][iso]
+    x, info = P.pcg(f, per_component_rhs(n, comp1, comp2), tol=1e-6)
+    assert info["converged"] and info["relres_true"] <= 1e-6
+    assert x[iso] == 0.0
